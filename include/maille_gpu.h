@@ -1,0 +1,164 @@
+/* maille_gpu.h -- C ABI of the B200 linear-elastic solve path (Tet4/Tet10 stiffness, deterministic
+ * sparse assembly, IC(0)-preconditioned conjugate gradients, Gauss-point stresses).
+ *
+ * The entry points replace the iterative branch of maille-core's solve (reference paths, relative
+ * to the reference project root):
+ *   - Model::solve                      crates/maille-core/src/model.rs:548-610
+ *   - FreeSystem::new / ::solve         crates/maille-core/src/model.rs:1442-1516
+ *   - FreeMatrix / Factor dispatch      crates/maille-core/src/model.rs:1390-1423
+ *   - Pcg::new / Pcg::solve             crates/maille-core/src/iterative.rs:199-248
+ *   - element_stiffness / _stresses     crates/maille-core/src/assembly.rs:64-79, 304-312
+ *   - product (reactions)               crates/maille-core/src/model.rs:1353-1369
+ * A host program calls them where SolverKind::is_iterative (solve.rs:187-195) selects the PCG
+ * path; the skyline direct solver stays in the host program.
+ *
+ * Conventions: all pointers are caller-owned host memory unless stated; the library copies in and
+ * out and never keeps host pointers. Every call returns a MailleStatus; no call aborts or throws
+ * across the ABI. Device code never traps: failures are written to an on-device status word that
+ * the host reads. A handle is used by one host thread at a time (it may move between threads).
+ */
+#ifndef MAILLE_GPU_H
+#define MAILLE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return codes, mirroring MailleError on this path (crates/maille-core/src/error.rs). */
+typedef enum {
+    MAILLE_OK = 0,
+    MAILLE_SINGULAR = 1,      /* IC(0) failed every diagonal shift, or p.Ap <= 0 / NaN
+                                 -> MailleError::Singular (error.rs:224) */
+    MAILLE_NOT_CONVERGED = 2, /* iteration cap reached -> IterativeNotConverged{iterations,
+                                 residual} (error.rs:226-229) */
+    MAILLE_INVALID_INPUT = 3, /* bad sizes, node index out of range, non-finite input */
+    MAILLE_CUDA_ERROR = 4,    /* message through maille_gpu_last_error() */
+    MAILLE_CANCELLED = 5      /* the cancel flag was raised (MailleError::Cancelled, error.rs:156) */
+} MailleStatus;
+
+/* Storage precision of the matrix and preconditioner. */
+typedef enum {
+    MAILLE_FP64 = 0,  /* plain form: FP64 throughout */
+    MAILLE_MIXED = 1  /* FP32 matrix and IC(0) factor in an FP32 inner PCG, inside FP64
+                         iterative refinement (outer residual f - K u against FP64 K, FP64
+                         solution accumulation, FP64 refinement dots, FP64 factor pivots) */
+} MaillePrecision;
+
+/* Ordering of the free nodes for the level-scheduled IC(0). */
+typedef enum {
+    MAILLE_ORDER_AUTO = 0,       /* multicolour */
+    MAILLE_ORDER_MULTICOLOR = 1, /* greedy colouring of the node graph visited in RCM order:
+                                    one level per colour, a few dozen levels */
+    MAILLE_ORDER_RCM = 2         /* reverse Cuthill-McKee on the node graph (the reference's
+                                    algorithm, solve.rs:200-245, applied to nodes): the
+                                    reference's convergence, hundreds of levels */
+} MailleOrdering;
+
+/* A linear static Tet4/Tet10 model (Model after `assemble`, model.rs:1070-1147). */
+typedef struct {
+    int64_t n_nodes;
+    const double* coords;    /* [3 n_nodes] x, y, z per node */
+    int32_t nodes_per_elem;  /* 4 (Tet4, TETRA_1 rule) or 10 (Tet10, TETRA_4 rule) */
+    int64_t n_elems;
+    const int64_t* conn;     /* [n_elems * nodes_per_elem], Maille node order (Tet10 mid-edge
+                                nodes in TET10_EDGES order, shape.rs:135) */
+    const double* young;     /* [n_elems] E per element (Tet4/Tet10 carry their Material) */
+    const double* poisson;   /* [n_elems] nu per element */
+    const uint8_t* fixed;    /* [3 n_nodes] 1 where a Bc fixes the DOF (3 node + c) */
+    const double* imposed;   /* [3 n_nodes] imposed values at fixed DOFs (ignored elsewhere) */
+    const double* f;         /* [3 n_nodes] assembled nodal loads F (loads + face pressures), or
+                                NULL for zero */
+    double rel_tol;          /* stop at ||r|| <= rel_tol ||b|| (the reference uses 1e-12);
+                                <= 0 selects 1e-12 */
+    int32_t max_iter;        /* <= 0 selects 10000 (iterative.rs:11) */
+    int32_t precision;       /* MaillePrecision */
+    int32_t ordering;        /* MailleOrdering */
+    int32_t device;          /* CUDA device ordinal */
+} MailleElasticProblem;
+
+/* Results, caller-allocated; any output pointer may be NULL to skip it. */
+typedef struct {
+    double* u;             /* [3 n_nodes] displacements (Field::displacements) */
+    double* reactions;     /* [3 n_nodes] K u - F at fixed DOFs, 0 elsewhere (Field::reactions) */
+    double* gauss_stress;  /* [n_elems * ngp * 9] per Gauss point: x, y, z, sxx, syy, szz, txy,
+                              tyz, txz (Stress, results.rs:6-20); ngp = 1 (Tet4) or 4 (Tet10) */
+    double* von_mises;     /* [n_elems * ngp] Stress::von_mises (results.rs:24-32) */
+    /* filled by the library */
+    int32_t iterations;         /* PCG iterations (mixed: total inner iterations) */
+    int32_t outer_iterations;   /* mixed: refinement steps; plain: 1 */
+    double final_rel_residual;  /* ||f - K u|| / ||f|| in FP64 on the free DOFs */
+    double shift;               /* diagonal shift IC(0) succeeded with (iterative.rs:14) */
+    int64_t free_dofs;
+    int64_t block_rows;         /* free nodes in the 3x3-block system */
+    int64_t blocks;             /* 3x3 blocks of the full symmetric pattern */
+    int32_t levels;             /* levels of the IC(0) sweeps */
+    double ms_setup;            /* host symbolic analysis (graph, ordering, pattern, scatter map) */
+    double ms_upload;           /* host -> device copies */
+    double ms_assembly;         /* element integration + scatter-reduce assembly */
+    double ms_factor;           /* IC(0) factorisation incl. shift retries */
+    double ms_solve;            /* PCG iterations (mixed: incl. refinement) */
+    double ms_post;             /* reactions + stresses + von Mises */
+    double ms_download;         /* device -> host copies */
+} MailleElasticResult;
+
+typedef struct MailleGpuHandle MailleGpuHandle;
+
+/* Last error message of the calling thread (empty string when none). */
+const char* maille_gpu_last_error(void);
+
+/* Library version string. */
+const char* maille_gpu_version(void);
+
+/* Number of CUDA devices visible (0 when none; never an error). */
+int32_t maille_gpu_device_count(void);
+
+/* One-shot solve: create + solve + destroy. Replaces, for a Tet4/Tet10 linear static model,
+ * FreeSystem::new (model.rs:1442-1499) with Pcg::new (iterative.rs:201-207), FreeSystem::solve
+ * (model.rs:1502-1516) with Pcg::solve (iterative.rs:210-248), then product (model.rs:586-593,
+ * 1353-1369) and element_stresses (model.rs:596-598). */
+int32_t maille_gpu_elastic_solve(const MailleElasticProblem* problem, MailleElasticResult* result);
+
+/* Handle API (reuse one analysis for several right-hand sides; the adjoint).
+ * create: symbolic analysis + upload + element integration + assembly + IC(0) factorisation
+ * (FreeSystem::new + Pcg::new). The handle owns all device memory. */
+int32_t maille_gpu_create(const MailleElasticProblem* problem, MailleGpuHandle** out);
+
+/* Solve K_ff u_f = F_f - K_fc u_c for a new load vector f ([3 n_nodes], NULL = the problem's),
+ * then reactions and stresses into `result` (FreeSystem::solve + product + element_stresses). */
+int32_t maille_gpu_solve(MailleGpuHandle* h, const double* f, MailleElasticResult* result);
+
+/* Adjoint of the last solve: with g = dJ/du ([3 n_nodes], host), solves K_ff lambda_f = g_f with
+ * the same PCG and factor (lambda = 0 on fixed DOFs), then
+ *   dJ/dE_e = -lambda_e^T (dK_e/dE_e) u_e = -lambda_e^T K_e u_e / E_e
+ * for every element into dJdE ([n_elems]). lambda ([3 n_nodes]) is returned when not NULL.
+ * No counterpart in the reference (it has no gradients). */
+int32_t maille_gpu_backward(MailleGpuHandle* h, const double* dJdu, double* dJdE, double* lambda);
+
+/* Raise (1) or clear (0) the cancel flag; checked between PCG iteration chunks. Safe to call
+ * from another thread while a solve runs (the Observer / Flow::Stop role, model.rs:1203-1218). */
+void maille_gpu_cancel(MailleGpuHandle* h, int32_t flag);
+
+/* CUDA stream (cudaStream_t) the handle launches on, for event timing by the caller. */
+void* maille_gpu_stream(MailleGpuHandle* h);
+
+void maille_gpu_destroy(MailleGpuHandle* h);
+
+/* Host helper: adds the nodal forces of face pressures to f ([3 n_nodes]):
+ * f_a -= p * integral over the face of N_a n dS, n the outward normal (face_pressure,
+ * assembly.rs:650-674, with the tet branch of face_rule, assembly.rs:556-585; TRIANGLE_3 on Tet4
+ * faces, TRIANGLE_6 on Tet10 faces). Faces are (element, face in 0..3: 0-1-2, 0-3-1, 1-3-2,
+ * 2-3-0) pairs; an out-of-range element or face adds nothing, like face_rule's None. Runs on the
+ * host: it is the part of the host program's `assemble` (model.rs:1124-1131) a caller without
+ * its own face integration needs. */
+int32_t maille_gpu_face_pressure_loads(int64_t n_nodes, const double* coords, int32_t npe,
+                                       int64_t n_elems, const int64_t* conn, int64_t n_press,
+                                       const int64_t* p_elem, const int32_t* p_face,
+                                       const double* p_value, double* f);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MAILLE_GPU_H */

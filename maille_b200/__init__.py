@@ -1,0 +1,10 @@
+"""maille_b200 -- B200 (sm_100a) implementation of maille-core's linear-elastic solve path:
+Tet4/Tet10 element stiffness, deterministic sparse assembly and IC(0)-preconditioned conjugate
+gradients, with Gauss-point stresses. The compute runs in libmaille_gpu.so (CUDA, C ABI in
+include/maille_gpu.h); this package is the host-side mirror of the reference's solve interface.
+"""
+from .model import (Bc, Dof, Field, ITERATIVE_FROM, Load, MailleError, Material, Mesh, Model,  # noqa: F401
+                    Pressure, SolverHandle, SolverKind, face_pressure_loads)
+from ._lib import MAILLE_FP64, MAILLE_MIXED, MAILLE_ORDER_AUTO, MAILLE_ORDER_MULTICOLOR, MAILLE_ORDER_RCM  # noqa: F401
+
+__version__ = "0.1.0"

@@ -1,0 +1,91 @@
+"""ctypes binding of the C ABI declared in include/maille_gpu.h (libmaille_gpu.so, in-tree).
+
+The library is the product: there is no Python or CPU fallback. Loading fails loudly when the
+shared library is missing, and every compute call reports the library's status codes.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmaille_gpu.so")
+
+MAILLE_OK, MAILLE_SINGULAR, MAILLE_NOT_CONVERGED, MAILLE_INVALID_INPUT, MAILLE_CUDA_ERROR, \
+    MAILLE_CANCELLED = range(6)
+MAILLE_FP64, MAILLE_MIXED = 0, 1
+MAILLE_ORDER_AUTO, MAILLE_ORDER_MULTICOLOR, MAILLE_ORDER_RCM = 0, 1, 2
+
+_d = ctypes.POINTER(ctypes.c_double)
+_i64 = ctypes.POINTER(ctypes.c_int64)
+_i32 = ctypes.POINTER(ctypes.c_int32)
+_u8 = ctypes.POINTER(ctypes.c_uint8)
+
+
+class ElasticProblem(ctypes.Structure):
+    _fields_ = [
+        ("n_nodes", ctypes.c_int64), ("coords", _d), ("nodes_per_elem", ctypes.c_int32),
+        ("n_elems", ctypes.c_int64), ("conn", _i64), ("young", _d), ("poisson", _d),
+        ("fixed", _u8), ("imposed", _d), ("f", _d), ("rel_tol", ctypes.c_double),
+        ("max_iter", ctypes.c_int32), ("precision", ctypes.c_int32), ("ordering", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+class ElasticResult(ctypes.Structure):
+    _fields_ = [
+        ("u", _d), ("reactions", _d), ("gauss_stress", _d), ("von_mises", _d),
+        ("iterations", ctypes.c_int32), ("outer_iterations", ctypes.c_int32),
+        ("final_rel_residual", ctypes.c_double), ("shift", ctypes.c_double),
+        ("free_dofs", ctypes.c_int64), ("block_rows", ctypes.c_int64), ("blocks", ctypes.c_int64),
+        ("levels", ctypes.c_int32), ("ms_setup", ctypes.c_double), ("ms_upload", ctypes.c_double),
+        ("ms_assembly", ctypes.c_double), ("ms_factor", ctypes.c_double),
+        ("ms_solve", ctypes.c_double), ("ms_post", ctypes.c_double),
+        ("ms_download", ctypes.c_double),
+    ]
+
+
+# every symbol include/maille_gpu.h declares, with its ctypes signature
+SIGNATURES = {
+    "maille_gpu_last_error": ([], ctypes.c_char_p),
+    "maille_gpu_version": ([], ctypes.c_char_p),
+    "maille_gpu_device_count": ([], ctypes.c_int32),
+    "maille_gpu_elastic_solve": ([ctypes.POINTER(ElasticProblem), ctypes.POINTER(ElasticResult)],
+                                 ctypes.c_int32),
+    "maille_gpu_create": ([ctypes.POINTER(ElasticProblem), ctypes.POINTER(ctypes.c_void_p)],
+                          ctypes.c_int32),
+    "maille_gpu_solve": ([ctypes.c_void_p, _d, ctypes.POINTER(ElasticResult)], ctypes.c_int32),
+    "maille_gpu_backward": ([ctypes.c_void_p, _d, _d, _d], ctypes.c_int32),
+    "maille_gpu_cancel": ([ctypes.c_void_p, ctypes.c_int32], None),
+    "maille_gpu_stream": ([ctypes.c_void_p], ctypes.c_void_p),
+    "maille_gpu_destroy": ([ctypes.c_void_p], None),
+    "maille_gpu_face_pressure_loads": ([ctypes.c_int64, _d, ctypes.c_int32, ctypes.c_int64, _i64,
+                                        ctypes.c_int64, _i64, _i32, _d, _d], ctypes.c_int32),
+}
+
+_lib = None
+
+
+def load():
+    """Loads libmaille_gpu.so (raises if it was not built: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m maille_b200.build`")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+    return _lib
+
+
+def last_error() -> str:
+    return load().maille_gpu_last_error().decode()
+
+
+def ptr(a, t):
+    return a.ctypes.data_as(t) if a is not None else None

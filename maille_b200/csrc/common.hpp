@@ -1,0 +1,71 @@
+// common.hpp -- shared host/device definitions of the B200 linear-elastic solve library.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/maille_gpu.h"
+
+namespace maille {
+
+// Tet element facts: nodes per element, Gauss points (TETRA_1 / TETRA_4, assembly.rs:212-229),
+// node pairs (a <= b) of the symmetric element matrix.
+inline int gauss_points(int npe) { return npe == 4 ? 1 : 4; }
+inline int node_pairs(int npe) { return npe * (npe + 1) / 2; }
+
+// Error carried up to the C ABI.
+struct Error {
+    int32_t status;
+    std::string message;
+};
+
+// Symbolic analysis of one mesh: everything that depends on topology and the fixed-DOF mask but
+// not on material values or loads. Built on the host (setup.cpp), uploaded once per handle.
+//
+// Block system: one 3x3 block row per "kept" node (a node with at least one free DOF). Fixed
+// DOFs of a kept node become identity rows/columns, so the free-DOF matrix K_ff is embedded
+// exactly; nodes with all three DOFs fixed are dropped. Rows are numbered in solver order
+// (perm[new] = old node), grouped by level: rows of level l are [level_ptr[l], level_ptr[l+1])
+// and depend only on rows of earlier levels in the lower triangle.
+struct Symbolic {
+    int64_t n_nodes = 0, n_elems = 0;
+    int npe = 0;
+    int32_t nb = 0;                    // block rows
+    int64_t free_dofs = 0;
+    std::vector<int32_t> perm;         // new -> old node
+    std::vector<int32_t> inv;          // old node -> new row, -1 when dropped
+    std::vector<uint8_t> fixmask;      // per new row: bit c set when DOF c is fixed
+    std::vector<int32_t> level_ptr;    // [levels + 1]
+    int32_t levels = 0;
+    // full symmetric 3x3-block CSR pattern in new numbering, columns ascending
+    std::vector<int64_t> row_ptr;      // [nb + 1]
+    std::vector<int32_t> col;          // [B]
+    std::vector<int64_t> diag;         // [nb] position of the diagonal block
+    std::vector<int64_t> tpos;         // [B] position of the transposed block
+    int64_t blocks = 0;
+    // deterministic assembly: lower slots (col <= row), each summing a sorted list of element
+    // node-pair blocks. contrib entry = (e * npairs + pair) | (transpose << 31)
+    std::vector<int64_t> lslot;        // [NL] position of the lower slot in the full pattern
+    std::vector<int64_t> lptr;         // [NL + 1]
+    std::vector<uint32_t> contrib;     // [pairs kept]
+    // node -> (element, local node) incidence over all nodes, sorted by element
+    std::vector<int64_t> inc_ptr;      // [n_nodes + 1]
+    std::vector<int32_t> inc;          // [n_elems * npe] e * npe + a
+    // elements that touch a fixed DOF (for the coupling K_fc u_c and the reactions)
+    std::vector<int32_t> belem;
+    std::vector<int32_t> bnodes;       // nodes with a fixed DOF that belong to a boundary element
+    double ms = 0.0;
+};
+
+// Builds the symbolic analysis. conn is [n_elems * npe] in the caller's node numbering.
+bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
+             const uint8_t* fixed, int ordering, Symbolic& s, Error& err);
+
+// Face pressure loads f_a -= p * integral(N_a n dS) added into f (assembly.rs:650-674 with the
+// tet branch of face_rule, assembly.rs:556-585). Host-side: part of the host program's assemble.
+bool face_pressure_loads(int64_t n_nodes, const double* coords, int npe, int64_t n_elems,
+                         const int64_t* conn, int64_t n_press, const int64_t* p_elem,
+                         const int32_t* p_face, const double* p_value, double* f, Error& err);
+
+}  // namespace maille

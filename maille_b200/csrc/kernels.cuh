@@ -1,0 +1,99 @@
+// kernels.cuh -- sm_100a kernels of the linear-elastic solve path.
+//
+// Data layout in HBM (new = solver numbering of the kept nodes, see setup.cpp):
+//   * K and F (the IC(0) factor) share one full 3x3-block CSR pattern: row_ptr (int64), col
+//     (int32), values as 9 consecutive entries per block, row-major (AoS). F holds L below the
+//     diagonal, L^T above it (so both sweeps gather along rows) and D = L_II^-1 on the diagonal.
+//   * Vectors are [3 nb] in new numbering, DOF c of row I at 3 I + c.
+//   * Element matrices are kept as their node-pair blocks a <= b: Ke[(e * NP + pair) * 9 + 3 i + j]
+//     = K_e[3 a + i][3 b + j].
+// Every reduction is deterministic: fixed per-warp shuffle trees, per-block partials in fixed
+// slots, and a final sum in slot order by the last block to finish (ticket counter).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace maille {
+
+constexpr int kThreads = 256;       // threads per block of the row kernels
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxLevels = 65536;
+
+// Device-resident scalars of one PCG run.
+struct PcgScalars {
+    double alpha, beta, rz, rr, bb, tol, pap;
+    int32_t iter, max_iter, done, status;  // status: 0 ok, 1 singular (also NaN)
+    unsigned int ticket[4];                // 0 spmv, 1 fwd, 2 bwd, 3 misc
+};
+
+// Element geometry / material inputs (old numbering).
+struct ElemIn {
+    int64_t ne;
+    const double* coords;
+    const int32_t* conn;
+    const double* young;
+    const double* poisson;
+};
+
+struct Pattern {
+    int32_t nb;
+    const int64_t* row_ptr;
+    const int32_t* col;
+    const int64_t* diag;
+    const int64_t* tpos;
+    const uint8_t* fixmask;
+};
+
+// ---- launchers (defined in kernels.cu) -------------------------------------------------------
+void launch_elem_stiffness(int npe, const ElemIn& in, double* ke_up, cudaStream_t st);
+void launch_assemble(const Pattern& pt, int64_t nl, const int64_t* lslot, const int32_t* lrow,
+                     const int64_t* lptr,
+                     const uint32_t* contrib, const double* ke_up, double* K, cudaStream_t st);
+void launch_factor_level(const Pattern& pt, int32_t r0, int32_t r1, const double* K, double* F,
+                        double shift, int32_t* fail, cudaStream_t st);
+template <typename T>
+void launch_spmv_pcg(const Pattern& pt, const T* K, const T* p, T* ap, PcgScalars* s,
+                     double* partials, int grid, cudaStream_t st);
+template <typename T>
+void launch_fwd(const Pattern& pt, int32_t r0, int32_t r1, int level, int nlevels, const T* F,
+                T* r, T* y, T* x, const T* p, const T* ap, PcgScalars* s, double* partials,
+                double* lvl_total, int grid, cudaStream_t st);
+template <typename T>
+void launch_bwd(const Pattern& pt, int32_t r0, int32_t r1, int level, const T* F, const T* r,
+                T* z, PcgScalars* s, double* partials, double* lvl_total, int nlevels, int grid,
+                cudaStream_t st);
+template <typename T>
+void launch_pupdate(int64_t n, const T* z, T* p, PcgScalars* s, cudaStream_t st);
+void launch_residual64(const Pattern& pt, const double* K, const double* b, const double* u,
+                       double* r, double* partials, unsigned int* ticket, double* out_sum,
+                       int grid, cudaStream_t st);
+void launch_norm2(int64_t n, const double* v, double* partials, unsigned int* ticket,
+                  double* out_sum, int grid, cudaStream_t st);
+void launch_scale_to_float(int64_t n, const double* src, const double* norm2, float* dst,
+                           cudaStream_t st);
+void launch_accumulate(int64_t n, const float* d, const double* norm2, double* u,
+                       cudaStream_t st);
+void launch_to_float(int64_t n, const double* src, float* dst, cudaStream_t st);
+void launch_norm2_f(int64_t n, const float* v, double* partials, unsigned int* ticket,
+                    double* out_sum, int grid, cudaStream_t st);
+void launch_pcg_init(PcgScalars* s, double tol, int32_t max_iter, cudaStream_t st);
+void launch_build_rhs(int32_t nb, const int32_t* perm, const uint8_t* fixmask, const double* f,
+                      const double* coupling, double* b, cudaStream_t st);
+void launch_gather_u(int64_t n_nodes, const int32_t* inv, const uint8_t* fixed,
+                     const double* imposed, const double* x, double* u, cudaStream_t st);
+void launch_elem_apply(int npe, int64_t nlist, const int32_t* list, const int32_t* conn,
+                       const double* ke_up, const double* u, double* ye, cudaStream_t st);
+void launch_node_gather(int npe, int64_t nnodes, const int32_t* nodes, const int64_t* inc_ptr,
+                        const int32_t* inc, const int32_t* elem_slot, const double* ye,
+                        double* y, cudaStream_t st);
+void launch_reactions(int64_t n_nodes, const int32_t* nodes, int64_t nnodes,
+                      const uint8_t* fixed, const double* y, const double* f, double* react,
+                      cudaStream_t st);
+void launch_stresses(int npe, const ElemIn& in, const double* u, double* gauss, double* vm,
+                     cudaStream_t st);
+void launch_adjoint_grad(int npe, int64_t ne, const int32_t* conn, const double* ke_up,
+                         const double* young, const double* lambda, const double* u,
+                         double* grad, cudaStream_t st);
+
+}  // namespace maille

@@ -1,0 +1,433 @@
+// setup.cpp -- host-side symbolic analysis: kept nodes, node graph, ordering (RCM or multicolour),
+// level sets, the full 3x3-block CSR pattern and the deterministic element-to-slot scatter map.
+//
+// Reference counterparts: FreeSystem::new numbers the free DOFs, builds the DOF graph
+// (Graph::from_elements, iterative.rs:38-76), orders it by reverse_cuthill_mckee (solve.rs:200-245)
+// and allocates the lower-triangular CSR profile (Csr::zeros, iterative.rs:91-114); each element
+// matrix entry is then added by a binary search (Csr::add, iterative.rs:121-128). Here the same
+// work is done once per mesh topology on nodes instead of scalar DOFs, and the binary searches
+// are replaced by a precomputed scatter map that the GPU reduces in a fixed order.
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <numeric>
+
+#include "common.hpp"
+
+namespace maille {
+namespace {
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+struct NodeGraph {
+    std::vector<int64_t> off;   // [n + 1]
+    std::vector<int32_t> adj;   // neighbours, self excluded, element-encounter order
+    int64_t degree(int32_t v) const { return off[v + 1] - off[v]; }
+};
+
+// BFS levels from `start` that do not enter `excluded` vertices (bfs_levels, solve.rs:248-270).
+std::vector<std::vector<int32_t>> bfs_levels(const NodeGraph& g, int32_t start,
+                                             const std::vector<uint8_t>& excluded) {
+    std::vector<uint8_t> seen = excluded;
+    seen[start] = 1;
+    std::vector<std::vector<int32_t>> levels{{start}};
+    for (;;) {
+        std::vector<int32_t> next;
+        for (int32_t v : levels.back())
+            for (int64_t p = g.off[v]; p < g.off[v + 1]; ++p) {
+                const int32_t w = g.adj[p];
+                if (!seen[w]) {
+                    seen[w] = 1;
+                    next.push_back(w);
+                }
+            }
+        if (next.empty()) return levels;
+        levels.push_back(std::move(next));
+    }
+}
+
+// Reverse Cuthill-McKee with a George-Liu pseudo-peripheral start and neighbours visited by
+// increasing degree (stable), one connected component at a time; the algorithm of
+// reverse_cuthill_mckee (solve.rs:200-245), applied to the node graph. order[new] = old.
+std::vector<int32_t> rcm(const NodeGraph& g) {
+    const int32_t n = (int32_t)g.off.size() - 1;
+    std::vector<uint8_t> visited(n, 0);
+    std::vector<int32_t> order;
+    order.reserve(n);
+    int32_t scan = 0;
+    for (;;) {
+        while (scan < n && visited[scan]) ++scan;
+        int32_t seed = -1;
+        for (int32_t v = scan; v < n; ++v)
+            if (!visited[v] && (seed < 0 || g.degree(v) < g.degree(seed))) seed = v;
+        if (seed < 0) break;
+        int32_t start = seed;
+        auto levels = bfs_levels(g, start, visited);
+        for (;;) {
+            int32_t far = -1;
+            for (int32_t v : levels.back())
+                if (far < 0 || g.degree(v) < g.degree(far)) far = v;
+            if (far < 0) break;
+            auto far_levels = bfs_levels(g, far, visited);
+            if (far_levels.size() <= levels.size()) break;
+            start = far;
+            levels = std::move(far_levels);
+        }
+        size_t head = order.size();
+        visited[start] = 1;
+        order.push_back(start);
+        std::vector<int32_t> next;
+        while (head < order.size()) {
+            const int32_t v = order[head++];
+            next.clear();
+            for (int64_t p = g.off[v]; p < g.off[v + 1]; ++p)
+                if (!visited[g.adj[p]]) next.push_back(g.adj[p]);
+            std::stable_sort(next.begin(), next.end(), [&](int32_t a, int32_t b) {
+                return g.degree(a) < g.degree(b);
+            });
+            for (int32_t w : next)
+                if (!visited[w]) {
+                    visited[w] = 1;
+                    order.push_back(w);
+                }
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    return order;
+}
+
+// Greedy colouring visiting vertices in `visit` order; returns colours.
+std::vector<int32_t> greedy_colour(const NodeGraph& g, const std::vector<int32_t>& visit) {
+    const int32_t n = (int32_t)visit.size();
+    std::vector<int32_t> colour(n, -1);
+    std::vector<int32_t> stamp;  // stamp[c] == v: colour c used by a neighbour of v
+    for (int32_t v : visit) {
+        for (int64_t p = g.off[v]; p < g.off[v + 1]; ++p) {
+            const int32_t c = colour[g.adj[p]];
+            if (c >= 0) {
+                if ((size_t)c >= stamp.size()) stamp.resize(c + 1, -1);
+                stamp[c] = v;
+            }
+        }
+        int32_t c = 0;
+        while ((size_t)c < stamp.size() && stamp[c] == v) ++c;
+        colour[v] = c;
+    }
+    return colour;
+}
+
+}  // namespace
+
+bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
+             const uint8_t* fixed, int ordering, Symbolic& s, Error& err) {
+    const double t0 = now_ms();
+    if (npe != 4 && npe != 10) {
+        err = {MAILLE_INVALID_INPUT, "nodes_per_elem must be 4 or 10"};
+        return false;
+    }
+    if (n_nodes <= 0 || n_elems <= 0) {
+        err = {MAILLE_INVALID_INPUT, "empty mesh"};
+        return false;
+    }
+    if (n_nodes >= (int64_t(1) << 31) || n_elems * node_pairs(npe) >= (int64_t(1) << 31)) {
+        err = {MAILLE_INVALID_INPUT, "mesh too large for 32-bit element-pair indices"};
+        return false;
+    }
+    for (int64_t k = 0; k < n_elems * npe; ++k)
+        if (conn[k] < 0 || conn[k] >= n_nodes) {
+            err = {MAILLE_INVALID_INPUT, "element " + std::to_string(k / npe) +
+                                             " refers to unknown node " + std::to_string(conn[k])};
+            return false;
+        }
+    s = Symbolic{};
+    s.n_nodes = n_nodes;
+    s.n_elems = n_elems;
+    s.npe = npe;
+    const int32_t N = (int32_t)n_nodes;
+
+    // node -> (element, local) incidence, sorted by element
+    s.inc_ptr.assign(N + 1, 0);
+    for (int64_t k = 0; k < n_elems * npe; ++k) s.inc_ptr[conn[k] + 1]++;
+    for (int32_t v = 0; v < N; ++v) s.inc_ptr[v + 1] += s.inc_ptr[v];
+    s.inc.resize(n_elems * npe);
+    {
+        std::vector<int64_t> cur(s.inc_ptr.begin(), s.inc_ptr.end() - 1);
+        for (int64_t k = 0; k < n_elems * npe; ++k) s.inc[cur[conn[k]]++] = (int32_t)k;
+    }
+
+    // kept nodes (at least one free DOF) in original order; graph on them
+    std::vector<int32_t> kept_of(N, -1), kept;
+    for (int32_t v = 0; v < N; ++v) {
+        const bool all = fixed && fixed[3 * v] && fixed[3 * v + 1] && fixed[3 * v + 2];
+        if (!all) {
+            kept_of[v] = (int32_t)kept.size();
+            kept.push_back(v);
+        }
+    }
+    for (int64_t g = 0; g < 3 * n_nodes; ++g) s.free_dofs += (fixed && fixed[g]) ? 0 : 1;
+    const int32_t nk = (int32_t)kept.size();
+    if (nk == 0) {
+        err = {MAILLE_INVALID_INPUT, "every DOF is fixed"};
+        return false;
+    }
+    NodeGraph g;
+    g.off.assign(nk + 1, 0);
+    {
+        std::vector<int32_t> mark(nk, -1);
+        g.adj.reserve((size_t)nk * (npe == 4 ? 15 : 28));
+        for (int32_t k = 0; k < nk; ++k) {
+            const int32_t v = kept[k];
+            mark[k] = k;
+            for (int64_t q = s.inc_ptr[v]; q < s.inc_ptr[v + 1]; ++q) {
+                const int64_t e = s.inc[q] / npe;
+                for (int a = 0; a < npe; ++a) {
+                    const int32_t w = kept_of[conn[e * npe + a]];
+                    if (w >= 0 && mark[w] != k) {
+                        mark[w] = k;
+                        g.adj.push_back(w);
+                    }
+                }
+            }
+            g.off[k + 1] = (int64_t)g.adj.size();
+        }
+    }
+
+    // ordering over kept nodes: order[new] = kept index
+    std::vector<int32_t> order = rcm(g);
+    if (ordering != MAILLE_ORDER_RCM) {
+        std::vector<int32_t> colour = greedy_colour(g, order);
+        std::vector<int32_t> rank(nk);
+        for (int32_t r = 0; r < nk; ++r) rank[order[r]] = r;
+        std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+            return colour[a] != colour[b] ? colour[a] < colour[b] : rank[a] < rank[b];
+        });
+    }
+    // levels of the lower-triangular dependency graph in that order, then group rows by level
+    // (a topological renumbering leaves the IC(0) factor unchanged)
+    {
+        std::vector<int32_t> rank(nk), level(nk, 0);
+        for (int32_t r = 0; r < nk; ++r) rank[order[r]] = r;
+        int32_t maxl = 0;
+        for (int32_t r = 0; r < nk; ++r) {
+            const int32_t k = order[r];
+            int32_t l = 0;
+            for (int64_t p = g.off[k]; p < g.off[k + 1]; ++p)
+                if (rank[g.adj[p]] < r) l = std::max(l, level[g.adj[p]] + 1);
+            level[k] = l;
+            maxl = std::max(maxl, l);
+        }
+        s.levels = maxl + 1;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int32_t a, int32_t b) { return level[a] < level[b]; });
+        s.level_ptr.assign(s.levels + 1, 0);
+        for (int32_t k = 0; k < nk; ++k) s.level_ptr[level[k] + 1]++;
+        for (int32_t l = 0; l < s.levels; ++l) s.level_ptr[l + 1] += s.level_ptr[l];
+    }
+    s.nb = nk;
+    s.perm.resize(nk);
+    s.inv.assign(N, -1);
+    s.fixmask.assign(nk, 0);
+    for (int32_t r = 0; r < nk; ++r) {
+        const int32_t v = kept[order[r]];
+        s.perm[r] = v;
+        s.inv[v] = r;
+        uint8_t m = 0;
+        for (int c = 0; c < 3; ++c)
+            if (fixed && fixed[3 * v + c]) m |= (uint8_t)(1u << c);
+        s.fixmask[r] = m;
+    }
+
+    // full block pattern in new numbering (neighbours + the diagonal), columns ascending
+    s.row_ptr.assign(nk + 1, 0);
+    for (int32_t r = 0; r < nk; ++r) {
+        const int32_t k = kept_of[s.perm[r]];
+        s.row_ptr[r + 1] = s.row_ptr[r] + (g.off[k + 1] - g.off[k]) + 1;
+    }
+    s.blocks = s.row_ptr[nk];
+    s.col.resize(s.blocks);
+    s.diag.resize(nk);
+    for (int32_t r = 0; r < nk; ++r) {
+        const int32_t k = kept_of[s.perm[r]];
+        int64_t p = s.row_ptr[r];
+        s.col[p++] = r;
+        for (int64_t q = g.off[k]; q < g.off[k + 1]; ++q) s.col[p++] = s.inv[kept[g.adj[q]]];
+        std::sort(s.col.begin() + s.row_ptr[r], s.col.begin() + s.row_ptr[r + 1]);
+        s.diag[r] = std::lower_bound(s.col.begin() + s.row_ptr[r],
+                                     s.col.begin() + s.row_ptr[r + 1], r) -
+                    s.col.begin();
+    }
+    g = NodeGraph{};
+    auto find = [&](int32_t i, int32_t j) -> int64_t {
+        auto b = s.col.begin() + s.row_ptr[i], e = s.col.begin() + s.row_ptr[i + 1];
+        auto it = std::lower_bound(b, e, j);
+        return (it != e && *it == j) ? (int64_t)(it - s.col.begin()) : -1;
+    };
+    s.tpos.resize(s.blocks);
+    for (int32_t r = 0; r < nk; ++r)
+        for (int64_t p = s.row_ptr[r]; p < s.row_ptr[r + 1]; ++p) s.tpos[p] = find(s.col[p], r);
+
+    // lower slots and the scatter map (counting sort by slot, element order kept inside a slot)
+    std::vector<int64_t> lidx(s.blocks, -1);
+    for (int32_t r = 0; r < nk; ++r)
+        for (int64_t p = s.row_ptr[r]; p <= s.diag[r]; ++p) {
+            lidx[p] = (int64_t)s.lslot.size();
+            s.lslot.push_back(p);
+        }
+    const int64_t nl = (int64_t)s.lslot.size();
+    const int np = node_pairs(npe);
+    std::vector<int64_t> target((size_t)n_elems * np, -1);
+    s.lptr.assign(nl + 1, 0);
+    {
+        int pa[55], pb[55], q = 0;
+        for (int a = 0; a < npe; ++a)
+            for (int b = a; b < npe; ++b) {
+                pa[q] = a;
+                pb[q] = b;
+                ++q;
+            }
+        for (int64_t e = 0; e < n_elems; ++e)
+            for (int p = 0; p < np; ++p) {
+                const int32_t I = s.inv[conn[e * npe + pa[p]]];
+                const int32_t J = s.inv[conn[e * npe + pb[p]]];
+                if (I < 0 || J < 0) continue;
+                const bool tr = I < J;
+                const int64_t pos = tr ? find(J, I) : find(I, J);
+                const int64_t ls = lidx[pos];
+                target[(size_t)e * np + p] = tr ? ~ls : ls;
+                s.lptr[ls + 1]++;
+            }
+    }
+    for (int64_t l = 0; l < nl; ++l) s.lptr[l + 1] += s.lptr[l];
+    s.contrib.resize(s.lptr[nl]);
+    {
+        std::vector<int64_t> cur(s.lptr.begin(), s.lptr.end() - 1);
+        for (int64_t k = 0; k < n_elems * np; ++k) {
+            const int64_t t = target[k];
+            if (t == -1) continue;
+            const bool tr = t < 0;
+            const int64_t ls = tr ? ~t : t;
+            s.contrib[cur[ls]++] = (uint32_t)k | (tr ? 0x80000000u : 0u);
+        }
+    }
+
+    // elements touching a fixed DOF, and the nodes with a fixed DOF they contain
+    if (fixed) {
+        std::vector<uint8_t> bn(N, 0);
+        for (int64_t e = 0; e < n_elems; ++e) {
+            bool any = false;
+            for (int a = 0; a < npe && !any; ++a) {
+                const int64_t v = conn[e * npe + a];
+                any = fixed[3 * v] || fixed[3 * v + 1] || fixed[3 * v + 2];
+            }
+            if (any) {
+                s.belem.push_back((int32_t)e);
+                for (int a = 0; a < npe; ++a) bn[conn[e * npe + a]] = 1;
+            }
+        }
+        for (int32_t v = 0; v < N; ++v)
+            if (bn[v]) s.bnodes.push_back(v);
+    }
+    s.ms = now_ms() - t0;
+    return true;
+}
+
+// face_pressure for the tet faces (assembly.rs:650-674; face_rule tet branch 556-585; face nodes
+// from Element::face_positions, mesh.rs:184-198; TRIANGLE_3 / TRIANGLE_6 rules).
+bool face_pressure_loads(int64_t n_nodes, const double* coords, int npe, int64_t n_elems,
+                         const int64_t* conn, int64_t n_press, const int64_t* p_elem,
+                         const int32_t* p_face, const double* p_value, double* f, Error& err) {
+    static const int faces[4][3] = {{0, 1, 2}, {0, 3, 1}, {1, 3, 2}, {2, 3, 0}};
+    static const int edges[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+    static const double t3[3][3] = {{1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0},
+                                    {2.0 / 3.0, 1.0 / 6.0, 1.0 / 6.0},
+                                    {1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0}};
+    const double A = 0.445948490915965, WA = 0.223381589678011 / 2.0;
+    const double B = 0.091576213509771, WB = 0.109951743655322 / 2.0;
+    const double t6[6][3] = {{A, A, WA}, {1.0 - 2.0 * A, A, WA}, {A, 1.0 - 2.0 * A, WA},
+                             {B, B, WB}, {1.0 - 2.0 * B, B, WB}, {B, 1.0 - 2.0 * B, WB}};
+    if (npe != 4 && npe != 10) {
+        err = {MAILLE_INVALID_INPUT, "nodes_per_elem must be 4 or 10"};
+        return false;
+    }
+    for (int64_t k = 0; k < n_press; ++k) {
+        const int64_t e = p_elem[k];
+        const int face = p_face[k];
+        if (e < 0 || e >= n_elems || face < 0 || face > 3) continue;  // face_rule gives None
+        int pos[6];
+        const int nn = npe == 4 ? 3 : 6;
+        for (int q = 0; q < 3; ++q) pos[q] = faces[face][q];
+        if (npe == 10) {
+            auto mid = [&](int a, int b) {
+                for (int q = 0; q < 6; ++q)
+                    if ((edges[q][0] == a && edges[q][1] == b) || (edges[q][0] == b && edges[q][1] == a))
+                        return 4 + q;
+                return 4;
+            };
+            pos[3] = mid(pos[0], pos[1]);
+            pos[4] = mid(pos[1], pos[2]);
+            pos[5] = mid(pos[2], pos[0]);
+        }
+        double c[6][3], corner[4][3];
+        for (int q = 0; q < nn; ++q) {
+            const int64_t v = conn[e * npe + pos[q]];
+            if (v < 0 || v >= n_nodes) {
+                err = {MAILLE_INVALID_INPUT, "pressure face refers to an unknown node"};
+                return false;
+            }
+            for (int d = 0; d < 3; ++d) c[q][d] = coords[3 * v + d];
+        }
+        for (int q = 0; q < 4; ++q)
+            for (int d = 0; d < 3; ++d) corner[q][d] = coords[3 * conn[e * npe + q] + d];
+        double u[3], w[3];
+        for (int d = 0; d < 3; ++d) {
+            u[d] = c[1][d] - c[0][d];
+            w[d] = c[2][d] - c[0][d];
+        }
+        const double cross[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2],
+                                 u[0] * w[1] - u[1] * w[0]};
+        const double twice_area =
+            std::sqrt(cross[0] * cross[0] + cross[1] * cross[1] + cross[2] * cross[2]);
+        double dot = 0.0;
+        for (int d = 0; d < 3; ++d) {
+            const double out = (c[0][d] + c[1][d] + c[2][d]) / 3.0 -
+                               (corner[0][d] + corner[1][d] + corner[2][d] + corner[3][d]) / 4.0;
+            dot += cross[d] * out;
+        }
+        const double sign = dot < 0.0 ? -1.0 : 1.0;
+        double normal[3];
+        for (int d = 0; d < 3; ++d) normal[d] = sign * cross[d] / twice_area;
+        const int ng = nn == 3 ? 3 : 6;
+        double forces[18] = {0};
+        for (int gp = 0; gp < ng; ++gp) {
+            const double xi = nn == 3 ? t3[gp][0] : t6[gp][0];
+            const double eta = nn == 3 ? t3[gp][1] : t6[gp][1];
+            const double wt = (nn == 3 ? t3[gp][2] : t6[gp][2]) * twice_area;
+            double nv[6];
+            const double l1 = 1.0 - xi - eta, l2 = xi, l3 = eta;
+            if (nn == 3) {
+                nv[0] = l1;
+                nv[1] = l2;
+                nv[2] = l3;
+            } else {
+                nv[0] = l1 * (2.0 * l1 - 1.0);
+                nv[1] = l2 * (2.0 * l2 - 1.0);
+                nv[2] = l3 * (2.0 * l3 - 1.0);
+                nv[3] = 4.0 * l1 * l2;
+                nv[4] = 4.0 * l2 * l3;
+                nv[5] = 4.0 * l3 * l1;
+            }
+            for (int a = 0; a < nn; ++a)
+                for (int d = 0; d < 3; ++d) forces[3 * a + d] -= p_value[k] * wt * nv[a] * normal[d];
+        }
+        for (int a = 0; a < nn; ++a)
+            for (int d = 0; d < 3; ++d) f[3 * conn[e * npe + pos[a]] + d] += forces[3 * a + d];
+    }
+    return true;
+}
+
+}  // namespace maille

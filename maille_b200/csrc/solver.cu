@@ -1,0 +1,765 @@
+// solver.cu -- handle lifecycle, PCG driver (plain FP64 and mixed FP32/FP64 refinement) and the
+// C ABI of include/maille_gpu.h.
+//
+// create = FreeSystem::new + Pcg::new (model.rs:1442-1499, iterative.rs:201-207) on the GPU:
+//   symbolic analysis (host, setup.cpp) -> upload -> element integration -> scatter-reduce
+//   assembly -> level-scheduled block IC(0) with the reference's diagonal-shift ladder.
+// solve  = FreeSystem::solve + Pcg::solve (model.rs:1502-1516, iterative.rs:210-248), then the
+//   reactions (product, model.rs:586-593) and Gauss-point stresses (model.rs:596-598).
+// The PCG iteration is a fixed kernel sequence (SpMV, forward levels, backward levels, p update)
+// captured once into a CUDA graph of several iterations; kernels skip their work once the
+// on-device `done` flag is set, and the host reads the device scalars after each graph launch.
+
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "common.hpp"
+#include "kernels.cuh"
+
+using namespace maille;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+struct CudaFailure {
+    std::string what;
+};
+
+#define CK(call)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            throw CudaFailure{std::string(#call) + ": " + cudaGetErrorString(e_)};           \
+    } while (0)
+
+template <typename T>
+T* dalloc(size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    CK(cudaMalloc(&p, n * sizeof(T)));
+    return static_cast<T*>(p);
+}
+
+template <typename T>
+T* dupload(const T* src, size_t n, cudaStream_t st) {
+    T* d = dalloc<T>(n);
+    if (n && src) CK(cudaMemcpyAsync(d, src, n * sizeof(T), cudaMemcpyHostToDevice, st));
+    return d;
+}
+
+// Vectors of one PCG precision.
+template <typename T>
+struct PcgVecs {
+    T *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr;
+};
+
+constexpr double kDefaultTol = 1e-12;      // iterative.rs:9
+constexpr int32_t kDefaultMaxIter = 10000;  // iterative.rs:11
+const double kShifts[6] = {0.0, 1e-3, 1e-2, 1e-1, 1.0, 10.0};  // iterative.rs:14
+
+}  // namespace
+
+struct MailleGpuHandle {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[8] = {};
+    Symbolic sym;
+    int npe = 0;
+    int64_t n_nodes = 0, n_elems = 0;
+    int precision = MAILLE_FP64;
+    double tol = kDefaultTol;
+    int32_t max_iter = kDefaultMaxIter;
+    double inner_tol = 1e-4;
+    int32_t max_outer = 60;
+    std::vector<uint8_t> h_fixed;
+    std::vector<double> h_f, h_imposed;
+    bool any_imposed = false;
+    // device: inputs (caller numbering)
+    double *coords = nullptr, *young = nullptr, *poisson = nullptr, *imposed = nullptr, *f = nullptr;
+    int32_t* conn = nullptr;
+    uint8_t* fixed = nullptr;
+    // device: symbolic
+    int32_t *perm = nullptr, *inv = nullptr, *col = nullptr, *lrow = nullptr;
+    uint8_t* fixmask = nullptr;
+    int64_t *row_ptr = nullptr, *diag = nullptr, *tpos = nullptr, *lslot = nullptr, *lptr = nullptr;
+    uint32_t* contrib = nullptr;
+    int64_t* inc_ptr = nullptr;
+    int32_t *inc = nullptr, *belem = nullptr, *bnodes = nullptr, *elem_slot = nullptr;
+    // device: numeric
+    double* ke = nullptr;
+    double *K = nullptr, *F = nullptr;
+    float *K32 = nullptr, *F32 = nullptr;
+    PcgVecs<double> v64;
+    PcgVecs<float> v32;
+    double *rr64 = nullptr;  // outer residual (mixed)
+    double *u_full = nullptr, *y_full = nullptr, *ye = nullptr, *gauss = nullptr, *vm = nullptr,
+           *react = nullptr, *lambda_full = nullptr, *grad = nullptr;
+    PcgScalars* scal = nullptr;
+    PcgScalars* h_scal = nullptr;  // pinned
+    double* partials = nullptr;
+    double* lvl_total = nullptr;
+    double* dsum = nullptr;        // [4] misc sums
+    double* h_sum = nullptr;       // pinned [4]
+    unsigned int* dticket = nullptr;
+    int32_t* dfail = nullptr;
+    int spmv_grid = 1;
+    std::vector<int> lvl_grid;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [0] FP64, [1] FP32
+    int graph_iters = 8;
+    std::atomic<int> cancel{0};
+    double shift = 0.0;
+    bool solved = false;
+    Pattern pattern() const {
+        return Pattern{sym.nb, row_ptr, col, diag, tpos, fixmask};
+    }
+    ~MailleGpuHandle();
+};
+
+namespace {
+
+void dfree(void* p) {
+    if (p) cudaFree(p);
+}
+
+}  // namespace
+
+MailleGpuHandle::~MailleGpuHandle() {
+    cudaSetDevice(device);
+    for (auto& g : graph)
+        if (g) cudaGraphExecDestroy(g);
+    void* bufs[] = {coords, young, poisson, imposed, f, conn, fixed, perm, inv, col, lrow, fixmask,
+                    row_ptr, diag, tpos, lslot, lptr, contrib, inc_ptr, inc, belem, bnodes,
+                    elem_slot, ke, K, F, K32, F32, v64.b, v64.x, v64.r, v64.z, v64.p, v64.ap,
+                    v32.b, v32.x, v32.r, v32.z, v32.p, v32.ap, rr64, u_full, y_full, ye, gauss, vm,
+                    react, lambda_full, grad, scal, partials, lvl_total, dsum, dticket, dfail};
+    for (void* p : bufs) dfree(p);
+    if (h_scal) cudaFreeHost(h_scal);
+    if (h_sum) cudaFreeHost(h_sum);
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+}
+
+namespace {
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+int grid_for_rows(int64_t rows) {
+    int64_t g = (rows + kWarps - 1) / kWarps;
+    if (g > 148 * 8) g = 148 * 8;
+    return (int)(g < 1 ? 1 : g);
+}
+
+// Kernel sequence of one PCG iteration (type T) on the handle's stream.
+template <typename T>
+void enqueue_iteration(MailleGpuHandle* h, const T* K, const T* F, PcgVecs<T>& v) {
+    const Pattern pt = h->pattern();
+    const int L = h->sym.levels;
+    launch_spmv_pcg<T>(pt, K, v.p, v.ap, h->scal, h->partials, h->spmv_grid, h->st);
+    for (int l = 0; l < L; ++l)
+        launch_fwd<T>(pt, h->sym.level_ptr[l], h->sym.level_ptr[l + 1], l, L, F, v.r, v.z, v.x,
+                      v.p, v.ap, h->scal, h->partials, h->lvl_total, h->lvl_grid[l], h->st);
+    for (int l = L - 1; l >= 0; --l)
+        launch_bwd<T>(pt, h->sym.level_ptr[l], h->sym.level_ptr[l + 1], l, F, v.r, v.z, h->scal,
+                      h->partials, h->lvl_total + kMaxLevels, L, h->lvl_grid[l], h->st);
+    launch_pupdate<T>(3 * (int64_t)h->sym.nb, v.z, v.p, h->scal, h->st);
+}
+
+template <typename T>
+void norm2_of(MailleGpuHandle* h, const T* v, int64_t n, double* out);
+
+template <>
+void norm2_of<double>(MailleGpuHandle* h, const double* v, int64_t n, double* out) {
+    launch_norm2(n, v, h->partials, h->dticket, out, 148 * 4, h->st);
+}
+
+}  // namespace
+
+namespace {
+
+template <>
+void norm2_of<float>(MailleGpuHandle* h, const float* v, int64_t n, double* out) {
+    launch_norm2_f(n, v, h->partials, h->dticket, out, 148 * 4, h->st);
+}
+
+// PCG on K x = b with the IC(0) factor F (both of type T): x, r, z, p, ap of `v`.
+// Returns the MailleStatus and the iteration count.
+template <typename T>
+int32_t run_pcg(MailleGpuHandle* h, const T* K, const T* F, PcgVecs<T>& v, double tol,
+                int32_t max_iter, int32_t* iterations, double* rel_res) {
+    const int64_t n = 3 * (int64_t)h->sym.nb;
+    const int L = h->sym.levels;
+    const Pattern pt = h->pattern();
+    CK(cudaMemsetAsync(v.x, 0, n * sizeof(T), h->st));
+    CK(cudaMemsetAsync(v.p, 0, n * sizeof(T), h->st));
+    CK(cudaMemsetAsync(v.ap, 0, n * sizeof(T), h->st));
+    CK(cudaMemcpyAsync(v.r, v.b, n * sizeof(T), cudaMemcpyDeviceToDevice, h->st));
+    norm2_of<T>(h, v.b, n, &h->scal->bb);
+    launch_pcg_init(h->scal, tol, max_iter, h->st);
+    // z = M^-1 b, rz = b.z, p = z (iterative.rs:217-220): the sweeps with alpha = 0
+    for (int l = 0; l < L; ++l)
+        launch_fwd<T>(pt, h->sym.level_ptr[l], h->sym.level_ptr[l + 1], l, L, F, v.r, v.z, v.x,
+                      v.p, v.ap, h->scal, h->partials, h->lvl_total, h->lvl_grid[l], h->st);
+    for (int l = L - 1; l >= 0; --l)
+        launch_bwd<T>(pt, h->sym.level_ptr[l], h->sym.level_ptr[l + 1], l, F, v.r, v.z, h->scal,
+                      h->partials, h->lvl_total + kMaxLevels, L, h->lvl_grid[l], h->st);
+    launch_pupdate<T>(n, v.z, v.p, h->scal, h->st);
+    CK(cudaGetLastError());
+
+    const int gi = std::is_same<T, double>::value ? 0 : 1;
+    // the graph bakes in the vector and matrix pointers of this precision
+    if (!h->graph[gi]) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < h->graph_iters; ++k) enqueue_iteration<T>(h, K, F, v);
+        CK(cudaStreamEndCapture(h->st, &g));
+        CK(cudaGraphInstantiate(&h->graph[gi], g, 0));
+        cudaGraphDestroy(g);
+    }
+    int32_t status = MAILLE_OK;
+    for (;;) {
+        CK(cudaGraphLaunch(h->graph[gi], h->st));
+        CK(cudaMemcpyAsync(h->h_scal, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        const PcgScalars& s = *h->h_scal;
+        if (s.done) {
+            status = s.status == 1 ? MAILLE_SINGULAR : (s.status == 2 ? MAILLE_NOT_CONVERGED : MAILLE_OK);
+            break;
+        }
+        if (h->cancel.load()) {
+            status = MAILLE_CANCELLED;
+            break;
+        }
+        if (s.iter >= max_iter) {
+            status = MAILLE_NOT_CONVERGED;
+            break;
+        }
+    }
+    const PcgScalars& s = *h->h_scal;
+    *iterations = s.iter;
+    *rel_res = s.bb > 0 ? std::sqrt(s.rr / s.bb) : 0.0;
+    return status;
+}
+
+void set_error(const std::string& m) { g_last_error = m; }
+
+int32_t fail(const Error& e) {
+    set_error(e.message);
+    return e.status;
+}
+
+bool check_problem(const MailleElasticProblem* p, Error& err) {
+    if (!p) {
+        err = {MAILLE_INVALID_INPUT, "null problem"};
+        return false;
+    }
+    if (!p->coords || !p->conn || !p->young || !p->poisson) {
+        err = {MAILLE_INVALID_INPUT, "coords, conn, young and poisson are required"};
+        return false;
+    }
+    for (int64_t k = 0; k < 3 * p->n_nodes; ++k)
+        if (!std::isfinite(p->coords[k])) {
+            err = {MAILLE_INVALID_INPUT, "non-finite coordinate at node " + std::to_string(k / 3)};
+            return false;
+        }
+    for (int64_t e = 0; e < p->n_elems; ++e)
+        if (!std::isfinite(p->young[e]) || !std::isfinite(p->poisson[e]) || p->young[e] <= 0.0 ||
+            p->poisson[e] <= -1.0 || p->poisson[e] >= 0.5) {
+            err = {MAILLE_INVALID_INPUT, "invalid material of element " + std::to_string(e)};
+            return false;
+        }
+    if (p->f)
+        for (int64_t k = 0; k < 3 * p->n_nodes; ++k)
+            if (!std::isfinite(p->f[k])) {
+                err = {MAILLE_INVALID_INPUT, "non-finite load at DOF " + std::to_string(k)};
+                return false;
+            }
+    if (p->imposed && p->fixed)
+        for (int64_t k = 0; k < 3 * p->n_nodes; ++k)
+            if (p->fixed[k] && !std::isfinite(p->imposed[k])) {
+                err = {MAILLE_INVALID_INPUT, "non-finite imposed value at DOF " + std::to_string(k)};
+                return false;
+            }
+    return true;
+}
+
+// Builds b (solver numbering) from the load vector on the device (h->f) and K_fc u_c.
+void build_rhs(MailleGpuHandle* h) {
+    const double* coupling = nullptr;
+    if (h->any_imposed) {
+        // u_c: imposed values at fixed DOFs, 0 elsewhere; coupling = K u_c on boundary nodes
+        CK(cudaMemsetAsync(h->y_full, 0, 3 * h->n_nodes * sizeof(double), h->st));
+        launch_elem_apply(h->npe, (int64_t)h->sym.belem.size(), h->belem, h->conn, h->ke,
+                          h->imposed, h->ye, h->st);
+        launch_node_gather(h->npe, (int64_t)h->sym.bnodes.size(), h->bnodes, h->inc_ptr, h->inc,
+                           h->elem_slot, h->ye, h->y_full, h->st);
+        coupling = h->y_full;
+    }
+    launch_build_rhs(h->sym.nb, h->perm, h->fixmask, h->f, coupling, h->v64.b, h->st);
+}
+
+int32_t factorize(MailleGpuHandle* h, Error& err) {
+    const Pattern pt = h->pattern();
+    for (double shift : kShifts) {
+        CK(cudaMemsetAsync(h->dfail, 0, sizeof(int32_t), h->st));
+        for (int l = 0; l < h->sym.levels; ++l)
+            launch_factor_level(pt, h->sym.level_ptr[l], h->sym.level_ptr[l + 1], h->K, h->F, shift,
+                                h->dfail, h->st);
+        CK(cudaGetLastError());
+        int32_t failed = 0;
+        CK(cudaMemcpyAsync(&failed, h->dfail, sizeof(int32_t), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        if (!failed) {
+            h->shift = shift;
+            return MAILLE_OK;
+        }
+    }
+    err = {MAILLE_SINGULAR, "IC(0) failed with every diagonal shift (Singular)"};
+    return MAILLE_SINGULAR;
+}
+
+int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, MailleElasticResult* res) {
+    Error err{MAILLE_OK, ""};
+    if (!out) return fail({MAILLE_INVALID_INPUT, "null handle pointer"});
+    *out = nullptr;
+    if (!check_problem(p, err)) return fail(err);
+    auto h = std::make_unique<MailleGpuHandle>();
+    h->device = p->device;
+    h->npe = p->nodes_per_elem;
+    h->n_nodes = p->n_nodes;
+    h->n_elems = p->n_elems;
+    h->precision = p->precision;
+    h->tol = p->rel_tol > 0 ? p->rel_tol : kDefaultTol;
+    h->max_iter = p->max_iter > 0 ? p->max_iter : kDefaultMaxIter;
+    if (const char* e = std::getenv("MAILLE_INNER_TOL")) h->inner_tol = std::atof(e);
+    if (const char* e = std::getenv("MAILLE_GRAPH_ITERS")) h->graph_iters = std::max(1, std::atoi(e));
+    const int64_t n3 = 3 * p->n_nodes;
+    h->h_fixed.assign(n3, 0);
+    if (p->fixed)
+        for (int64_t k = 0; k < n3; ++k) h->h_fixed[k] = p->fixed[k] ? 1 : 0;
+    h->h_imposed.assign(n3, 0.0);
+    if (p->imposed)
+        for (int64_t k = 0; k < n3; ++k)
+            if (h->h_fixed[k]) {
+                h->h_imposed[k] = p->imposed[k];
+                if (p->imposed[k] != 0.0) h->any_imposed = true;
+            }
+    h->h_f.assign(n3, 0.0);
+    if (p->f) std::memcpy(h->h_f.data(), p->f, n3 * sizeof(double));
+
+    const double t_setup0 = now_ms();
+    if (!analyse(p->n_nodes, p->nodes_per_elem, p->n_elems, p->conn, h->h_fixed.data(), p->ordering,
+                 h->sym, err))
+        return fail(err);
+    if (h->sym.levels >= kMaxLevels) return fail({MAILLE_INVALID_INPUT, "too many IC(0) levels"});
+    const double t_setup1 = now_ms();
+    try {
+        int ndev = 0;
+        CK(cudaGetDeviceCount(&ndev));
+        if (p->device < 0 || p->device >= ndev)
+            return fail({MAILLE_CUDA_ERROR, "no CUDA device " + std::to_string(p->device)});
+        CK(cudaSetDevice(p->device));
+        CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+        for (auto& e : h->ev) CK(cudaEventCreate(&e));
+        cudaStream_t st = h->st;
+        const Symbolic& s = h->sym;
+        CK(cudaEventRecord(h->ev[0], st));
+        // inputs
+        std::vector<int32_t> conn32(p->n_elems * p->nodes_per_elem);
+        for (size_t k = 0; k < conn32.size(); ++k) conn32[k] = (int32_t)p->conn[k];
+        h->coords = dupload(p->coords, n3, st);
+        h->conn = dupload(conn32.data(), conn32.size(), st);
+        h->young = dupload(p->young, p->n_elems, st);
+        h->poisson = dupload(p->poisson, p->n_elems, st);
+        h->imposed = dupload(h->h_imposed.data(), n3, st);
+        h->f = dupload(h->h_f.data(), n3, st);
+        h->fixed = dupload(h->h_fixed.data(), n3, st);
+        // symbolic
+        h->perm = dupload(s.perm.data(), s.perm.size(), st);
+        h->inv = dupload(s.inv.data(), s.inv.size(), st);
+        h->fixmask = dupload(s.fixmask.data(), s.fixmask.size(), st);
+        h->row_ptr = dupload(s.row_ptr.data(), s.row_ptr.size(), st);
+        h->col = dupload(s.col.data(), s.col.size(), st);
+        h->diag = dupload(s.diag.data(), s.diag.size(), st);
+        h->tpos = dupload(s.tpos.data(), s.tpos.size(), st);
+        std::vector<int32_t> lrow(s.lslot.size());
+        {
+            size_t q = 0;
+            for (int32_t r = 0; r < s.nb; ++r)
+                for (int64_t pp = s.row_ptr[r]; pp <= s.diag[r]; ++pp) lrow[q++] = r;
+        }
+        h->lslot = dupload(s.lslot.data(), s.lslot.size(), st);
+        h->lrow = dupload(lrow.data(), lrow.size(), st);
+        h->lptr = dupload(s.lptr.data(), s.lptr.size(), st);
+        h->contrib = dupload(s.contrib.data(), s.contrib.size(), st);
+        h->inc_ptr = dupload(s.inc_ptr.data(), s.inc_ptr.size(), st);
+        h->inc = dupload(s.inc.data(), s.inc.size(), st);
+        h->belem = dupload(s.belem.data(), s.belem.size(), st);
+        h->bnodes = dupload(s.bnodes.data(), s.bnodes.size(), st);
+        std::vector<int32_t> slot(p->n_elems, -1);
+        for (size_t k = 0; k < s.belem.size(); ++k) slot[s.belem[k]] = (int32_t)k;
+        h->elem_slot = dupload(slot.data(), slot.size(), st);
+        // numeric buffers
+        const int np = node_pairs(h->npe);
+        const int64_t n = 3 * (int64_t)s.nb;
+        h->ke = dalloc<double>((size_t)p->n_elems * np * 9);
+        h->K = dalloc<double>((size_t)s.blocks * 9);
+        h->F = dalloc<double>((size_t)s.blocks * 9);
+        for (double** q : {&h->v64.b, &h->v64.x, &h->v64.r, &h->v64.z, &h->v64.p, &h->v64.ap})
+            *q = dalloc<double>(n);
+        if (h->precision == MAILLE_MIXED) {
+            h->K32 = dalloc<float>((size_t)s.blocks * 9);
+            h->F32 = dalloc<float>((size_t)s.blocks * 9);
+            for (float** q : {&h->v32.b, &h->v32.x, &h->v32.r, &h->v32.z, &h->v32.p, &h->v32.ap})
+                *q = dalloc<float>(n);
+            h->rr64 = dalloc<double>(n);
+        }
+        h->u_full = dalloc<double>(n3);
+        h->y_full = dalloc<double>(n3);
+        h->react = dalloc<double>(n3);
+        h->ye = dalloc<double>(std::max<size_t>(1, s.belem.size()) * 3 * h->npe);
+        h->scal = dalloc<PcgScalars>(1);
+        CK(cudaMemsetAsync(h->scal, 0, sizeof(PcgScalars), st));
+        CK(cudaMallocHost(&h->h_scal, sizeof(PcgScalars)));
+        CK(cudaMallocHost(&h->h_sum, 4 * sizeof(double)));
+        h->partials = dalloc<double>(148 * 16);
+        h->lvl_total = dalloc<double>(2 * kMaxLevels);
+        h->dsum = dalloc<double>(4);
+        h->dticket = dalloc<unsigned int>(1);
+        CK(cudaMemsetAsync(h->dticket, 0, sizeof(unsigned int), st));
+        h->dfail = dalloc<int32_t>(1);
+        h->spmv_grid = grid_for_rows(s.nb);
+        h->lvl_grid.resize(s.levels);
+        for (int l = 0; l < s.levels; ++l)
+            h->lvl_grid[l] = grid_for_rows(s.level_ptr[l + 1] - s.level_ptr[l]);
+        // graph size: keep a few thousand kernel nodes at most
+        const int per_iter = 2 * s.levels + 2;
+        h->graph_iters = std::max(1, std::min(h->graph_iters, 4000 / per_iter));
+        CK(cudaEventRecord(h->ev[1], st));
+        // element integration + assembly
+        ElemIn in{p->n_elems, h->coords, h->conn, h->young, h->poisson};
+        launch_elem_stiffness(h->npe, in, h->ke, st);
+        launch_assemble(h->pattern(), (int64_t)s.lslot.size(), h->lslot, h->lrow, h->lptr,
+                        h->contrib, h->ke, h->K, st);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(h->ev[2], st));
+        if (factorize(h.get(), err) != MAILLE_OK) return fail(err);
+        if (h->precision == MAILLE_MIXED) {
+            launch_to_float((int64_t)s.blocks * 9, h->K, h->K32, st);
+            launch_to_float((int64_t)s.blocks * 9, h->F, h->F32, st);
+            CK(cudaGetLastError());
+        }
+        CK(cudaEventRecord(h->ev[3], st));
+        CK(cudaStreamSynchronize(st));
+        if (res) {
+            res->ms_setup = t_setup1 - t_setup0;
+            res->ms_upload = elapsed(h->ev[0], h->ev[1]);
+            res->ms_assembly = elapsed(h->ev[1], h->ev[2]);
+            res->ms_factor = elapsed(h->ev[2], h->ev[3]);
+        }
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+    *out = h.release();
+    return MAILLE_OK;
+}
+
+int32_t solve_impl(MailleGpuHandle* h, const double* f, MailleElasticResult* res) {
+    if (!h) return fail({MAILLE_INVALID_INPUT, "null handle"});
+    try {
+        CK(cudaSetDevice(h->device));
+        cudaStream_t st = h->st;
+        const Symbolic& s = h->sym;
+        const int64_t n3 = 3 * h->n_nodes;
+        const int64_t n = 3 * (int64_t)s.nb;
+        const double t0 = now_ms();
+        if (f) {
+            for (int64_t k = 0; k < n3; ++k)
+                if (!std::isfinite(f[k])) return fail({MAILLE_INVALID_INPUT, "non-finite load"});
+            std::memcpy(h->h_f.data(), f, n3 * sizeof(double));
+            CK(cudaMemcpyAsync(h->f, f, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+        CK(cudaEventRecord(h->ev[4], st));
+        build_rhs(h);
+        int32_t status = MAILLE_OK, iters = 0, outer = 1;
+        double rel = 0.0;
+        if (h->precision == MAILLE_MIXED) {
+            // FP64 iterative refinement around an FP32 IC(0)-PCG
+            norm2_of<double>(h, h->v64.b, n, h->dsum + 1);
+            CK(cudaMemsetAsync(h->v64.x, 0, n * sizeof(double), st));
+            CK(cudaMemcpyAsync(h->h_sum + 1, h->dsum + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            const double bb = h->h_sum[1];
+            outer = 0;
+            if (bb > 0.0) {
+                for (;;) {
+                    launch_residual64(h->pattern(), h->K, h->v64.b, h->v64.x, h->rr64, h->partials,
+                                      h->dticket, h->dsum, h->spmv_grid, st);
+                    CK(cudaMemcpyAsync(h->h_sum, h->dsum, sizeof(double), cudaMemcpyDeviceToHost, st));
+                    CK(cudaStreamSynchronize(st));
+                    rel = std::sqrt(h->h_sum[0] / bb);
+                    if (!(rel == rel)) {
+                        status = MAILLE_SINGULAR;
+                        break;
+                    }
+                    if (std::sqrt(h->h_sum[0]) <= h->tol * std::sqrt(bb)) break;
+                    if (outer >= h->max_outer || iters >= h->max_iter) {
+                        status = MAILLE_NOT_CONVERGED;
+                        break;
+                    }
+                    launch_scale_to_float(n, h->rr64, h->dsum, h->v32.b, st);
+                    int32_t it = 0;
+                    double inner_rel = 0.0;
+                    const int32_t st_in = run_pcg<float>(h, h->K32, h->F32, h->v32, h->inner_tol,
+                                                         h->max_iter - iters, &it, &inner_rel);
+                    iters += it;
+                    ++outer;
+                    if (st_in == MAILLE_SINGULAR || st_in == MAILLE_CANCELLED) {
+                        status = st_in;
+                        break;
+                    }
+                    launch_accumulate(n, h->v32.x, h->dsum, h->v64.x, st);
+                }
+            }
+        } else {
+            status = run_pcg<double>(h, h->K, h->F, h->v64, h->tol, h->max_iter, &iters, &rel);
+        }
+        CK(cudaEventRecord(h->ev[5], st));
+        if (res) {
+            res->iterations = iters;
+            res->outer_iterations = outer;
+            res->final_rel_residual = rel;
+            res->shift = h->shift;
+            res->free_dofs = s.free_dofs;
+            res->block_rows = s.nb;
+            res->blocks = s.blocks;
+            res->levels = s.levels;
+        }
+        if (status != MAILLE_OK) {
+            CK(cudaStreamSynchronize(st));
+            if (status == MAILLE_SINGULAR) set_error("Singular: IC(0)-PCG met p.Ap <= 0 or NaN");
+            else if (status == MAILLE_NOT_CONVERGED)
+                set_error("IterativeNotConverged: iterations " + std::to_string(iters) +
+                          ", relative residual " + std::to_string(rel));
+            else if (status == MAILLE_CANCELLED) set_error("Cancelled");
+            return status;
+        }
+        // u in caller numbering, reactions, stresses
+        launch_gather_u(h->n_nodes, h->inv, h->fixed, h->imposed, h->v64.x, h->u_full, st);
+        CK(cudaMemsetAsync(h->react, 0, n3 * sizeof(double), st));
+        if (!s.belem.empty()) {
+            CK(cudaMemsetAsync(h->y_full, 0, n3 * sizeof(double), st));
+            launch_elem_apply(h->npe, (int64_t)s.belem.size(), h->belem, h->conn, h->ke, h->u_full,
+                              h->ye, st);
+            launch_node_gather(h->npe, (int64_t)s.bnodes.size(), h->bnodes, h->inc_ptr, h->inc,
+                               h->elem_slot, h->ye, h->y_full, st);
+            launch_reactions(h->n_nodes, h->bnodes, (int64_t)s.bnodes.size(), h->fixed, h->y_full,
+                             h->f, h->react, st);
+        }
+        const int ng = gauss_points(h->npe);
+        if (!h->gauss) {
+            h->gauss = dalloc<double>((size_t)h->n_elems * ng * 9);
+            h->vm = dalloc<double>((size_t)h->n_elems * ng);
+        }
+        ElemIn in{h->n_elems, h->coords, h->conn, h->young, h->poisson};
+        launch_stresses(h->npe, in, h->u_full, h->gauss, h->vm, st);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(h->ev[6], st));
+        if (res) {
+            if (res->u) CK(cudaMemcpyAsync(res->u, h->u_full, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+            if (res->reactions)
+                CK(cudaMemcpyAsync(res->reactions, h->react, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+            if (res->gauss_stress)
+                CK(cudaMemcpyAsync(res->gauss_stress, h->gauss, (size_t)h->n_elems * ng * 9 * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st));
+            if (res->von_mises)
+                CK(cudaMemcpyAsync(res->von_mises, h->vm, (size_t)h->n_elems * ng * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st));
+        }
+        CK(cudaEventRecord(h->ev[7], st));
+        CK(cudaStreamSynchronize(st));
+        if (res) {
+            res->ms_solve = elapsed(h->ev[4], h->ev[5]);
+            res->ms_post = elapsed(h->ev[5], h->ev[6]);
+            res->ms_download = elapsed(h->ev[6], h->ev[7]);
+            // a fixed DOF that no element touches: K u = 0 there (product skips it)
+            if (res->reactions && s.belem.size() < (size_t)h->n_elems) {
+                for (int64_t v = 0; v < h->n_nodes; ++v)
+                    if (s.inc_ptr[v] == s.inc_ptr[v + 1])
+                        for (int c = 0; c < 3; ++c)
+                            if (h->h_fixed[3 * v + c]) res->reactions[3 * v + c] = -h->h_f[3 * v + c];
+            }
+        }
+        (void)t0;
+        h->solved = true;
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+    return MAILLE_OK;
+}
+
+int32_t backward_impl(MailleGpuHandle* h, const double* dJdu, double* dJdE, double* lambda) {
+    if (!h || !dJdu || !dJdE) return fail({MAILLE_INVALID_INPUT, "null argument"});
+    if (!h->solved) return fail({MAILLE_INVALID_INPUT, "backward needs a solve first"});
+    try {
+        CK(cudaSetDevice(h->device));
+        cudaStream_t st = h->st;
+        const Symbolic& s = h->sym;
+        const int64_t n3 = 3 * h->n_nodes;
+        const int64_t n = 3 * (int64_t)s.nb;
+        for (int64_t k = 0; k < n3; ++k)
+            if (!std::isfinite(dJdu[k])) return fail({MAILLE_INVALID_INPUT, "non-finite dJ/du"});
+        // adjoint right-hand side: g at free DOFs (no coupling term: lambda_c = 0)
+        CK(cudaMemcpyAsync(h->y_full, dJdu, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+        launch_build_rhs(s.nb, h->perm, h->fixmask, h->y_full, nullptr, h->v64.b, st);
+        // K is symmetric: the same PCG and factor solve K lambda = g (saved u is kept in u_full)
+        if (!h->lambda_full) {
+            h->lambda_full = dalloc<double>(n3);
+            h->grad = dalloc<double>(h->n_elems);
+        }
+        int32_t iters = 0;
+        double rel = 0.0;
+        int32_t status;
+        if (h->precision == MAILLE_MIXED) {
+            // refinement as in the forward solve
+            norm2_of<double>(h, h->v64.b, n, h->dsum + 1);
+            CK(cudaMemsetAsync(h->v64.x, 0, n * sizeof(double), st));
+            CK(cudaMemcpyAsync(h->h_sum + 1, h->dsum + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            const double bb = h->h_sum[1];
+            status = MAILLE_OK;
+            int outer = 0;
+            while (bb > 0.0) {
+                launch_residual64(h->pattern(), h->K, h->v64.b, h->v64.x, h->rr64, h->partials,
+                                  h->dticket, h->dsum, h->spmv_grid, st);
+                CK(cudaMemcpyAsync(h->h_sum, h->dsum, sizeof(double), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                if (std::sqrt(h->h_sum[0]) <= h->tol * std::sqrt(bb)) break;
+                if (outer >= h->max_outer || iters >= h->max_iter) {
+                    status = MAILLE_NOT_CONVERGED;
+                    break;
+                }
+                launch_scale_to_float(n, h->rr64, h->dsum, h->v32.b, st);
+                int32_t it = 0;
+                double ir = 0;
+                const int32_t si = run_pcg<float>(h, h->K32, h->F32, h->v32, h->inner_tol,
+                                                  h->max_iter - iters, &it, &ir);
+                iters += it;
+                ++outer;
+                if (si == MAILLE_SINGULAR || si == MAILLE_CANCELLED) {
+                    status = si;
+                    break;
+                }
+                launch_accumulate(n, h->v32.x, h->dsum, h->v64.x, st);
+            }
+        } else {
+            status = run_pcg<double>(h, h->K, h->F, h->v64, h->tol, h->max_iter, &iters, &rel);
+        }
+        if (status != MAILLE_OK) {
+            set_error("adjoint solve failed");
+            return status;
+        }
+        // lambda in caller numbering (0 at fixed DOFs), then the element gradient
+        CK(cudaMemsetAsync(h->y_full, 0, n3 * sizeof(double), st));
+        launch_gather_u(h->n_nodes, h->inv, h->fixed, h->y_full, h->v64.x, h->lambda_full, st);
+        launch_adjoint_grad(h->npe, h->n_elems, h->conn, h->ke, h->young, h->lambda_full, h->u_full,
+                            h->grad, st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(dJdE, h->grad, h->n_elems * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (lambda)
+            CK(cudaMemcpyAsync(lambda, h->lambda_full, n3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+    return MAILLE_OK;
+}
+
+}  // namespace
+
+// ---- C ABI -------------------------------------------------------------------------------------
+
+extern "C" {
+
+const char* maille_gpu_last_error(void) { return g_last_error.c_str(); }
+
+const char* maille_gpu_version(void) { return "maille-b200 0.1.0 (sm_100a)"; }
+
+int32_t maille_gpu_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int32_t maille_gpu_create(const MailleElasticProblem* problem, MailleGpuHandle** out) {
+    g_last_error.clear();
+    return create_impl(problem, out, nullptr);
+}
+
+int32_t maille_gpu_solve(MailleGpuHandle* h, const double* f, MailleElasticResult* result) {
+    g_last_error.clear();
+    return solve_impl(h, f, result);
+}
+
+int32_t maille_gpu_backward(MailleGpuHandle* h, const double* dJdu, double* dJdE, double* lambda) {
+    g_last_error.clear();
+    return backward_impl(h, dJdu, dJdE, lambda);
+}
+
+void maille_gpu_cancel(MailleGpuHandle* h, int32_t flag) {
+    if (h) h->cancel.store(flag ? 1 : 0);
+}
+
+void* maille_gpu_stream(MailleGpuHandle* h) { return h ? (void*)h->st : nullptr; }
+
+void maille_gpu_destroy(MailleGpuHandle* h) { delete h; }
+
+int32_t maille_gpu_elastic_solve(const MailleElasticProblem* problem, MailleElasticResult* result) {
+    g_last_error.clear();
+    MailleGpuHandle* h = nullptr;
+    int32_t s = create_impl(problem, &h, result);
+    if (s != MAILLE_OK) return s;
+    s = solve_impl(h, nullptr, result);
+    delete h;
+    return s;
+}
+
+int32_t maille_gpu_face_pressure_loads(int64_t n_nodes, const double* coords, int32_t npe,
+                                       int64_t n_elems, const int64_t* conn, int64_t n_press,
+                                       const int64_t* p_elem, const int32_t* p_face,
+                                       const double* p_value, double* f) {
+    g_last_error.clear();
+    Error err{MAILLE_OK, ""};
+    if (!coords || !conn || !f || (n_press > 0 && (!p_elem || !p_face || !p_value)))
+        return fail({MAILLE_INVALID_INPUT, "null argument"});
+    if (!face_pressure_loads(n_nodes, coords, npe, n_elems, conn, n_press, p_elem, p_face, p_value,
+                             f, err))
+        return fail(err);
+    return MAILLE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,996 @@
+// maille_oracle.cpp -- CPU FP64 restatement of the reference's linear-elastic solve path.
+//
+// TEST INFRASTRUCTURE ONLY. This file is the oracle: tests/, __graft_entry__.smoke() and the
+// cpu_baseline / reference legs of bench.py load it as the checker and as the timed CPU
+// baseline. The product library (maille_b200/) never links, loads or calls it.
+//
+// The reference (timothee-faget/maille, pure Rust, single-threaded) cannot be compiled in this
+// image (no cargo/rustc), so this is a single-threaded C++17 restatement that keeps the
+// reference's order of floating-point operations: it is compiled with -ffp-contract=off (Rust
+// never fuses a*b+c), sums are left folds like Rust's Iterator::sum, and `dot` keeps the
+// reference's 8-lane combine order. Every function cites the reference file:line it follows
+// (paths relative to the reference project root, crate maille-core unless stated).
+//
+// Parity pin: the oracle is checked against the reference's own known-answer tests (analytic
+// patch test, uniaxial traction, hydrostatic cube with face pressure, face-load KATs, element
+// invariants, the iterative.rs / solve.rs unit tests and the examples/cube fixture), restated in
+// tests/test_oracle_kats.py.
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <optional>
+#include <vector>
+
+namespace {
+
+using std::size_t;
+using Vec = std::vector<double>;
+using IVec = std::vector<size_t>;
+constexpr size_t NONE = std::numeric_limits<size_t>::max();
+
+// --- constants -------------------------------------------------------------------------------
+
+// src/iterative.rs:9-14
+constexpr double TOLERANCE = 1e-12;
+constexpr size_t MAX_ITERATIONS = 10000;
+constexpr double SHIFTS[6] = {0.0, 1e-3, 1e-2, 1e-1, 1.0, 10.0};
+// src/solve.rs:185
+constexpr size_t ITERATIVE_FROM = 100000;
+
+// status codes shared with the tests (mirror of MailleError on this path, src/error.rs:224-229)
+enum Status : int { OK = 0, SINGULAR = 1, NOT_CONVERGED = 2, INVALID = 3 };
+
+// --- quadrature: src/quadrature.rs ------------------------------------------------------------
+
+struct TetGP { double xi, eta, zeta, w; };
+struct TriGP { double xi, eta, w; };
+
+// TETRA_1, quadrature.rs:100-105
+const TetGP TETRA_1[1] = {{0.25, 0.25, 0.25, 1.0 / 6.0}};
+// TET_A / TET_B and TETRA_4, quadrature.rs:108-138
+constexpr double TET_A = 0.5854101966249685;
+constexpr double TET_B = 0.1381966011250105;
+const TetGP TETRA_4[4] = {{TET_B, TET_B, TET_B, 1.0 / 24.0},
+                          {TET_A, TET_B, TET_B, 1.0 / 24.0},
+                          {TET_B, TET_A, TET_B, 1.0 / 24.0},
+                          {TET_B, TET_B, TET_A, 1.0 / 24.0}};
+// TRIANGLE_3, quadrature.rs:19-35
+const TriGP TRIANGLE_3[3] = {{1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0},
+                             {2.0 / 3.0, 1.0 / 6.0, 1.0 / 6.0},
+                             {1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0}};
+// TRIANGLE_6 (Dunavant), quadrature.rs:38-54
+constexpr double T6A = 0.445948490915965;
+constexpr double T6WA = 0.223381589678011 / 2.0;
+constexpr double T6B = 0.091576213509771;
+constexpr double T6WB = 0.109951743655322 / 2.0;
+const TriGP TRIANGLE_6[6] = {{T6A, T6A, T6WA},
+                             {1.0 - 2.0 * T6A, T6A, T6WA},
+                             {T6A, 1.0 - 2.0 * T6A, T6WA},
+                             {T6B, T6B, T6WB},
+                             {1.0 - 2.0 * T6B, T6B, T6WB},
+                             {T6B, 1.0 - 2.0 * T6B, T6WB}};
+
+// --- shape functions: src/shape.rs -----------------------------------------------------------
+
+// TET_FACES, shape.rs:129 ; TET10_EDGES, shape.rs:135
+const int TET_FACES[4][3] = {{0, 1, 2}, {0, 3, 1}, {1, 3, 2}, {2, 3, 0}};
+const int TET10_EDGES[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+
+// tet_barycentric + tet4 + tet10, shape.rs:95-153. n: values, dn: [npe][3] derivatives.
+void tet_shape(int npe, double xi, double eta, double zeta, double* n, double (*dn)[3]) {
+    const double l[4] = {1.0 - xi - eta - zeta, xi, eta, zeta};
+    const double dl[4][3] = {{-1.0, -1.0, -1.0}, {1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+    if (npe == 4) {
+        for (int i = 0; i < 4; ++i) {
+            n[i] = l[i];
+            for (int c = 0; c < 3; ++c) dn[i][c] = dl[i][c];
+        }
+        return;
+    }
+    for (int i = 0; i < 4; ++i) {
+        n[i] = l[i] * (2.0 * l[i] - 1.0);
+        for (int c = 0; c < 3; ++c) dn[i][c] = (4.0 * l[i] - 1.0) * dl[i][c];
+    }
+    for (int k = 0; k < 6; ++k) {
+        const int a = TET10_EDGES[k][0], b = TET10_EDGES[k][1];
+        n[4 + k] = 4.0 * l[a] * l[b];
+        for (int c = 0; c < 3; ++c) dn[4 + k][c] = 4.0 * (l[a] * dl[b][c] + l[b] * dl[a][c]);
+    }
+}
+
+// tri3 / tri6 values, shape.rs:11-48
+void tri_values(int nn, double xi, double eta, double* n) {
+    if (nn == 3) {
+        n[0] = 1.0 - xi - eta;
+        n[1] = xi;
+        n[2] = eta;
+        return;
+    }
+    const double l1 = 1.0 - xi - eta, l2 = xi, l3 = eta;
+    n[0] = l1 * (2.0 * l1 - 1.0);
+    n[1] = l2 * (2.0 * l2 - 1.0);
+    n[2] = l3 * (2.0 * l3 - 1.0);
+    n[3] = 4.0 * l1 * l2;
+    n[4] = 4.0 * l2 * l3;
+    n[5] = 4.0 * l3 * l1;
+}
+
+// Mapping3d::new, shape.rs:164-190: det J by cofactors and dN/dx = J^-1 dN/dxi.
+double mapping3d(int npe, const double (*coords)[3], const double (*dn)[3], double (*dn_dx)[3]) {
+    double j[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int k = 0; k < npe; ++k)
+        for (int i = 0; i < 3; ++i)
+            for (int r = 0; r < 3; ++r) j[i][r] += dn[k][i] * coords[k][r];
+    auto cof = [&](int r, int c) {
+        const int r1 = (r + 1) % 3, r2 = (r + 2) % 3, c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+        return j[r1][c1] * j[r2][c2] - j[r1][c2] * j[r2][c1];
+    };
+    double det = 0.0;
+    det = j[0][0] * cof(0, 0);
+    det = det + j[0][1] * cof(0, 1);
+    det = det + j[0][2] * cof(0, 2);
+    double inv[3][3];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) inv[r][c] = cof(c, r) / det;
+    for (int k = 0; k < npe; ++k)
+        for (int r = 0; r < 3; ++r) {
+            double s = inv[r][0] * dn[k][0];
+            s = s + inv[r][1] * dn[k][1];
+            s = s + inv[r][2] * dn[k][2];
+            dn_dx[k][r] = s;
+        }
+    return det;
+}
+
+// --- element kernels: src/element.rs ---------------------------------------------------------
+
+// solid_d, element.rs:193-206 (Voigt xx, yy, zz, yz, xz, xy; engineering shears)
+void solid_d(double young, double nu, double d[6][6]) {
+    const double c = young / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double g = young / (2.0 * (1.0 + nu));
+    for (int i = 0; i < 6; ++i)
+        for (int k = 0; k < 6; ++k) d[i][k] = 0.0;
+    for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 3; ++k) d[i][k] = (i == k) ? c * (1.0 - nu) : c * nu;
+    for (int i = 3; i < 6; ++i) d[i][i] = g;
+}
+
+// solid_strain_displacement, element.rs:209-220: column 3k+c of B (6 rows).
+void b_columns(int npe, const double (*g)[3], double (*b)[6]) {
+    for (int k = 0; k < npe; ++k) {
+        const double gx = g[k][0], gy = g[k][1], gz = g[k][2];
+        const double c0[6] = {gx, 0.0, 0.0, 0.0, gz, gy};
+        const double c1[6] = {0.0, gy, 0.0, gz, 0.0, gx};
+        const double c2[6] = {0.0, 0.0, gz, gy, gx, 0.0};
+        for (int r = 0; r < 6; ++r) {
+            b[3 * k][r] = c0[r];
+            b[3 * k + 1][r] = c1[r];
+            b[3 * k + 2][r] = c2[r];
+        }
+    }
+}
+
+// Rule of SolidKernel::tet4 / ::tet10, assembly.rs:212-229
+int rule_of(int npe, const TetGP** rule) {
+    if (npe == 4) {
+        *rule = TETRA_1;
+        return 1;
+    }
+    *rule = TETRA_4;
+    return 4;
+}
+
+// solid_stiffness, element.rs:223-243. ke is m x m row-major, ke[j*m+i].
+void solid_stiffness(int npe, const double (*coords)[3], const double d[6][6], double* ke) {
+    const int m = 3 * npe;
+    std::fill(ke, ke + m * m, 0.0);
+    const TetGP* rule;
+    const int ng = rule_of(npe, &rule);
+    double n[10], dn[10][3], dn_dx[10][3], b[30][6];
+    for (int gp = 0; gp < ng; ++gp) {
+        tet_shape(npe, rule[gp].xi, rule[gp].eta, rule[gp].zeta, n, dn);
+        const double det = mapping3d(npe, coords, dn, dn_dx);
+        b_columns(npe, dn_dx, b);
+        const double factor = rule[gp].w * std::fabs(det);
+        for (int i = 0; i < m; ++i) {
+            double db[6];
+            for (int r = 0; r < 6; ++r) {
+                double s = d[r][0] * b[i][0];
+                for (int c = 1; c < 6; ++c) s = s + d[r][c] * b[i][c];
+                db[r] = s;
+            }
+            for (int jj = 0; jj < m; ++jj) {
+                double s = b[jj][0] * db[0];
+                for (int r = 1; r < 6; ++r) s = s + b[jj][r] * db[r];
+                ke[jj * m + i] += factor * s;
+            }
+        }
+    }
+}
+
+// solid_stresses, element.rs:270-302 (no thermal strain on this path: strain_e empty, e = 0).
+// out per Gauss point: x, y, z, sxx, syy, szz, txy, tyz, txz (field order of results.rs:6-20).
+void solid_stresses(int npe, const double (*coords)[3], const double d[6][6], const double* u_e,
+                    double* out) {
+    const TetGP* rule;
+    const int ng = rule_of(npe, &rule);
+    const int m = 3 * npe;
+    double n[10], dn[10][3], dn_dx[10][3], b[30][6];
+    for (int gp = 0; gp < ng; ++gp) {
+        tet_shape(npe, rule[gp].xi, rule[gp].eta, rule[gp].zeta, n, dn);
+        mapping3d(npe, coords, dn, dn_dx);
+        b_columns(npe, dn_dx, b);
+        double eps[6], sigma[6];
+        for (int r = 0; r < 6; ++r) {
+            double s = b[0][r] * u_e[0];
+            for (int k = 1; k < m; ++k) s = s + b[k][r] * u_e[k];
+            eps[r] = s - 0.0;
+        }
+        for (int r = 0; r < 6; ++r) {
+            double s = d[r][0] * eps[0];
+            for (int c = 1; c < 6; ++c) s = s + d[r][c] * eps[c];
+            sigma[r] = s;
+        }
+        double at[3];
+        for (int k = 0; k < 3; ++k) {
+            double s = n[0] * coords[0][k];
+            for (int i = 1; i < npe; ++i) s = s + n[i] * coords[i][k];
+            at[k] = s;
+        }
+        double* o = out + 9 * gp;
+        o[0] = at[0];
+        o[1] = at[1];
+        o[2] = at[2];
+        o[3] = sigma[0];
+        o[4] = sigma[1];
+        o[5] = sigma[2];
+        o[6] = sigma[5];  // tau_xy
+        o[7] = sigma[3];  // tau_yz
+        o[8] = sigma[4];  // tau_xz
+    }
+}
+
+// Stress::von_mises, results.rs:24-32 (s in the layout written by solid_stresses)
+double von_mises(const double* s) {
+    const double a = s[3], b = s[4], c = s[5];
+    const double shear = s[6] * s[6] + s[7] * s[7] + s[8] * s[8];
+    const double v = a * a + b * b + c * c - a * b - b * c - c * a + 3.0 * shear;
+    return std::sqrt(v > 0.0 ? v : 0.0);
+}
+
+// --- face pressure: src/assembly.rs:527-593 (tet branch 556-585), 650-674; mesh.rs:184-198 -----
+
+int face_positions(int npe, int face, int* pos) {
+    if (face < 0 || face > 3) return 0;
+    const int a = TET_FACES[face][0], b = TET_FACES[face][1], c = TET_FACES[face][2];
+    pos[0] = a;
+    pos[1] = b;
+    pos[2] = c;
+    if (npe == 4) return 3;
+    auto mid = [](int p, int q) {
+        for (int k = 0; k < 6; ++k)
+            if ((TET10_EDGES[k][0] == p && TET10_EDGES[k][1] == q) ||
+                (TET10_EDGES[k][0] == q && TET10_EDGES[k][1] == p))
+                return 4 + k;
+        return 4;
+    };
+    pos[3] = mid(a, b);
+    pos[4] = mid(b, c);
+    pos[5] = mid(c, a);
+    return 6;
+}
+
+// forces[3*k + c] for the k-th face node, positions in pos. Returns the number of face nodes.
+int face_pressure(int npe, const double (*ecoords)[3], int face, double value, int* pos,
+                  double* forces) {
+    const int nn = face_positions(npe, face, pos);
+    if (nn == 0) return 0;
+    double c[6][3];
+    for (int k = 0; k < nn; ++k)
+        for (int q = 0; q < 3; ++q) c[k][q] = ecoords[pos[k]][q];
+    double u[3], v[3];
+    for (int k = 0; k < 3; ++k) {
+        u[k] = c[1][k] - c[0][k];
+        v[k] = c[2][k] - c[0][k];
+    }
+    const double cross[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2],
+                             u[0] * v[1] - u[1] * v[0]};
+    double sq = cross[0] * cross[0];
+    sq = sq + cross[1] * cross[1];
+    sq = sq + cross[2] * cross[2];
+    const double twice_area = std::sqrt(sq);
+    const TriGP* rule = (nn == 3) ? TRIANGLE_3 : TRIANGLE_6;
+    const int np = (nn == 3) ? 3 : 6;
+    double outward[3];
+    for (int k = 0; k < 3; ++k)
+        outward[k] = (c[0][k] + c[1][k] + c[2][k]) / 3.0 -
+                     (ecoords[0][k] + ecoords[1][k] + ecoords[2][k] + ecoords[3][k]) / 4.0;
+    double dot = cross[0] * outward[0];
+    dot = dot + cross[1] * outward[1];
+    dot = dot + cross[2] * outward[2];
+    const double sign = dot < 0.0 ? -1.0 : 1.0;
+    double normal[3];
+    for (int k = 0; k < 3; ++k) normal[k] = sign * cross[k] / twice_area;
+    for (int k = 0; k < 3 * nn; ++k) forces[k] = 0.0;
+    for (int g = 0; g < np; ++g) {
+        const double w = rule[g].w * twice_area;
+        double nv[6];
+        tri_values(nn, rule[g].xi, rule[g].eta, nv);
+        for (int a = 0; a < nn; ++a)
+            for (int q = 0; q < 3; ++q) forces[3 * a + q] -= value * w * nv[a] * normal[q];
+    }
+    return nn;
+}
+
+// --- sparse machinery: src/solve.rs, src/iterative.rs -----------------------------------------
+
+// dot, solve.rs:100-110: 8 partial sums, fixed combine, sequential tail.
+double dot(const double* a, const double* b, size_t n) {
+    const size_t full = n / 8 * 8;
+    double tail = 0.0;
+    for (size_t k = full; k < n; ++k) tail = tail + a[k] * b[k];
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (size_t k = 0; k < full; k += 8)
+        for (int l = 0; l < 8; ++l) s[l] += a[k + l] * b[k + l];
+    return ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7])) + tail;
+}
+
+// Graph (CSR adjacency), iterative.rs:19-76
+struct Graph {
+    IVec offsets, targets;
+    size_t len() const { return offsets.size() - 1; }
+    size_t degree(size_t v) const { return offsets[v + 1] - offsets[v]; }
+};
+
+// Graph::from_elements, iterative.rs:38-76 (element lists given as CSR: eoff/eidx)
+Graph graph_from_elements(size_t n, const IVec& eoff, const IVec& eidx) {
+    const size_t ne = eoff.size() - 1;
+    IVec incident(n + 1, 0);
+    for (size_t e = 0; e < ne; ++e)
+        for (size_t p = eoff[e]; p < eoff[e + 1]; ++p) incident[eidx[p] + 1] += 1;
+    for (size_t v = 0; v < n; ++v) incident[v + 1] += incident[v];
+    IVec cursor = incident;
+    IVec of_vertex(incident[n]);
+    for (size_t e = 0; e < ne; ++e)
+        for (size_t p = eoff[e]; p < eoff[e + 1]; ++p) of_vertex[cursor[eidx[p]]++] = e;
+    Graph g;
+    g.offsets.reserve(n + 1);
+    g.offsets.push_back(0);
+    IVec mark(n, NONE);
+    for (size_t v = 0; v < n; ++v) {
+        mark[v] = v;
+        for (size_t q = incident[v]; q < incident[v + 1]; ++q) {
+            const size_t e = of_vertex[q];
+            for (size_t p = eoff[e]; p < eoff[e + 1]; ++p) {
+                const size_t w = eidx[p];
+                if (mark[w] != v) {
+                    mark[w] = v;
+                    g.targets.push_back(w);
+                }
+            }
+        }
+        g.offsets.push_back(g.targets.size());
+    }
+    return g;
+}
+
+// bfs_levels, solve.rs:248-270
+std::vector<IVec> bfs_levels(const Graph& g, size_t start, const std::vector<char>& excluded) {
+    std::vector<char> seen = excluded;
+    seen[start] = 1;
+    std::vector<IVec> levels{IVec{start}};
+    for (;;) {
+        IVec next;
+        for (size_t v : levels.back())
+            for (size_t p = g.offsets[v]; p < g.offsets[v + 1]; ++p) {
+                const size_t w = g.targets[p];
+                if (!seen[w]) {
+                    seen[w] = 1;
+                    next.push_back(w);
+                }
+            }
+        if (next.empty()) return levels;
+        levels.push_back(std::move(next));
+    }
+}
+
+// reverse_cuthill_mckee, solve.rs:200-245 (order[new] = old)
+IVec reverse_cuthill_mckee(const Graph& g) {
+    const size_t n = g.len();
+    std::vector<char> visited(n, 0);
+    IVec order;
+    order.reserve(n);
+    size_t scan_from = 0;  // every vertex before it is visited (same first minimum as a full scan)
+    for (;;) {
+        while (scan_from < n && visited[scan_from]) ++scan_from;
+        size_t seed = NONE;
+        for (size_t v = scan_from; v < n; ++v)
+            if (!visited[v] && (seed == NONE || g.degree(v) < g.degree(seed))) seed = v;
+        if (seed == NONE) break;
+        size_t start = seed;
+        auto levels = bfs_levels(g, start, visited);
+        for (;;) {
+            const IVec& last = levels.back();
+            size_t far = NONE;
+            for (size_t v : last)
+                if (far == NONE || g.degree(v) < g.degree(far)) far = v;
+            if (far == NONE) break;
+            auto far_levels = bfs_levels(g, far, visited);
+            if (far_levels.size() <= levels.size()) break;
+            start = far;
+            levels = std::move(far_levels);
+        }
+        const size_t first = order.size();
+        visited[start] = 1;
+        order.push_back(start);
+        size_t head = first;
+        while (head < order.size()) {
+            const size_t v = order[head++];
+            IVec next;
+            for (size_t p = g.offsets[v]; p < g.offsets[v + 1]; ++p)
+                if (!visited[g.targets[p]]) next.push_back(g.targets[p]);
+            std::stable_sort(next.begin(), next.end(),
+                             [&](size_t a, size_t b) { return g.degree(a) < g.degree(b); });
+            for (size_t w : next)
+                if (!visited[w]) {
+                    visited[w] = 1;
+                    order.push_back(w);
+                }
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    return order;
+}
+
+// Csr: lower triangle incl. diagonal, columns ascending, diagonal last. iterative.rs:82-189
+struct Csr {
+    IVec offsets, cols;
+    Vec values;
+    size_t n() const { return offsets.size() - 1; }
+
+    // Csr::zeros, iterative.rs:91-114
+    static Csr zeros(const Graph& g, const IVec& order, const IVec& rank) {
+        Csr m;
+        m.offsets.reserve(order.size() + 1);
+        m.offsets.push_back(0);
+        for (size_t r = 0; r < order.size(); ++r) {
+            const size_t v = order[r];
+            const size_t start = m.cols.size();
+            for (size_t p = g.offsets[v]; p < g.offsets[v + 1]; ++p) {
+                const size_t c = rank[g.targets[p]];
+                if (c < r) m.cols.push_back(c);
+            }
+            std::sort(m.cols.begin() + start, m.cols.end());
+            m.cols.push_back(r);
+            m.offsets.push_back(m.cols.size());
+        }
+        m.values.assign(m.cols.size(), 0.0);
+        return m;
+    }
+
+    // Csr::add, iterative.rs:121-128. Returns false when the entry is outside the profile.
+    bool add(size_t i, size_t j, double v) {
+        if (j > i) std::swap(i, j);
+        auto b = cols.begin() + offsets[i], e = cols.begin() + offsets[i + 1];
+        auto it = std::lower_bound(b, e, j);
+        if (it == e || *it != j) return false;
+        values[it - cols.begin()] += v;
+        return true;
+    }
+
+    // Csr::multiply, iterative.rs:131-142
+    void multiply(const double* x, double* y) const {
+        const size_t nn = n();
+        std::fill(y, y + nn, 0.0);
+        for (size_t i = 0; i < nn; ++i) {
+            const size_t start = offsets[i], diag = offsets[i + 1] - 1;
+            double s = values[diag] * x[i];
+            for (size_t p = start; p < diag; ++p) {
+                s += values[p] * x[cols[p]];
+                y[cols[p]] += values[p] * x[i];
+            }
+            y[i] += s;
+        }
+    }
+
+    // Csr::incomplete_cholesky, iterative.rs:146-170
+    std::optional<Vec> incomplete_cholesky(double shift) const {
+        const size_t nn = n();
+        Vec l(values.size(), 0.0), w(nn, 0.0);
+        for (size_t i = 0; i < nn; ++i) {
+            const size_t start = offsets[i], diag = offsets[i + 1] - 1;
+            for (size_t p = start; p < diag; ++p) {
+                const size_t j = cols[p];
+                const size_t js = offsets[j], jd = offsets[j + 1] - 1;
+                double s = 0.0;
+                for (size_t q = js; q < jd; ++q) s = s + l[q] * w[cols[q]];
+                l[p] = (values[p] - s) / l[jd];
+                w[j] = l[p];
+            }
+            double squares = 0.0;
+            for (size_t p = start; p < diag; ++p) squares = squares + l[p] * l[p];
+            const double pivot = values[diag] * (1.0 + shift) - squares;
+            if (std::isnan(pivot) || pivot <= 1e-12 * values[diag]) return std::nullopt;
+            l[diag] = std::sqrt(pivot);
+            for (size_t p = start; p < diag; ++p) w[cols[p]] = 0.0;
+        }
+        return l;
+    }
+
+    // Csr::precondition, iterative.rs:173-188
+    void precondition(const Vec& l, const double* r, double* z) const {
+        const size_t nn = n();
+        std::copy(r, r + nn, z);
+        for (size_t i = 0; i < nn; ++i) {
+            const size_t start = offsets[i], diag = offsets[i + 1] - 1;
+            double s = 0.0;
+            for (size_t p = start; p < diag; ++p) s = s + l[p] * z[cols[p]];
+            z[i] = (z[i] - s) / l[diag];
+        }
+        for (size_t i = nn; i-- > 0;) {
+            const size_t start = offsets[i], diag = offsets[i + 1] - 1;
+            z[i] /= l[diag];
+            for (size_t p = start; p < diag; ++p) z[cols[p]] -= l[p] * z[i];
+        }
+    }
+};
+
+struct SolveStats {
+    size_t iterations = 0;
+    double rel_residual = 0.0;
+    double shift = 0.0;
+};
+
+// Pcg::new + Pcg::solve, iterative.rs:201-248. tol replaces the TOLERANCE constant (default 1e-12).
+int pcg_solve(const Csr& a, const Vec& b, double tol, size_t max_iter, Vec& x, SolveStats& st,
+              const Vec* l_given = nullptr) {
+    Vec l;
+    if (l_given) {
+        l = *l_given;
+    } else {
+        bool ok = false;
+        for (double shift : SHIFTS) {
+            auto got = a.incomplete_cholesky(shift);
+            if (got) {
+                l = std::move(*got);
+                st.shift = shift;
+                ok = true;
+                break;
+            }
+        }
+        if (!ok) return SINGULAR;
+    }
+    const size_t n = b.size();
+    auto norm = [n](const Vec& v) { return std::sqrt(dot(v.data(), v.data(), n)); };
+    const double b_norm = norm(b);
+    x.assign(n, 0.0);
+    st.iterations = 0;
+    if (b_norm == 0.0) {
+        st.rel_residual = 0.0;
+        return OK;
+    }
+    Vec r = b, z(n), p(n), ap(n);
+    a.precondition(l, r.data(), z.data());
+    p = z;
+    double rz = dot(r.data(), z.data(), n);
+    for (size_t it = 0; it < max_iter; ++it) {
+        a.multiply(p.data(), ap.data());
+        const double curvature = dot(p.data(), ap.data(), n);
+        if (std::isnan(curvature) || curvature <= 0.0) {
+            st.iterations = it + 1;
+            return SINGULAR;
+        }
+        const double alpha = rz / curvature;
+        for (size_t k = 0; k < n; ++k) {
+            x[k] += alpha * p[k];
+            r[k] -= alpha * ap[k];
+        }
+        const double rn = norm(r);
+        st.iterations = it + 1;
+        st.rel_residual = rn / b_norm;
+        if (rn <= tol * b_norm) return OK;
+        a.precondition(l, r.data(), z.data());
+        const double rz_next = dot(r.data(), z.data(), n);
+        const double beta = rz_next / rz;
+        rz = rz_next;
+        for (size_t k = 0; k < n; ++k) p[k] = z[k] + beta * p[k];
+    }
+    st.rel_residual = norm(r) / b_norm;
+    return NOT_CONVERGED;
+}
+
+// SkylineMatrix + Cholesky, solve.rs:10-139 (the direct solver, kept as a second oracle)
+struct Skyline {
+    IVec first, start;
+    Vec data;
+    explicit Skyline(IVec f) : first(std::move(f)) {
+        start.assign(first.size() + 1, 0);
+        for (size_t i = 0; i < first.size(); ++i) start[i + 1] = start[i] + i + 1 - first[i];
+        data.assign(start.back(), 0.0);
+    }
+    size_t n() const { return first.size(); }
+    double get(size_t i, size_t j) const {
+        if (j > i) std::swap(i, j);
+        return j < first[i] ? 0.0 : data[start[i] + j - first[i]];
+    }
+    void add(size_t i, size_t j, double v) {
+        if (j > i) std::swap(i, j);
+        data[start[i] + j - first[i]] += v;
+    }
+    // factorize, solve.rs:70-94
+    int factorize() {
+        const size_t nn = n();
+        double max_diag = 0.0;
+        for (size_t i = 0; i < nn; ++i) max_diag = std::fmax(max_diag, get(i, i));
+        const double tol = 1e-12 * max_diag;
+        for (size_t i = 0; i < nn; ++i) {
+            const size_t fi = first[i];
+            for (size_t j = fi; j <= i; ++j) {
+                const size_t k0 = std::max(fi, first[j]);
+                const size_t ri = start[i] - fi, rj = start[j] - first[j];
+                const double s = dot(&data[ri + k0], &data[rj + k0], j - k0);
+                const double a = data[ri + j] - s;
+                if (i == j) {
+                    if (std::isnan(a) || a <= tol) return SINGULAR;
+                    data[ri + j] = std::sqrt(a);
+                } else {
+                    data[ri + j] = a / data[rj + j];
+                }
+            }
+        }
+        return OK;
+    }
+    // Cholesky::solve, solve.rs:118-138
+    Vec solve(const Vec& b) const {
+        Vec x = b;
+        const size_t nn = n();
+        for (size_t i = 0; i < nn; ++i) {
+            const size_t fi = first[i];
+            const double* row = &data[start[i]];
+            double s = 0.0;
+            for (size_t k = fi; k < i; ++k) s = s + row[k - fi] * x[k];
+            x[i] = (x[i] - s) / row[i - fi];
+        }
+        for (size_t i = nn; i-- > 0;) {
+            const size_t fi = first[i];
+            const double* row = &data[start[i]];
+            x[i] /= row[i - fi];
+            for (size_t k = fi; k < i; ++k) x[k] -= row[k - fi] * x[i];
+        }
+        return x;
+    }
+};
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+// Element matrix of element e of a solid mesh (element_stiffness, assembly.rs:64-79, Tet branch)
+struct SolidMesh {
+    size_t n_nodes, n_elems;
+    int npe;
+    const double* coords;
+    const int64_t* conn;
+    const double* young;
+    const double* poisson;
+    void elem_coords(size_t e, double (*c)[3]) const {
+        for (int a = 0; a < npe; ++a)
+            for (int k = 0; k < 3; ++k) c[a][k] = coords[3 * conn[e * npe + a] + k];
+    }
+    void stiffness(size_t e, double* ke) const {
+        double c[10][3], d[6][6];
+        elem_coords(e, c);
+        solid_d(young[e], poisson[e], d);
+        solid_stiffness(npe, c, d, ke);
+    }
+};
+
+}  // namespace
+
+// ============================================================================================
+// C ABI used by the tests and bench (ctypes). Everything below is test infrastructure.
+// ============================================================================================
+extern "C" {
+
+// element_stiffness of one Tet4/Tet10 (coords npe x 3), ke: (3npe)^2 row-major
+void oracle_element_stiffness(int npe, const double* coords, double young, double nu, double* ke) {
+    double d[6][6];
+    solid_d(young, nu, d);
+    solid_stiffness(npe, reinterpret_cast<const double(*)[3]>(coords), d, ke);
+}
+
+// element_stresses of one element: out ngp x 9 (x, y, z, sxx, syy, szz, txy, tyz, txz)
+void oracle_element_stresses(int npe, const double* coords, double young, double nu,
+                             const double* u_e, double* out) {
+    double d[6][6];
+    solid_d(young, nu, d);
+    solid_stresses(npe, reinterpret_cast<const double(*)[3]>(coords), d, u_e, out);
+}
+
+double oracle_von_mises(const double* s9) { return von_mises(s9); }
+
+// face_pressure of one element: positions (<=6) and forces (3 per face node). Returns node count.
+int oracle_face_pressure(int npe, const double* coords, int face, double value, int* positions,
+                         double* forces) {
+    return face_pressure(npe, reinterpret_cast<const double(*)[3]>(coords), face, value, positions,
+                         forces);
+}
+
+double oracle_dot(const double* a, const double* b, int64_t n) { return dot(a, b, (size_t)n); }
+
+// Graph::from_elements. Call with out_targets = NULL to get the target count.
+int64_t oracle_graph_from_elements(int64_t n, int64_t n_el, const int64_t* eoff,
+                                   const int64_t* eidx, int64_t* out_offsets,
+                                   int64_t* out_targets) {
+    IVec o(eoff, eoff + n_el + 1), ix(eidx, eidx + eoff[n_el]);
+    Graph g = graph_from_elements((size_t)n, o, ix);
+    if (out_offsets)
+        for (size_t v = 0; v <= (size_t)n; ++v) out_offsets[v] = (int64_t)g.offsets[v];
+    if (out_targets)
+        for (size_t p = 0; p < g.targets.size(); ++p) out_targets[p] = (int64_t)g.targets[p];
+    return (int64_t)g.targets.size();
+}
+
+// reverse_cuthill_mckee on a CSR adjacency
+void oracle_rcm(int64_t n, const int64_t* offsets, const int64_t* targets, int64_t* order) {
+    Graph g;
+    g.offsets.assign(offsets, offsets + n + 1);
+    g.targets.assign(targets, targets + offsets[n]);
+    IVec o = reverse_cuthill_mckee(g);
+    for (size_t k = 0; k < o.size(); ++k) order[k] = (int64_t)o[k];
+}
+
+// A Csr built on `graph` in numbering `order` (identity when order == NULL), filled with
+// triplets (Csr::add in the renumbered indices ti, tj). mode 0: Pcg::new + Pcg::solve(b) -> x;
+// mode 1: incomplete_cholesky(0) + precondition(b) -> x; mode 2: multiply(b) -> x.
+// Returns the status (0 OK, 1 SINGULAR, 2 NOT_CONVERGED, 3 outside profile).
+int oracle_csr_run(int64_t n, const int64_t* offsets, const int64_t* targets, const int64_t* order,
+                   int64_t nt, const int64_t* ti, const int64_t* tj, const double* tv,
+                   const double* b, int mode, double tol, double* x, int64_t* iterations) {
+    Graph g;
+    g.offsets.assign(offsets, offsets + n + 1);
+    g.targets.assign(targets, targets + offsets[n]);
+    IVec ord(n), rank(n);
+    for (int64_t k = 0; k < n; ++k) ord[k] = order ? (size_t)order[k] : (size_t)k;
+    for (int64_t k = 0; k < n; ++k) rank[ord[k]] = (size_t)k;
+    Csr a = Csr::zeros(g, ord, rank);
+    for (int64_t t = 0; t < nt; ++t)
+        if (!a.add((size_t)ti[t], (size_t)tj[t], tv[t])) return INVALID;
+    Vec bb(b, b + n), xx(n);
+    if (mode == 2) {
+        a.multiply(bb.data(), xx.data());
+    } else if (mode == 1) {
+        auto l = a.incomplete_cholesky(0.0);
+        if (!l) return SINGULAR;
+        a.precondition(*l, bb.data(), xx.data());
+    } else {
+        SolveStats st;
+        int s = pcg_solve(a, bb, tol, MAX_ITERATIONS, xx, st);
+        if (iterations) *iterations = (int64_t)st.iterations;
+        if (s != OK) return s;
+    }
+    std::copy(xx.begin(), xx.end(), x);
+    return OK;
+}
+
+// Model::solve for a linear static Tet4/Tet10 model (model.rs:548-610 with assemble 1070-1147,
+// FreeSystem::new/solve 1442-1516, product 1353-1369, element_stresses 304-312).
+//   loads: nodal load vector (3 n_nodes; the sum of the model's Loads at their DOFs)
+//   pressures: (element, face, value) triples added through face_pressure + add_load
+//   solver: 0 Auto, 1 Direct, 2 Iterative (SolverKind, solve.rs:170-195)
+//   tol: PCG relative-residual tolerance (the reference's constant is 1e-12; 0 selects it)
+//   dof_order: optional permutation of the free DOFs (order[new] = old free index) that replaces
+//              RCM; NULL keeps reverse_cuthill_mckee. Used to check the GPU ordering's factor.
+//   out: u, reactions (3 n_nodes), gauss (n_elems*ngp*9), vm (n_elems*ngp), f_out (3 n_nodes),
+//        info[0..7] = iterations, rel_residual, shift, free dofs, nnz(L), ms setup, ms factor, ms pcg
+int oracle_model_solve(int64_t n_nodes, const double* coords, int npe, int64_t n_elems,
+                       const int64_t* conn, const double* young, const double* poisson,
+                       const uint8_t* fixed, const double* imposed, const double* loads,
+                       int64_t n_press, const int64_t* p_elem, const int32_t* p_face,
+                       const double* p_value, int solver, double tol, int64_t max_iter,
+                       const int64_t* dof_order, double* u, double* reactions, double* gauss,
+                       double* vm, double* f_out, double* info) {
+    if (tol <= 0.0) tol = TOLERANCE;
+    if (max_iter <= 0) max_iter = (int64_t)MAX_ITERATIONS;
+    const double t0 = now_ms();
+    SolidMesh mesh{(size_t)n_nodes, (size_t)n_elems, npe, coords, conn, young, poisson};
+    const size_t n = 3 * (size_t)n_nodes;
+    const int m = 3 * npe;
+    // assemble, model.rs:1070-1147: element DOFs (element_dofs, assembly.rs:20-32), loads,
+    // pressures, imposed/fixed
+    Vec f(n, 0.0);
+    for (size_t g = 0; g < n; ++g) f[g] += loads ? loads[g] : 0.0;
+    for (int64_t k = 0; k < n_press; ++k) {
+        const size_t e = (size_t)p_elem[k];
+        double c[10][3], forces[18];
+        int pos[6];
+        mesh.elem_coords(e, c);
+        const int nn = face_pressure(npe, c, p_face[k], p_value[k], pos, forces);
+        for (int a = 0; a < nn; ++a)
+            for (int q = 0; q < 3; ++q)
+                f[3 * (size_t)conn[e * npe + pos[a]] + q] += forces[3 * a + q];
+    }
+    auto dof = [&](size_t e, int l) { return 3 * (size_t)conn[e * npe + l / 3] + l % 3; };
+    Vec uu(n);
+    for (size_t g = 0; g < n; ++g) uu[g] = fixed[g] ? imposed[g] : 0.0;
+
+    // FreeSystem::new, model.rs:1442-1499
+    IVec free(n, NONE);
+    size_t count = 0;
+    for (size_t g = 0; g < n; ++g)
+        if (!fixed[g]) free[g] = count++;
+    IVec eoff(mesh.n_elems + 1, 0), eidx;
+    for (size_t e = 0; e < mesh.n_elems; ++e) {
+        for (int l = 0; l < m; ++l)
+            if (free[dof(e, l)] != NONE) eidx.push_back(free[dof(e, l)]);
+        eoff[e + 1] = eidx.size();
+    }
+    Graph graph = graph_from_elements(count, eoff, eidx);
+    IVec order;
+    if (dof_order) {
+        order.assign(count, 0);
+        for (size_t k = 0; k < count; ++k) order[k] = (size_t)dof_order[k];
+    } else {
+        order = reverse_cuthill_mckee(graph);
+    }
+    IVec rank(count);
+    for (size_t r = 0; r < count; ++r) rank[order[r]] = r;
+    const bool iterative = solver == 2 || (solver == 0 && count >= ITERATIVE_FROM);
+    Csr csr;
+    std::optional<Skyline> sky;
+    if (iterative) {
+        csr = Csr::zeros(graph, order, rank);
+    } else {
+        IVec first(count);
+        for (size_t a = 0; a < count; ++a) first[a] = a;
+        for (size_t a = 0; a < count; ++a)
+            for (size_t p = graph.offsets[a]; p < graph.offsets[a + 1]; ++p)
+                first[rank[a]] = std::min(first[rank[a]], rank[graph.targets[p]]);
+        sky.emplace(first);
+    }
+    graph = Graph{};
+    Vec coupling(count, 0.0);
+    Vec ke((size_t)m * m);
+    for (size_t e = 0; e < mesh.n_elems; ++e) {
+        mesh.stiffness(e, ke.data());
+        for (int r = 0; r < m; ++r) {
+            const size_t a = free[dof(e, r)];
+            if (a == NONE) continue;
+            for (int c = 0; c < m; ++c) {
+                const size_t b = free[dof(e, c)];
+                const double k = ke[(size_t)r * m + c];
+                if (b != NONE) {
+                    if (rank[b] <= rank[a]) {
+                        if (iterative)
+                            csr.add(rank[a], rank[b], k);
+                        else
+                            sky->add(rank[a], rank[b], k);
+                    }
+                } else {
+                    coupling[rank[a]] += k * uu[dof(e, c)];
+                }
+            }
+        }
+    }
+    const double t1 = now_ms();
+    // FreeSystem::solve, model.rs:1502-1516
+    Vec rhs(count);
+    for (size_t k = 0; k < count; ++k) rhs[k] = -coupling[k];
+    for (size_t g = 0; g < n; ++g)
+        if (free[g] != NONE) rhs[rank[free[g]]] += f[g];
+    Vec x;
+    SolveStats st;
+    int status = OK;
+    double t2 = t1;
+    if (iterative) {
+        Vec l;
+        bool ok = false;
+        for (double shift : SHIFTS) {
+            auto got = csr.incomplete_cholesky(shift);
+            if (got) {
+                l = std::move(*got);
+                st.shift = shift;
+                ok = true;
+                break;
+            }
+        }
+        t2 = now_ms();
+        if (!ok)
+            status = SINGULAR;
+        else
+            status = pcg_solve(csr, rhs, tol, (size_t)max_iter, x, st, &l);
+    } else {
+        status = sky->factorize();
+        t2 = now_ms();
+        if (status == OK) x = sky->solve(rhs);
+    }
+    const double t3 = now_ms();
+    if (info) {
+        info[0] = (double)st.iterations;
+        info[1] = st.rel_residual;
+        info[2] = st.shift;
+        info[3] = (double)count;
+        info[4] = iterative ? (double)csr.cols.size() : (double)sky->data.size();
+        info[5] = t1 - t0;
+        info[6] = t2 - t1;
+        info[7] = t3 - t2;
+    }
+    if (f_out) std::copy(f.begin(), f.end(), f_out);
+    if (status != OK) return status;
+    for (size_t g = 0; g < n; ++g)
+        if (free[g] != NONE) uu[g] = x[rank[free[g]]];
+    std::copy(uu.begin(), uu.end(), u);
+
+    // reactions = product(dofs, matrix, u, fixed) - f on fixed DOFs, model.rs:586-593, 1353-1369
+    if (reactions) {
+        Vec y(n, 0.0);
+        for (size_t e = 0; e < mesh.n_elems; ++e) {
+            bool any = false;
+            for (int l = 0; l < m; ++l) any = any || fixed[dof(e, l)];
+            if (!any) continue;
+            mesh.stiffness(e, ke.data());
+            for (int r = 0; r < m; ++r) {
+                const size_t g = dof(e, r);
+                if (!fixed[g]) continue;
+                double s = 0.0;
+                for (int c = 0; c < m; ++c) s = s + ke[(size_t)r * m + c] * uu[dof(e, c)];
+                y[g] += s;
+            }
+        }
+        for (size_t g = 0; g < n; ++g)
+            if (fixed[g]) y[g] -= f[g];
+        std::copy(y.begin(), y.end(), reactions);
+    }
+    // Gauss-point stresses and von Mises, element_stresses, assembly.rs:304-312
+    if (gauss) {
+        const int ng = npe == 4 ? 1 : 4;
+        for (size_t e = 0; e < mesh.n_elems; ++e) {
+            double c[10][3], d[6][6], ue[30];
+            mesh.elem_coords(e, c);
+            solid_d(young[e], poisson[e], d);
+            for (int l = 0; l < m; ++l) ue[l] = uu[dof(e, l)];
+            double* o = gauss + e * ng * 9;
+            solid_stresses(npe, c, d, ue, o);
+            if (vm)
+                for (int gp = 0; gp < ng; ++gp) vm[e * ng + gp] = von_mises(o + 9 * gp);
+        }
+    }
+    return OK;
+}
+
+// nodal_stresses / smooth, results.rs:137-230: Gauss values extrapolated to the element nodes
+// (TET4_EXTRAPOLATION 98, TET10_EXTRAPOLATION 118-132) and averaged. gauss: n_elems*ngp*9 as
+// written above; out: n_nodes*6 (sxx, syy, szz, txy, tyz, txz).
+void oracle_nodal_stresses(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
+                           const double* gauss, double* out) {
+    const double V = 1.9270509831248424, M = 0.8090169943749475, O = -0.30901699437494745;
+    const double T10[10][4] = {{V, O, O, O}, {O, V, O, O}, {O, O, V, O}, {O, O, O, V},
+                               {M, M, O, O}, {O, M, M, O}, {M, O, M, O}, {M, O, O, M},
+                               {O, M, O, M}, {O, O, M, M}};
+    const int ng = npe == 4 ? 1 : 4;
+    Vec sum((size_t)n_nodes * 6, 0.0);
+    std::vector<size_t> count((size_t)n_nodes, 0);
+    for (int64_t e = 0; e < n_elems; ++e) {
+        for (int a = 0; a < npe; ++a) {
+            const size_t nd = (size_t)conn[e * npe + a];
+            for (int g = 0; g < ng; ++g) {
+                const double w = npe == 4 ? 1.0 : T10[a][g];
+                const double* p = gauss + (e * ng + g) * 9 + 3;
+                for (int c = 0; c < 6; ++c) sum[nd * 6 + c] += w * p[c];
+            }
+            count[nd] += 1;
+        }
+    }
+    for (int64_t k = 0; k < n_nodes; ++k)
+        for (int c = 0; c < 6; ++c)
+            out[k * 6 + c] = sum[k * 6 + c] / (double)std::max<size_t>(count[k], 1);
+}
+
+}  // extern "C"
