@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 linear-elastic solve path (one JSON line on rank 0).
+
+Workload (the mixed-precision configuration): Tet10 unit cube, 40^3 cells x 6 quadratic tets
+(531 441 nodes, 384 000 tets, 1 574 640 free DOF), 4-point Gauss rule, per-element E lognormal
+(median 210 000 MPa, sigma_log 0.5, seeded), nu = 0.3, z = 0 clamped, 10 MPa pressure on z = 1.
+Synthetic data generated in code (maille_b200/meshgen.py).
+
+A step is one full numeric solve on device-resident inputs: element integration, scatter-reduce
+assembly, IC(0) factorisation, FP32 inner PCG inside FP64 refinement to the relative residual
+`--tol`, reactions, Gauss stresses and von Mises. `value` = free DOF solved per second (all ranks),
+checked to reach 1e-8 relative displacement error against a tight FP64 solve. Beside it: the
+plain FP64 GPU form on the same workload and tolerance, the live SpMV roofline, the end-to-end
+rate through the C ABI with host buffers (`e2e`), and the CPU oracle baseline.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--cells C]
+Under torchrun each rank solves its own replica (replicas only: the IC(0) solve does not shard).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DOF/s to 1e-8 rel. error: mixed/batched vs plain FP64 GPU; SpMV HBM GB/s"
+UNIT = "DOF/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=40)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling (200 ms) during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
+              "utilization.gpu")
+
+    def __init__(self, local_rank):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v for v in vis.split(",") if v.strip()]
+        self.index = ids[local_rank] if local_rank < len(ids) and ids[local_rank].isdigit() else str(local_rank)
+        self.proc = None
+
+    def start(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.index, f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        rows = [l.split(",") for l in open(self.f.name).read().strip().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 10:
+                continue
+            try:
+                util = float(r[9])
+                mx = float(r[2])
+                if util > 0:
+                    sm.append(float(r[1]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(rows), "samples_under_load": len(sm)}
+
+
+def solve_model(mb, p, precision, tol, device):
+    m = mb.Model.from_arrays(p.coords, p.conn, p.young, p.poisson, p.fixed, p.imposed, p.loads,
+                             (p.p_elem, p.p_face, p.p_value))
+    m.with_solver(mb.SolverKind.ITERATIVE).with_tolerance(tol).with_precision(precision)
+    return m
+
+
+def time_handle(torch, h, steps, warmup, L):
+    """W untimed and K timed steps of refactor + solve on device-resident inputs; CUDA events on
+    the library's stream. Returns (ms per step, last info, kernel launches per step)."""
+    stream = torch.cuda.ExternalStream(h.stream)
+    for _ in range(warmup):
+        L.maille_gpu_refactor(h._h, None, None)
+        h.solve()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0 = L.maille_gpu_kernel_launches()
+    start.record(stream)
+    info = None
+    for _ in range(steps):
+        s = L.maille_gpu_refactor(h._h, None, None)
+        if s != 0:
+            raise RuntimeError("refactor failed: " + L.maille_gpu_last_error().decode())
+        r = h._L  # solve without downloading the results (device-resident)
+        from maille_b200._lib import ElasticResult
+        res = ElasticResult()
+        s = r.maille_gpu_solve(h._h, None, ctypes.byref(res))
+        if s != 0:
+            raise RuntimeError("solve failed: " + L.maille_gpu_last_error().decode())
+        info = {k: getattr(res, k) for k, _ in ElasticResult._fields_
+                if k not in ("u", "reactions", "gauss_stress", "von_mises")}
+    end.record(stream)
+    end.synchronize()
+    launches = (L.maille_gpu_kernel_launches() - k0) / steps
+    return start.elapsed_time(end) / steps, info, launches
+
+
+def spmv_roofline(torch, h, L, precision, blocks, nb, reps=50):
+    """Average duration of the PCG SpMV kernel over `reps` launches (CUDA events on the
+    library's stream) and its algorithmic bytes: per block 9 values + one int32 column index,
+    per row one int64 row pointer, the vector read once and the result written once."""
+    stream = torch.cuda.ExternalStream(h.stream)
+    L.maille_gpu_spmv_device(h._h, precision, 5)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    L.maille_gpu_spmv_device(h._h, precision, reps)
+    end.record(stream)
+    end.synchronize()
+    ms = start.elapsed_time(end) / reps
+    vb = 4 if precision == 1 else 8
+    n = 3 * nb
+    bytes_ = blocks * (9 * vb + 4) + (nb + 1) * 8 + 2 * n * vb
+    return ms, bytes_
+
+
+def cpu_baseline(p, tol, iterations_needed, max_iter=5):
+    """The CPU oracle (single-thread restatement of the reference path) on the full workload:
+    element integration + assembly + RCM + IC(0) + `max_iter` PCG iterations timed, the PCG part
+    scaled to the oracle's iteration count at `tol` (from its recorded full run)."""
+    import oracle
+    r = oracle.model_solve(p, solver=2, tol=tol, max_iter=max_iter)
+    per_iter = r["ms_solve"] / max(1, r["iterations"])
+    total_ms = r["ms_setup"] + r["ms_factor"] + per_iter * iterations_needed
+    return {"value": p.free_dofs / (total_ms / 1000.0), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": (f"oracle on the full workload: setup {r['ms_setup']:.0f} ms + IC(0) "
+                       f"{r['ms_factor']:.0f} ms + {r['iterations']} PCG iterations timed "
+                       f"({per_iter:.1f} ms each), PCG scaled to the oracle's {iterations_needed} "
+                       f"iterations to tol {tol:g} (tests/golden summary)"),
+            "ms_full_solve_estimate": total_ms}
+
+
+def oracle_iterations(tol):
+    path = os.path.join(ROOT, "tests", "golden", f"tet10_40_oracle_tol{tol:.0e}.json")
+    if os.path.exists(path):
+        return json.load(open(path))["iterations"], path
+    return None, path
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from maille_b200 import meshgen as mg
+    p = mg.mixed_tet10(args.cells)
+    need, path = oracle_iterations(args.tol)
+    if need is None:
+        print(json.dumps({"impl": "reference", "unavailable": f"no oracle iteration record {path}"}))
+        return
+    small = mg.mixed_tet10(4)
+    import oracle
+    for _ in range(args.warmup):  # untimed warm-up on a small mesh of the same family
+        oracle.model_solve(small, solver=2, tol=args.tol)
+    vals = []
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(p, args.tol, need))
+    value = statistics.median(v["value"] for v in vals)
+    ms = p.free_dofs / value * 1000.0
+    cb = dict(vals[0])
+    cb["value"] = value
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"tet10_{args.cells}^3_lognormal_mixed", "free_dofs": p.free_dofs,
+                   "tol": args.tol},
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def run_ours(args):
+    import torch
+    import maille_b200 as mb
+    from maille_b200 import meshgen as mg
+    from maille_b200._lib import MAILLE_FP64, MAILLE_MIXED, ElasticResult
+    from maille_b200.model import problem_struct, face_pressure_loads
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    L = mb._lib.load()
+    p = mg.mixed_tet10(args.cells)
+    f = face_pressure_loads(p.coords, p.conn, list(zip(p.p_elem, p.p_face, p.p_value)))
+    p.loads = f
+    p.p_elem, p.p_face, p.p_value = p.p_elem[:0], p.p_face[:0], p.p_value[:0]
+
+    # tight FP64 reference solution (untimed) for the accuracy check
+    ref = solve_model(mb, p, MAILLE_FP64, 1e-13, local).solve(device=local)
+    u_ref = ref.displacements
+
+    hm = mb.SolverHandle(solve_model(mb, p, MAILLE_MIXED, args.tol, local), device=local)
+    clocks = Clocks(local)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ms_mixed, info_m, launches = time_handle(torch, hm, args.steps, args.warmup, L)
+    clk = clocks.stop()
+    mixed_field = hm.solve()
+    err_mixed = float(np.linalg.norm(mixed_field.displacements - u_ref) / np.linalg.norm(u_ref))
+
+    # max over ranks of the per-step time
+    if world > 1:
+        t = torch.tensor([ms_mixed], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_mixed = float(t.item())
+    free = p.free_dofs
+    value = world * free / (ms_mixed / 1000.0)
+
+    # SpMV roofline (FP32 SpMV of the inner PCG, and the FP64 SpMV of the refinement)
+    hbm, peak_kind = peaks()
+    ms32, bytes32 = spmv_roofline(torch, hm, L, MAILLE_MIXED, info_m["blocks"], info_m["block_rows"])
+    ms64, bytes64 = spmv_roofline(torch, hm, L, MAILLE_FP64, info_m["blocks"], info_m["block_rows"])
+    gbs32, gbs64 = bytes32 / ms32 / 1e6, bytes64 / ms64 / 1e6
+    hm.close()
+
+    plain = None
+    if not args.no_plain:
+        hp = mb.SolverHandle(solve_model(mb, p, MAILLE_FP64, args.tol, local), device=local)
+        ms_plain, info_p, _ = time_handle(torch, hp, args.steps, max(1, args.warmup - 1), L)
+        plain_field = hp.solve()
+        hp.close()
+        if world > 1:
+            t = torch.tensor([ms_plain], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms_plain = float(t.item())
+        plain = {"value": world * free / (ms_plain / 1000.0), "ms_per_step": ms_plain,
+                 "iterations": info_p["iterations"],
+                 "rel_err_vs_fp64": float(np.linalg.norm(plain_field.displacements - u_ref) / np.linalg.norm(u_ref)),
+                 "ms_assembly": info_p["ms_assembly"], "ms_factor": info_p["ms_factor"],
+                 "ms_solve": info_p["ms_solve"]}
+
+    # end to end through the C ABI: host buffers (pinned), create + solve + results + destroy
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    coords, conn, young, poisson = pin(p.coords), pin(p.conn.astype(np.int64)), pin(p.young), pin(p.poisson)
+    fixed, imposed, floads = pin(p.fixed), pin(p.imposed), pin(f)
+    prob, keep = problem_struct(coords, conn, young, poisson, fixed, imposed, floads, args.tol,
+                                10000, MAILLE_MIXED, 0, local)
+    ng = 4
+    outs = dict(u=pin(np.zeros(3 * p.n_nodes)), r=pin(np.zeros(3 * p.n_nodes)),
+                g=pin(np.zeros(p.n_elems * ng * 9)), vm=pin(np.zeros(p.n_elems * ng)))
+    from maille_b200._lib import ptr, _d
+    res = ElasticResult(u=ptr(outs["u"], _d), reactions=ptr(outs["r"], _d),
+                        gauss_stress=ptr(outs["g"], _d), von_mises=ptr(outs["vm"], _d))
+    assert L.maille_gpu_elastic_solve(ctypes.byref(prob), ctypes.byref(res)) == 0
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s = L.maille_gpu_elastic_solve(ctypes.byref(prob), ctypes.byref(res))
+        if s != 0:
+            raise RuntimeError(L.maille_gpu_last_error().decode())
+    e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = sum(a.nbytes for a in (coords, conn, young, poisson, fixed, imposed, floads))
+    d2h = sum(a.nbytes for a in outs.values())
+    e2e = {"value": world * free / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+           "phases_ms": {k: getattr(res, k) for k in ("ms_setup", "ms_upload", "ms_assembly",
+                                                      "ms_factor", "ms_solve", "ms_post",
+                                                      "ms_download")}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        need, path = oracle_iterations(args.tol)
+        if need is not None:
+            cpu = cpu_baseline(p, args.tol, need)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic",
+        "config": {"workload": f"tet10_{args.cells}^3_lognormal_mixed", "free_dofs": free,
+                   "tol": args.tol, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (matrices > 1 GB)", "ordering": "multicolor",
+                   "levels": info_m["levels"], "blocks": info_m["blocks"]},
+        "accuracy": {"rel_err_vs_fp64": err_mixed, "target": 1e-8, "ok": err_mixed <= 1e-8},
+        "mixed": {"iterations": info_m["iterations"], "outer": info_m["outer_iterations"],
+                  "ms_assembly": info_m["ms_assembly"], "ms_factor": info_m["ms_factor"],
+                  "ms_solve": info_m["ms_solve"], "ms_post": info_m["ms_post"]},
+        "plain_fp64": plain,
+        "speedup_mixed_vs_plain": (plain["ms_per_step"] / ms_mixed) if plain else None,
+        "roofline": {"bound": "hbm", "kernel": "k_spmv_pcg<float> (3x3-block CSR SpMV, FP32)",
+                     "achieved": gbs32, "peak": hbm, "unit": "GB/s", "frac": gbs32 / hbm,
+                     "peak_kind": peak_kind, "bytes_per_launch": bytes32, "ms_per_launch": ms32,
+                     "traffic": None},
+        "spmv_fp64": {"achieved": gbs64, "frac": gbs64 / hbm, "bytes_per_launch": bytes64,
+                      "ms_per_launch": ms64},
+        "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

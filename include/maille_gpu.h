@@ -137,6 +137,25 @@ int32_t maille_gpu_solve(MailleGpuHandle* h, const double* f, MailleElasticResul
  * No counterpart in the reference (it has no gradients). */
 int32_t maille_gpu_backward(MailleGpuHandle* h, const double* dJdu, double* dJdE, double* lambda);
 
+/* Numeric refactorisation on the handle's topology: new per-element materials ([n_elems] each,
+ * NULL keeps the current ones), then element integration, assembly and IC(0) again, as the
+ * reference rebuilds FreeSystem when the matrix changes (model.rs:1011). The ordering, pattern
+ * and scatter map are reused; the next solve uses the new matrix. */
+int32_t maille_gpu_refactor(MailleGpuHandle* h, const double* young, const double* poisson);
+
+/* y = K x with the assembled free-DOF matrix (Csr::multiply, iterative.rs:131-142): x and y are
+ * [3 n_nodes] in the caller's numbering; x is read at free DOFs, y is 0 at fixed DOFs. */
+int32_t maille_gpu_multiply(MailleGpuHandle* h, const double* x, double* y);
+
+/* Enqueues `count` launches of the PCG's 3x3-block SpMV kernel on the handle's device vectors
+ * and stream (precision MAILLE_FP64 or MAILLE_MIXED for the FP32 matrix), without waiting: for
+ * timing the kernel with events on maille_gpu_stream(). No counterpart in the reference. */
+int32_t maille_gpu_spmv_device(MailleGpuHandle* h, int32_t precision, int32_t count);
+
+/* Kernels this library has launched in the process (a CUDA graph launch adds its kernel nodes).
+ * No counterpart in the reference. */
+int64_t maille_gpu_kernel_launches(void);
+
 /* Raise (1) or clear (0) the cancel flag; checked between PCG iteration chunks. Safe to call
  * from another thread while a solve runs (the Observer / Flow::Stop role, model.rs:1203-1218). */
 void maille_gpu_cancel(MailleGpuHandle* h, int32_t flag);

@@ -61,6 +61,10 @@ SIGNATURES = {
     "maille_gpu_cancel": ([ctypes.c_void_p, ctypes.c_int32], None),
     "maille_gpu_stream": ([ctypes.c_void_p], ctypes.c_void_p),
     "maille_gpu_destroy": ([ctypes.c_void_p], None),
+    "maille_gpu_refactor": ([ctypes.c_void_p, _d, _d], ctypes.c_int32),
+    "maille_gpu_multiply": ([ctypes.c_void_p, _d, _d], ctypes.c_int32),
+    "maille_gpu_spmv_device": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
+    "maille_gpu_kernel_launches": ([], ctypes.c_int64),
     "maille_gpu_face_pressure_loads": ([ctypes.c_int64, _d, ctypes.c_int32, ctypes.c_int64, _i64,
                                         ctypes.c_int64, _i64, _i32, _d, _d], ctypes.c_int32),
 }

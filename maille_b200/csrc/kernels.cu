@@ -3,11 +3,15 @@
 // Tensor cores stay off on purpose: no step is a dense contraction. Every kernel here is
 // HBM-bandwidth bound except the element integration (FP64 FMA).
 
+#include <atomic>
 #include <cmath>
 
 #include "kernels.cuh"
 
 namespace maille {
+
+// kernels launched by this library since load (graph launches add their kernel nodes)
+std::atomic<long long> g_kernel_launches{0};
 namespace {
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -890,6 +894,7 @@ void ensure_consts() {
 }  // namespace
 
 void launch_elem_stiffness(int npe, const ElemIn& in, double* ke_up, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     ensure_consts();
     if (npe == 4)
         k_elem_stiffness<4><<<(unsigned)((in.ne + Tet<4>::G - 1) / Tet<4>::G), kThreads, 0, st>>>(in, ke_up);
@@ -900,12 +905,14 @@ void launch_elem_stiffness(int npe, const ElemIn& in, double* ke_up, cudaStream_
 void launch_assemble(const Pattern& pt, int64_t nl, const int64_t* lslot, const int32_t* lrow,
                      const int64_t* lptr, const uint32_t* contrib, const double* ke_up, double* K,
                      cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_assemble<<<blocks_for(nl, kThreads, INT32_MAX), kThreads, 0, st>>>(pt, nl, lslot, lrow, lptr,
                                                                        contrib, ke_up, K);
 }
 
 void launch_factor_level(const Pattern& pt, int32_t r0, int32_t r1, const double* K, double* F,
                          double shift, int32_t* fail, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     const int64_t rows = r1 - r0;
     k_factor<<<blocks_for(rows, kWarps, INT32_MAX), kThreads, 0, st>>>(pt, r0, r1, K, F, shift, fail);
 }
@@ -913,6 +920,7 @@ void launch_factor_level(const Pattern& pt, int32_t r0, int32_t r1, const double
 template <typename T>
 void launch_spmv_pcg(const Pattern& pt, const T* K, const T* p, T* ap, PcgScalars* s,
                      double* partials, int grid, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_spmv_pcg<T><<<grid, kThreads, 0, st>>>(pt, K, p, ap, s, partials);
 }
 
@@ -920,6 +928,7 @@ template <typename T>
 void launch_fwd(const Pattern& pt, int32_t r0, int32_t r1, int level, int nlevels, const T* F,
                 T* r, T* y, T* x, const T* p, const T* ap, PcgScalars* s, double* partials,
                 double* lvl_total, int grid, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_fwd<T><<<grid, kThreads, 0, st>>>(pt, r0, r1, level, nlevels, F, r, y, x, p, ap, s, partials,
                                         lvl_total);
 }
@@ -928,11 +937,13 @@ template <typename T>
 void launch_bwd(const Pattern& pt, int32_t r0, int32_t r1, int level, const T* F, const T* r,
                 T* z, PcgScalars* s, double* partials, double* lvl_total, int nlevels, int grid,
                 cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_bwd<T><<<grid, kThreads, 0, st>>>(pt, r0, r1, level, nlevels, F, r, z, s, partials, lvl_total);
 }
 
 template <typename T>
 void launch_pupdate(int64_t n, const T* z, T* p, PcgScalars* s, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_pupdate<T><<<blocks_for(n, kThreads, 148 * 16), kThreads, 0, st>>>(n, z, p, s);
 }
 
@@ -956,49 +967,59 @@ template void launch_pupdate<float>(int64_t, const float*, float*, PcgScalars*, 
 void launch_residual64(const Pattern& pt, const double* K, const double* b, const double* u,
                        double* r, double* partials, unsigned int* ticket, double* out_sum,
                        int grid, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_residual64<<<grid, kThreads, 0, st>>>(pt, K, b, u, r, partials, ticket, out_sum);
 }
 
 void launch_norm2(int64_t n, const double* v, double* partials, unsigned int* ticket,
                   double* out_sum, int grid, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_norm2<double><<<grid, kThreads, 0, st>>>(n, v, partials, ticket, out_sum);
 }
 
 void launch_norm2_f(int64_t n, const float* v, double* partials, unsigned int* ticket,
                     double* out_sum, int grid, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_norm2<float><<<grid, kThreads, 0, st>>>(n, v, partials, ticket, out_sum);
 }
 
 void launch_scale_to_float(int64_t n, const double* src, const double* norm2, float* dst,
                            cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_scale_to_float<<<blocks_for(n, kThreads, 148 * 16), kThreads, 0, st>>>(n, src, norm2, dst);
 }
 
 void launch_accumulate(int64_t n, const float* d, const double* norm2, double* u, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_accumulate<<<blocks_for(n, kThreads, 148 * 16), kThreads, 0, st>>>(n, d, norm2, u);
 }
 
 void launch_to_float(int64_t n, const double* src, float* dst, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_to_float<<<blocks_for(n, kThreads, 148 * 32), kThreads, 0, st>>>(n, src, dst);
 }
 
 void launch_pcg_init(PcgScalars* s, double tol, int32_t max_iter, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_pcg_init<<<1, 1, 0, st>>>(s, tol, max_iter);
 }
 
 void launch_build_rhs(int32_t nb, const int32_t* perm, const uint8_t* fixmask, const double* f,
                       const double* coupling, double* b, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_build_rhs<<<blocks_for(3 * (int64_t)nb, kThreads, INT32_MAX), kThreads, 0, st>>>(nb, perm, fixmask, f, coupling, b);
 }
 
 void launch_gather_u(int64_t n_nodes, const int32_t* inv, const uint8_t* fixed,
                      const double* imposed, const double* x, double* u, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_gather_u<<<blocks_for(3 * n_nodes, kThreads, INT32_MAX), kThreads, 0, st>>>(n_nodes, inv, fixed, imposed, x, u);
 }
 
 void launch_elem_apply(int npe, int64_t nlist, const int32_t* list, const int32_t* conn,
                        const double* ke_up, const double* u, double* ye, cudaStream_t st) {
     if (nlist <= 0) return;
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_elem_apply<<<blocks_for(nlist * 3 * npe, kThreads, INT32_MAX), kThreads, 0, st>>>(npe, nlist, list, conn, ke_up, u, ye);
 }
 
@@ -1006,6 +1027,7 @@ void launch_node_gather(int npe, int64_t nnodes, const int32_t* nodes, const int
                         const int32_t* inc, const int32_t* elem_slot, const double* ye, double* y,
                         cudaStream_t st) {
     if (nnodes <= 0) return;
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_node_gather<<<blocks_for(nnodes, kThreads, INT32_MAX), kThreads, 0, st>>>(npe, nnodes, nodes, inc_ptr, inc, elem_slot, ye, y);
 }
 
@@ -1013,11 +1035,13 @@ void launch_reactions(int64_t n_nodes, const int32_t* nodes, int64_t nnodes, con
                       const double* y, const double* f, double* react, cudaStream_t st) {
     (void)n_nodes;
     if (nnodes <= 0) return;
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_reactions<<<blocks_for(3 * nnodes, kThreads, INT32_MAX), kThreads, 0, st>>>(nodes, nnodes, fixed, y, f, react);
 }
 
 void launch_stresses(int npe, const ElemIn& in, const double* u, double* gauss, double* vm,
                      cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     ensure_consts();
     const int ng = npe == 4 ? 1 : 4;
     if (npe == 4)
@@ -1029,6 +1053,7 @@ void launch_stresses(int npe, const ElemIn& in, const double* u, double* gauss, 
 void launch_adjoint_grad(int npe, int64_t ne, const int32_t* conn, const double* ke_up,
                          const double* young, const double* lambda, const double* u, double* grad,
                          cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     k_adjoint_grad<<<blocks_for(ne, 128, INT32_MAX), 128, 0, st>>>(npe, ne, conn, ke_up, young, lambda, u, grad);
 }
 

@@ -11,6 +11,7 @@
 // slots, and a final sum in slot order by the last block to finish (ticket counter).
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -19,6 +20,9 @@ namespace maille {
 constexpr int kThreads = 256;       // threads per block of the row kernels
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxLevels = 65536;
+
+// kernels launched by this library since load (a graph launch adds its kernel nodes)
+extern std::atomic<long long> g_kernel_launches;
 
 // Device-resident scalars of one PCG run.
 struct PcgScalars {

@@ -89,10 +89,12 @@ struct MailleGpuHandle {
     double inner_tol = 1e-4;
     int32_t max_outer = 60;
     std::vector<uint8_t> h_fixed;
-    std::vector<double> h_f, h_imposed;
+    std::vector<double> h_f, h_f0, h_imposed;
     bool any_imposed = false;
     // device: inputs (caller numbering)
-    double *coords = nullptr, *young = nullptr, *poisson = nullptr, *imposed = nullptr, *f = nullptr;
+    double *coords = nullptr, *young = nullptr, *poisson = nullptr, *imposed = nullptr, *f = nullptr,
+           *f0 = nullptr;  // f: loads of the current solve, f0: the problem's loads
+    const double* f_cur = nullptr;
     int32_t* conn = nullptr;
     uint8_t* fixed = nullptr;
     // device: symbolic
@@ -112,6 +114,7 @@ struct MailleGpuHandle {
     double *u_full = nullptr, *y_full = nullptr, *ye = nullptr, *gauss = nullptr, *vm = nullptr,
            *react = nullptr, *lambda_full = nullptr, *grad = nullptr;
     PcgScalars* scal = nullptr;
+    PcgScalars* spmv_scal = nullptr;
     PcgScalars* h_scal = nullptr;  // pinned
     double* partials = nullptr;
     double* lvl_total = nullptr;
@@ -123,6 +126,7 @@ struct MailleGpuHandle {
     std::vector<int> lvl_grid;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [0] FP64, [1] FP32
     int graph_iters = 8;
+    long long graph_kernels = 0;
     std::atomic<int> cancel{0};
     double shift = 0.0;
     bool solved = false;
@@ -144,11 +148,11 @@ MailleGpuHandle::~MailleGpuHandle() {
     cudaSetDevice(device);
     for (auto& g : graph)
         if (g) cudaGraphExecDestroy(g);
-    void* bufs[] = {coords, young, poisson, imposed, f, conn, fixed, perm, inv, col, lrow, fixmask,
+    void* bufs[] = {coords, young, poisson, imposed, f, f0, conn, fixed, perm, inv, col, lrow, fixmask,
                     row_ptr, diag, tpos, lslot, lptr, contrib, inc_ptr, inc, belem, bnodes,
                     elem_slot, ke, K, F, K32, F32, v64.b, v64.x, v64.r, v64.z, v64.p, v64.ap,
                     v32.b, v32.x, v32.r, v32.z, v32.p, v32.ap, rr64, u_full, y_full, ye, gauss, vm,
-                    react, lambda_full, grad, scal, partials, lvl_total, dsum, dticket, dfail};
+                    react, lambda_full, grad, scal, spmv_scal, partials, lvl_total, dsum, dticket, dfail};
     for (void* p : bufs) dfree(p);
     if (h_scal) cudaFreeHost(h_scal);
     if (h_sum) cudaFreeHost(h_sum);
@@ -231,15 +235,19 @@ int32_t run_pcg(MailleGpuHandle* h, const T* K, const T* F, PcgVecs<T>& v, doubl
     // the graph bakes in the vector and matrix pointers of this precision
     if (!h->graph[gi]) {
         cudaGraph_t g;
+        const long long before = g_kernel_launches.load();
         CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
         for (int k = 0; k < h->graph_iters; ++k) enqueue_iteration<T>(h, K, F, v);
         CK(cudaStreamEndCapture(h->st, &g));
+        h->graph_kernels = g_kernel_launches.load() - before;
+        g_kernel_launches.store(before);  // captured, not launched
         CK(cudaGraphInstantiate(&h->graph[gi], g, 0));
         cudaGraphDestroy(g);
     }
     int32_t status = MAILLE_OK;
     for (;;) {
         CK(cudaGraphLaunch(h->graph[gi], h->st));
+        g_kernel_launches.fetch_add(h->graph_kernels);
         CK(cudaMemcpyAsync(h->h_scal, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, h->st));
         CK(cudaStreamSynchronize(h->st));
         const PcgScalars& s = *h->h_scal;
@@ -316,7 +324,7 @@ void build_rhs(MailleGpuHandle* h) {
                            h->elem_slot, h->ye, h->y_full, h->st);
         coupling = h->y_full;
     }
-    launch_build_rhs(h->sym.nb, h->perm, h->fixmask, h->f, coupling, h->v64.b, h->st);
+    launch_build_rhs(h->sym.nb, h->perm, h->fixmask, h->f_cur, coupling, h->v64.b, h->st);
 }
 
 int32_t factorize(MailleGpuHandle* h, Error& err) {
@@ -337,6 +345,25 @@ int32_t factorize(MailleGpuHandle* h, Error& err) {
     }
     err = {MAILLE_SINGULAR, "IC(0) failed with every diagonal shift (Singular)"};
     return MAILLE_SINGULAR;
+}
+
+// Element integration + scatter-reduce assembly + IC(0) (+ FP32 copies), all on the device.
+int32_t numeric_phase(MailleGpuHandle* h, Error& err) {
+    const Symbolic& s = h->sym;
+    ElemIn in{h->n_elems, h->coords, h->conn, h->young, h->poisson};
+    launch_elem_stiffness(h->npe, in, h->ke, h->st);
+    launch_assemble(h->pattern(), (int64_t)s.lslot.size(), h->lslot, h->lrow, h->lptr, h->contrib,
+                    h->ke, h->K, h->st);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->ev[2], h->st));
+    if (factorize(h, err) != MAILLE_OK) return err.status;
+    if (h->precision == MAILLE_MIXED) {
+        launch_to_float((int64_t)s.blocks * 9, h->K, h->K32, h->st);
+        launch_to_float((int64_t)s.blocks * 9, h->F, h->F32, h->st);
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(h->ev[3], h->st));
+    return MAILLE_OK;
 }
 
 int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, MailleElasticResult* res) {
@@ -393,7 +420,10 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         h->young = dupload(p->young, p->n_elems, st);
         h->poisson = dupload(p->poisson, p->n_elems, st);
         h->imposed = dupload(h->h_imposed.data(), n3, st);
-        h->f = dupload(h->h_f.data(), n3, st);
+        h->f0 = dupload(h->h_f.data(), n3, st);
+        h->f = dalloc<double>(n3);
+        h->f_cur = h->f0;
+        h->h_f0 = h->h_f;
         h->fixed = dupload(h->h_fixed.data(), n3, st);
         // symbolic
         h->perm = dupload(s.perm.data(), s.perm.size(), st);
@@ -457,20 +487,7 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         const int per_iter = 2 * s.levels + 2;
         h->graph_iters = std::max(1, std::min(h->graph_iters, 4000 / per_iter));
         CK(cudaEventRecord(h->ev[1], st));
-        // element integration + assembly
-        ElemIn in{p->n_elems, h->coords, h->conn, h->young, h->poisson};
-        launch_elem_stiffness(h->npe, in, h->ke, st);
-        launch_assemble(h->pattern(), (int64_t)s.lslot.size(), h->lslot, h->lrow, h->lptr,
-                        h->contrib, h->ke, h->K, st);
-        CK(cudaGetLastError());
-        CK(cudaEventRecord(h->ev[2], st));
-        if (factorize(h.get(), err) != MAILLE_OK) return fail(err);
-        if (h->precision == MAILLE_MIXED) {
-            launch_to_float((int64_t)s.blocks * 9, h->K, h->K32, st);
-            launch_to_float((int64_t)s.blocks * 9, h->F, h->F32, st);
-            CK(cudaGetLastError());
-        }
-        CK(cudaEventRecord(h->ev[3], st));
+        if (numeric_phase(h.get(), err) != MAILLE_OK) return fail(err);
         CK(cudaStreamSynchronize(st));
         if (res) {
             res->ms_setup = t_setup1 - t_setup0;
@@ -499,6 +516,10 @@ int32_t solve_impl(MailleGpuHandle* h, const double* f, MailleElasticResult* res
                 if (!std::isfinite(f[k])) return fail({MAILLE_INVALID_INPUT, "non-finite load"});
             std::memcpy(h->h_f.data(), f, n3 * sizeof(double));
             CK(cudaMemcpyAsync(h->f, f, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+            h->f_cur = h->f;
+        } else {
+            h->h_f = h->h_f0;
+            h->f_cur = h->f0;
         }
         CK(cudaEventRecord(h->ev[4], st));
         build_rhs(h);
@@ -575,7 +596,7 @@ int32_t solve_impl(MailleGpuHandle* h, const double* f, MailleElasticResult* res
             launch_node_gather(h->npe, (int64_t)s.bnodes.size(), h->bnodes, h->inc_ptr, h->inc,
                                h->elem_slot, h->ye, h->y_full, st);
             launch_reactions(h->n_nodes, h->bnodes, (int64_t)s.bnodes.size(), h->fixed, h->y_full,
-                             h->f, h->react, st);
+                             h->f_cur, h->react, st);
         }
         const int ng = gauss_points(h->npe);
         if (!h->gauss) {
@@ -747,6 +768,84 @@ int32_t maille_gpu_elastic_solve(const MailleElasticProblem* problem, MailleElas
     delete h;
     return s;
 }
+
+int32_t maille_gpu_refactor(MailleGpuHandle* h, const double* young, const double* poisson) {
+    g_last_error.clear();
+    if (!h) return fail({MAILLE_INVALID_INPUT, "null handle"});
+    for (int64_t e = 0; e < h->n_elems; ++e) {
+        const double E = young ? young[e] : 1.0, nu = poisson ? poisson[e] : 0.0;
+        if (!std::isfinite(E) || !std::isfinite(nu) || E <= 0.0 || nu <= -1.0 || nu >= 0.5)
+            return fail({MAILLE_INVALID_INPUT, "invalid material of element " + std::to_string(e)});
+    }
+    try {
+        CK(cudaSetDevice(h->device));
+        if (young)
+            CK(cudaMemcpyAsync(h->young, young, h->n_elems * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        if (poisson)
+            CK(cudaMemcpyAsync(h->poisson, poisson, h->n_elems * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        Error err{MAILLE_OK, ""};
+        if (numeric_phase(h, err) != MAILLE_OK) return fail(err);
+        h->solved = false;
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+    return MAILLE_OK;
+}
+
+int32_t maille_gpu_spmv_device(MailleGpuHandle* h, int32_t precision, int32_t count) {
+    g_last_error.clear();
+    if (!h || count < 0) return fail({MAILLE_INVALID_INPUT, "null handle or negative count"});
+    if (precision == MAILLE_MIXED && !h->K32)
+        return fail({MAILLE_INVALID_INPUT, "the handle holds no FP32 matrix"});
+    try {
+        CK(cudaSetDevice(h->device));
+        if (!h->spmv_scal) {
+            h->spmv_scal = dalloc<PcgScalars>(1);
+            CK(cudaMemsetAsync(h->spmv_scal, 0, sizeof(PcgScalars), h->st));
+        }
+        for (int32_t k = 0; k < count; ++k) {
+            if (precision == MAILLE_MIXED)
+                launch_spmv_pcg<float>(h->pattern(), h->K32, h->v32.p, h->v32.ap, h->spmv_scal,
+                                       h->partials, h->spmv_grid, h->st);
+            else
+                launch_spmv_pcg<double>(h->pattern(), h->K, h->v64.p, h->v64.ap, h->spmv_scal,
+                                        h->partials, h->spmv_grid, h->st);
+        }
+        CK(cudaGetLastError());
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+    return MAILLE_OK;
+}
+
+int32_t maille_gpu_multiply(MailleGpuHandle* h, const double* x, double* y) {
+    g_last_error.clear();
+    if (!h || !x || !y) return fail({MAILLE_INVALID_INPUT, "null argument"});
+    try {
+        CK(cudaSetDevice(h->device));
+        const int64_t n3 = 3 * h->n_nodes;
+        CK(cudaMemcpyAsync(h->y_full, x, n3 * sizeof(double), cudaMemcpyHostToDevice, h->st));
+        launch_build_rhs(h->sym.nb, h->perm, h->fixmask, h->y_full, nullptr, h->v64.p, h->st);
+        if (!h->spmv_scal) {
+            h->spmv_scal = dalloc<PcgScalars>(1);
+            CK(cudaMemsetAsync(h->spmv_scal, 0, sizeof(PcgScalars), h->st));
+        }
+        launch_spmv_pcg<double>(h->pattern(), h->K, h->v64.p, h->v64.ap, h->spmv_scal, h->partials,
+                                h->spmv_grid, h->st);
+        CK(cudaMemsetAsync(h->u_full, 0, n3 * sizeof(double), h->st));
+        CK(cudaMemsetAsync(h->react, 0, n3 * sizeof(double), h->st));
+        launch_gather_u(h->n_nodes, h->inv, h->fixed, h->react, h->v64.ap, h->y_full, h->st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(y, h->y_full, n3 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        h->solved = false;
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+    return MAILLE_OK;
+}
+
+int64_t maille_gpu_kernel_launches(void) { return (int64_t)g_kernel_launches.load(); }
 
 int32_t maille_gpu_face_pressure_loads(int64_t n_nodes, const double* coords, int32_t npe,
                                        int64_t n_elems, const int64_t* conn, int64_t n_press,

@@ -58,6 +58,8 @@ def lib():
             ctypes.c_int64, _i64, _i32, _d, ctypes.c_int, ctypes.c_double, ctypes.c_int64, _i64,
             _d, _d, _d, _d, _d, _d]
         L.oracle_model_solve.restype = ctypes.c_int
+        L.oracle_energy.argtypes = [ctypes.c_int64, _d, ctypes.c_int, ctypes.c_int64, _i64, _d, _d, _d]
+        L.oracle_energy.restype = ctypes.c_double
         L.oracle_nodal_stresses.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int64, _i64, _d, _d]
         _lib = L
     return _lib
@@ -183,6 +185,16 @@ def model_solve(prob, solver: int = 2, tol: float = 1e-12, max_iter: int = 10000
     return dict(status=s, u=u, reactions=r, gauss=g, von_mises=vm, f=f, iterations=int(info[0]),
                 rel_residual=info[1], shift=info[2], free_dofs=int(info[3]), nnz=int(info[4]),
                 ms_setup=info[5], ms_factor=info[6], ms_solve=info[7], wall_s=wall)
+
+
+def energy(prob, v):
+    """v^T K v summed element by element."""
+    coords = _c(prob.coords, np.float64)
+    conn = _c(prob.conn, np.int64)
+    vv = _c(v, np.float64)
+    return lib().oracle_energy(coords.shape[0], _p(coords, _d), conn.shape[1], conn.shape[0],
+                               _p(conn, _i64), _p(_c(prob.young, np.float64), _d),
+                               _p(_c(prob.poisson, np.float64), _d), _p(vv, _d))
 
 
 def nodal_stresses(prob, gauss):

@@ -965,6 +965,28 @@ int oracle_model_solve(int64_t n_nodes, const double* coords, int npe, int64_t n
     return OK;
 }
 
+// Energy v^T K v = sum_e v_e^T K_e v_e of a displacement-like vector v (3 n_nodes), with the
+// element matrices of element_stiffness (assembly.rs:64-79). Used to measure energy-norm errors.
+double oracle_energy(int64_t n_nodes, const double* coords, int npe, int64_t n_elems,
+                     const int64_t* conn, const double* young, const double* poisson,
+                     const double* v) {
+    SolidMesh mesh{(size_t)n_nodes, (size_t)n_elems, npe, coords, conn, young, poisson};
+    const int m = 3 * npe;
+    Vec ke((size_t)m * m);
+    double total = 0.0;
+    for (size_t e = 0; e < mesh.n_elems; ++e) {
+        mesh.stiffness(e, ke.data());
+        double ve[30];
+        for (int l = 0; l < m; ++l) ve[l] = v[3 * (size_t)conn[e * npe + l / 3] + l % 3];
+        for (int r = 0; r < m; ++r) {
+            double s = 0.0;
+            for (int c = 0; c < m; ++c) s += ke[(size_t)r * m + c] * ve[c];
+            total += ve[r] * s;
+        }
+    }
+    return total;
+}
+
 // nodal_stresses / smooth, results.rs:137-230: Gauss values extrapolated to the element nodes
 // (TET4_EXTRAPOLATION 98, TET10_EXTRAPOLATION 118-132) and averaged. gauss: n_elems*ngp*9 as
 // written above; out: n_nodes*6 (sxx, syy, szz, txy, tyz, txz).

@@ -1,0 +1,194 @@
+"""CPU tests of the C ABI boundary and the host logic: the library loads, exports every symbol
+include/maille_gpu.h declares, validates its inputs before touching a device, and the host-side
+helpers agree with the oracle. No GPU compute runs here."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import cases
+import maille_b200 as mb
+from maille_b200 import _lib, build, meshgen as mg
+from maille_b200.model import problem_struct
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build()
+    return _lib.load()
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "maille_gpu.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(maille_gpu_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(lib):
+    names = header_functions()
+    assert "maille_gpu_elastic_solve" in names and len(names) >= 10
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_build_recipe_targets_sm100a_only():
+    assert "arch=compute_100a,code=sm_100a" in build.FLAGS
+    assert sum("arch=" in f for f in build.FLAGS) == 1
+
+
+def test_version_and_device_count_need_no_gpu(lib):
+    assert b"sm_100a" in lib.maille_gpu_version()
+    assert lib.maille_gpu_device_count() >= 0
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Field offsets of the ctypes structs equal those gcc computes from include/maille_gpu.h."""
+    import subprocess
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "maille_gpu.h"', "int main(void) {"]
+    for cname, py in (("MailleElasticProblem", _lib.ElasticProblem),
+                      ("MailleElasticResult", _lib.ElasticResult)):
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, py in (("MailleElasticProblem", _lib.ElasticProblem),
+                      ("MailleElasticResult", _lib.ElasticResult)):
+        assert got[(cname, "size")] == ctypes.sizeof(py)
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def _solve_status(lib, p):
+    r = _lib.ElasticResult()
+    return lib.maille_gpu_elastic_solve(ctypes.byref(p), ctypes.byref(r))
+
+
+def test_invalid_inputs_are_rejected_before_any_device_work(lib):
+    p0 = mg.plain_tet4(2)
+    good = dict(coords=p0.coords, conn=p0.conn, young=p0.young, poisson=p0.poisson,
+                fixed=p0.fixed, imposed=p0.imposed, f=p0.loads)
+
+    def status(**kw):
+        args = dict(good)
+        args.update(kw)
+        p, keep = problem_struct(**args)
+        return _solve_status(lib, p)
+
+    bad_conn = p0.conn.copy()
+    bad_conn[3, 2] = p0.coords.shape[0] + 5
+    assert status(conn=bad_conn) == _lib.MAILLE_INVALID_INPUT
+    assert "unknown node" in _lib.last_error()
+    coords = p0.coords.copy()
+    coords[1, 0] = np.nan
+    assert status(coords=coords) == _lib.MAILLE_INVALID_INPUT
+    assert status(young=-p0.young) == _lib.MAILLE_INVALID_INPUT
+    f = p0.loads.copy()
+    f[4] = np.inf
+    assert status(f=f) == _lib.MAILLE_INVALID_INPUT
+    assert status(fixed=np.ones_like(p0.fixed)) == _lib.MAILLE_INVALID_INPUT  # nothing free
+    assert lib.maille_gpu_elastic_solve(None, None) == _lib.MAILLE_INVALID_INPUT
+    # wrong element family
+    p, keep = problem_struct(**good)
+    p.nodes_per_elem = 5
+    p.n_elems = p0.conn.size // 5
+    assert _solve_status(lib, p) == _lib.MAILLE_INVALID_INPUT
+
+
+def test_missing_device_is_a_cuda_error_not_a_fallback(lib):
+    if lib.maille_gpu_device_count() > 0:
+        pytest.skip("a device is visible")
+    p0 = mg.plain_tet4(2)
+    p, keep = problem_struct(p0.coords, p0.conn, p0.young, p0.poisson, p0.fixed, p0.imposed,
+                             p0.loads)
+    assert _solve_status(lib, p) == _lib.MAILLE_CUDA_ERROR
+
+
+@pytest.mark.parametrize("quadratic", [False, True])
+def test_face_pressure_helper_matches_the_oracle(lib, oracle_lib, quadratic):
+    p = cases.hydrostatic(quadratic)
+    f = mb.face_pressure_loads(p.coords, p.conn, list(zip(p.p_elem, p.p_face, p.p_value)))
+    r = oracle_lib.model_solve(p, solver=1)
+    assert np.abs(f - r["f"]).max() < 1e-13
+    # resultant: -p * area on each loaded unit face
+    for c in range(3):
+        assert abs(f[c::3].sum() + 50.0) < 1e-12
+
+
+def test_mesh_validation_mirrors_mesh_new():
+    # tests/solid.rs bad_tetrahedra_are_refused_with_their_index
+    nodes = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 0]], float)
+    with pytest.raises(mb.MailleError) as e:
+        mb.Mesh(nodes, [[0, 1, 2, 3], [0, 2, 1, 3]], 210e3, 0.3)
+    assert e.value.kind == "InvertedTetrahedron" and "element 1" in str(e.value)
+    with pytest.raises(mb.MailleError) as e:
+        mb.Mesh(nodes, [[0, 1, 2, 4]], 210e3, 0.3)
+    assert e.value.kind == "DegenerateTetrahedron"
+    q_nodes, q_conn = mg.to_quadratic_tet(nodes[:4], np.array([[0, 1, 2, 3]]))
+    q_nodes[4] += [0.0, 0.1, 0.0]
+    with pytest.raises(mb.MailleError) as e:
+        mb.Mesh(q_nodes, q_conn, 210e3, 0.3)
+    assert e.value.kind == "CurvedTetrahedron"
+    with pytest.raises(mb.MailleError):
+        mb.Mesh(nodes, [[0, 1, 2, 9]], 210e3, 0.3)
+
+
+def test_solver_kind_selection_follows_the_reference():
+    # solve.rs:185-195
+    assert mb.ITERATIVE_FROM == 100_000
+    assert not mb.SolverKind.AUTO.is_iterative(99_999)
+    assert mb.SolverKind.AUTO.is_iterative(100_000)
+    assert mb.SolverKind.ITERATIVE.is_iterative(1)
+    assert not mb.SolverKind.DIRECT.is_iterative(10 ** 7)
+    m = mb.Model.from_arrays(*_small_arrays())
+    with pytest.raises(mb.MailleError) as e:
+        m.solve()  # Auto below the threshold selects the host's skyline solver
+    assert e.value.kind == "DirectSolverOnHost"
+
+
+def _small_arrays():
+    p = mg.plain_tet4(2)
+    return p.coords, p.conn, p.young, p.poisson, p.fixed
+
+
+def test_meshgen_matches_the_reference_mesh_sizes():
+    # box_grid / to_quadratic_tet node and element counts of the benchmark meshes
+    nodes, tets = mg.box_grid((20, 20, 20), (1, 1, 1))
+    assert nodes.shape == (9261, 3) and tets.shape == (48000, 4)
+    n10, c10 = mg.to_quadratic_tet(*mg.box_grid((6, 6, 6), (1, 1, 1)))
+    assert n10.shape[0] == 13 ** 3 and c10.shape == (6 * 216, 10)
+    # every tet is positively oriented and Tet10 mids sit at the edge midpoints
+    e = nodes[tets[:, 1:]] - nodes[tets[:, :1]]
+    assert (np.einsum("ij,ij->i", e[:, 0], np.cross(e[:, 1], e[:, 2])) > 0).all()
+    for k, (a, b) in enumerate(mg.TET10_EDGES):
+        assert np.allclose(n10[c10[:, 4 + k]], 0.5 * (n10[c10[:, a]] + n10[c10[:, b]]))
+    # first-encounter numbering of the mid nodes (the reference's HashMap insertion order)
+    first = c10[:, 4:].ravel()
+    seen = []
+    for v in first:
+        if v not in seen:
+            seen.append(v)
+        if len(seen) > 50:
+            break
+    assert seen == list(range(7 ** 3, 7 ** 3 + len(seen)))
+
+
+def test_workload_generators_are_seeded_and_shaped():
+    a = mg.uniform(3, 5)
+    assert np.array_equal(a, mg.uniform(3, 5)) and (a >= 0).all() and (a < 1).all()
+    z = mg.normal(2, 200000)
+    assert abs(z.mean()) < 0.01 and abs(z.std() - 1) < 0.01
+    p = mg.plain_tet4(20)
+    assert p.free_dofs == 26460 and p.p_elem.size == 800
+    p, rho = mg.simp_tet4(4)
+    assert np.allclose(p.young, 210000 * rho ** 3) and rho.min() >= 0.01 and rho.max() <= 1.0

@@ -1,0 +1,247 @@
+"""GPU parity: the CUDA solve path against the CPU oracle and the reference's analytic checks.
+
+Tolerances (from the solve contract): FP64 displacements and von Mises within 1e-10 relative L2
+of the oracle; the mixed form within 1e-8 relative displacement error of an FP64 oracle
+converged to 1e-14; analytic checks with the reference's own tolerances.
+"""
+import numpy as np
+import pytest
+
+import cases
+import maille_b200 as mb
+from maille_b200 import meshgen as mg
+from maille_b200._lib import (MAILLE_FP64, MAILLE_MIXED, MAILLE_ORDER_MULTICOLOR,
+                              MAILLE_ORDER_RCM)
+
+pytestmark = pytest.mark.gpu
+
+
+def model_of(p, tol=1e-12, precision=MAILLE_FP64, ordering=MAILLE_ORDER_MULTICOLOR,
+             max_iter=10000):
+    m = mb.Model.from_arrays(p.coords, p.conn, p.young, p.poisson, p.fixed, p.imposed, p.loads,
+                             (p.p_elem, p.p_face, p.p_value))
+    m.with_solver(mb.SolverKind.ITERATIVE).with_tolerance(tol).with_precision(precision)
+    m.ordering = ordering
+    m.max_iterations = max_iter
+    return m
+
+
+def solve(p, **kw):
+    return model_of(p, **kw).solve()
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def voigt(g):
+    return np.stack([g[..., 3], g[..., 4], g[..., 5], g[..., 7], g[..., 8], g[..., 6]], -1)
+
+
+# --- the reference's analytic checks through the GPU path -----------------------------------
+
+@pytest.mark.parametrize("quadratic", [False, True])
+def test_uniform_strain_patch_is_exact(gpu, quadratic):
+    # tests/solid.rs:52-116
+    p = cases.patch(quadratic)
+    f = solve(p)
+    assert np.abs(f.displacements.reshape(-1, 3) - cases.uniform_field(p.coords)).max() < 1e-12
+    sigma = cases.d_matrix() @ cases.EPS
+    assert np.abs(voigt(f.stresses) - sigma).max() <= 1e-9 * np.abs(sigma).max()
+
+
+@pytest.mark.parametrize("quadratic", [False, True])
+def test_uniaxial_traction(gpu, quadratic):
+    # tests/solid.rs:118-175
+    L, delta = 4.0, 0.01
+    p = cases.uniaxial(quadratic, L, delta)
+    f = solve(p)
+    strain = delta / L
+    assert np.abs(f.stresses[..., 3] - cases.E * strain).max() <= 1e-9 * cases.E * strain
+    assert np.abs(f.stresses[..., 4]).max() < 1e-9 * cases.E * strain
+    u = f.displacements.reshape(-1, 3)
+    assert np.abs(u[:, 1] + cases.NU * strain * p.coords[:, 1]).max() < 1e-12
+    assert np.abs(u[:, 2] + cases.NU * strain * p.coords[:, 2]).max() < 1e-12
+    pull = f.reactions[0::3][np.abs(p.coords[:, 0] - L) < 1e-12].sum()
+    assert abs(pull - cases.E * strain) <= 1e-9 * cases.E * strain
+
+
+@pytest.mark.parametrize("quadratic", [False, True])
+def test_cube_under_hydrostatic_pressure_shrinks_uniformly(gpu, quadratic):
+    # tests/pressure.rs:194-224
+    p = cases.hydrostatic(quadratic)
+    f = solve(p)
+    strain = -50.0 * (1 - 2 * cases.NU) / cases.E
+    assert np.abs(f.displacements.reshape(-1, 3) - strain * p.coords).max() < 1e-12
+    assert np.abs(f.stresses[..., 3] + 50).max() < 1e-6 and np.abs(f.stresses[..., 6]).max() < 1e-6
+
+
+def test_cube_example_follows_the_analytic_field(gpu):
+    # crates/maille-cli/tests/examples.rs:669-681 on the reference's examples/cube model
+    p = cases.cube_example()
+    u = solve(p).displacements.reshape(-1, 3)
+    x = p.coords
+    assert np.abs(u[:, 0] - 0.01 * x[:, 0]).max() < 1e-12
+    assert np.abs(u[:, 1] + 0.25 * 0.01 * x[:, 1]).max() < 1e-12
+    assert np.abs(u[:, 2] + 0.25 * 0.01 * x[:, 2]).max() < 1e-12
+
+
+def test_tet10_cantilever_matches_beam_theory(gpu):
+    # tests/solid.rs:259-270
+    for n in [(10, 2, 2), (20, 2, 2)]:
+        p, tip = cases.cantilever(n, True)
+        ratio = solve(p).displacements[3 * tip + 2] / cases.timoshenko()
+        assert abs(ratio - 1) < 0.02
+
+
+def test_tet4_cantilever_locks(gpu):
+    # tests/solid.rs:272-279
+    p, tip = cases.cantilever((10, 2, 2), False)
+    coarse = solve(p).displacements[3 * tip + 2] / cases.timoshenko()
+    p, tip = cases.cantilever((20, 4, 4), False)
+    fine = solve(p).displacements[3 * tip + 2] / cases.timoshenko()
+    assert coarse < 0.6 and coarse < fine < 0.95
+
+
+def test_iterative_solution_matches_the_oracle_direct_one(gpu, oracle_lib):
+    # tests/iterative.rs:68-83 with the GPU as the iterative solver
+    p = cases.iterative_cantilever()
+    d = oracle_lib.model_solve(p, solver=1)
+    f = solve(p)
+    gap = lambda a, b: np.abs(a - b).max() / np.abs(b).max()  # noqa: E731
+    assert gap(f.displacements, d["u"]) < 1e-8
+    assert gap(f.reactions, d["reactions"]) < 1e-8
+    assert gap(f.stresses[..., 3], d["gauss"][..., 3]) < 1e-7
+
+
+# --- parity with the oracle on the benchmark configurations (reduced sizes) -----------------
+
+@pytest.mark.parametrize("ordering", [MAILLE_ORDER_MULTICOLOR, MAILLE_ORDER_RCM])
+def test_plain_tet4_config_matches_the_oracle(gpu, oracle_lib, ordering):
+    # Plain FP64 Tet4 20^3, pressure 10 on z = 1, z = 0 clamped, reference tolerance 1e-12
+    p = mg.plain_tet4(20)
+    ref = oracle_lib.model_solve(p, solver=2, tol=1e-12)
+    f = solve(p, tol=1e-12, ordering=ordering)
+    assert f.info["free_dofs"] == 26460
+    assert rel(f.displacements, ref["u"]) < 1e-10
+    assert rel(f.von_mises, ref["von_mises"]) < 1e-10
+    assert rel(f.stresses[..., 3:], ref["gauss"][..., 3:]) < 1e-10
+    assert rel(f.reactions, ref["reactions"]) < 1e-10
+    assert np.array_equal(f.stresses[..., :3], ref["gauss"][..., :3]) or \
+        np.abs(f.stresses[..., :3] - ref["gauss"][..., :3]).max() < 1e-14
+    assert f.info["final_rel_residual"] <= 1e-12
+
+
+def test_plain_tet4_config_tolerance_1e10_with_the_reference_ordering(gpu, oracle_lib):
+    # the config's own tolerance: same ordering family as the reference, same stopping rule
+    p = mg.plain_tet4(20)
+    ref = oracle_lib.model_solve(p, solver=2, tol=1e-10)
+    f = solve(p, tol=1e-10, ordering=MAILLE_ORDER_RCM)
+    assert rel(f.displacements, ref["u"]) < 1e-10
+    assert rel(f.von_mises, ref["von_mises"]) < 1e-10
+
+
+def test_rcm_ordering_takes_the_reference_iteration_count(gpu, oracle_lib):
+    # node RCM + block IC(0) equals the reference's scalar RCM + scalar IC(0) on these meshes
+    for p in (mg.plain_tet4(20), mg.mixed_tet10(12)):
+        ref = oracle_lib.model_solve(p, solver=2, tol=1e-12)
+        f = solve(p, tol=1e-12, ordering=MAILLE_ORDER_RCM)
+        assert abs(f.info["iterations"] - ref["iterations"]) <= 2, (f.info["iterations"], ref["iterations"])
+
+
+def test_lognormal_tet10_matches_the_oracle(gpu, oracle_lib):
+    p = mg.mixed_tet10(10)
+    ref = oracle_lib.model_solve(p, solver=2, tol=1e-12)
+    f = solve(p, tol=1e-12)
+    assert rel(f.displacements, ref["u"]) < 1e-10
+    assert rel(f.von_mises, ref["von_mises"]) < 1e-10
+    assert rel(f.reactions, ref["reactions"]) < 1e-10
+
+
+@pytest.mark.parametrize("cells", [6, 12])
+def test_mixed_precision_reaches_1e8_of_the_fp64_oracle(gpu, oracle_lib, cells):
+    # the mixed form: FP32 matrix/factor inner PCG inside FP64 refinement, checked against an
+    # FP64 oracle converged to 1e-14 (relative displacement and energy-norm error <= 1e-8)
+    p = mg.mixed_tet10(cells)
+    ref = oracle_lib.model_solve(p, solver=2, tol=1e-14)
+    f = solve(p, tol=1e-10, precision=MAILLE_MIXED)
+    assert f.info["outer_iterations"] >= 2
+    assert rel(f.displacements, ref["u"]) <= 1e-8
+    e = f.displacements - ref["u"]
+    e_energy = np.sqrt(oracle_lib.energy(p, e) / oracle_lib.energy(p, ref["u"]))
+    assert e_energy <= 1e-8
+
+
+# --- properties and error contract ----------------------------------------------------------
+
+def test_repeated_solves_are_bit_identical(gpu):
+    p = mg.mixed_tet10(8)
+    a = solve(p)
+    b = solve(p)
+    assert np.array_equal(a.displacements, b.displacements)
+    assert np.array_equal(a.von_mises, b.von_mises)
+    assert np.array_equal(a.reactions, b.reactions)
+
+
+def test_zero_load_gives_exact_zero(gpu):
+    # iterative.rs:214-216 / 311-324
+    p = mg.plain_tet4(6)
+    p.p_elem = p.p_elem[:0]
+    p.p_face = p.p_face[:0]
+    p.p_value = p.p_value[:0]
+    f = solve(p)
+    assert np.all(f.displacements == 0.0) and f.info["iterations"] == 0
+
+
+def test_unconstrained_structure_is_reported(gpu):
+    # tests/iterative.rs:199-224
+    with pytest.raises(mb.MailleError) as e:
+        solve(cases.unconstrained())
+    assert e.value.kind in ("Singular", "IterativeNotConverged")
+
+
+def test_iteration_cap_reports_not_converged(gpu):
+    with pytest.raises(mb.MailleError) as e:
+        solve(mg.plain_tet4(8), max_iter=3)
+    assert e.value.kind == "IterativeNotConverged"
+    assert e.value.iterations == 3 and e.value.residual > 1e-12
+
+
+def test_cancel_flag_stops_the_solve(gpu):
+    m = model_of(mg.plain_tet4(8))
+    h = mb.SolverHandle(m)
+    h.cancel(True)
+    with pytest.raises(mb.MailleError) as e:
+        h.solve()
+    assert e.value.kind == "Cancelled"
+    h.cancel(False)
+    assert h.solve().info["iterations"] > 0
+    h.close()
+
+
+def test_handle_solves_several_right_hand_sides(gpu):
+    p = mg.plain_tet4(10)
+    m = model_of(p)
+    with mb.SolverHandle(m) as h:
+        a = h.solve()
+        f2 = np.zeros(3 * p.n_nodes)
+        f2[3 * np.nonzero(np.abs(p.coords[:, 2] - 1) < 1e-12)[0]] = 0.01  # shear load on top
+        b = h.solve(f2)
+        c = h.solve()
+    assert np.array_equal(a.displacements, c.displacements)
+    q = mg.plain_tet4(10)
+    q.loads = f2
+    q.p_elem, q.p_face, q.p_value = q.p_elem[:0], q.p_face[:0], q.p_value[:0]
+    assert rel(b.displacements, solve(q).displacements) < 1e-12
+
+
+def test_full_size_plain_tet10_properties(gpu):
+    """Tet10 40^3 lognormal, FP64: equilibrium, residual and determinism at the full size."""
+    p = mg.mixed_tet10(40)
+    f = solve(p, tol=1e-10)
+    assert f.info["free_dofs"] == 1574640
+    assert f.info["final_rel_residual"] <= 1e-10
+    # the reactions balance the 10 MPa pressure on the unit top face
+    assert abs(f.reactions[2::3].sum() - 10.0) < 1e-6
+    assert abs(f.reactions[0::3].sum()) < 1e-6 and abs(f.reactions[1::3].sum()) < 1e-6
+    assert np.isfinite(f.von_mises).all() and (f.von_mises >= 0).all()
