@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
+    ap.add_argument("--only", choices=["mixed", "plain"], default=None,
+                    help="profiling mode: time one form only (no reference solve, e2e or CPU); "
+                         "prints a short line, not the benchmark line")
     return ap.parse_args()
 
 
@@ -226,6 +229,27 @@ def run_reference(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def run_only(args):
+    """One form, W + K steps of refactor + solve, nothing else (for profiler launch lists)."""
+    import torch
+    import maille_b200 as mb
+    from maille_b200 import meshgen as mg
+    from maille_b200._lib import MAILLE_FP64, MAILLE_MIXED
+    from maille_b200.model import face_pressure_loads
+    torch.cuda.set_device(0)
+    L = mb._lib.load()
+    p = mg.mixed_tet10(args.cells)
+    p.loads = face_pressure_loads(p.coords, p.conn, list(zip(p.p_elem, p.p_face, p.p_value)))
+    p.p_elem, p.p_face, p.p_value = p.p_elem[:0], p.p_face[:0], p.p_value[:0]
+    prec = MAILLE_MIXED if args.only == "mixed" else MAILLE_FP64
+    h = mb.SolverHandle(solve_model(mb, p, prec, args.tol, 0), device=0)
+    ms, info, launches = time_handle(torch, h, args.steps, args.warmup, L)
+    h.close()
+    print(json.dumps({"only": args.only, "workload": f"tet10_{args.cells}^3", "ms_per_step": ms,
+                      "iterations": info["iterations"], "updates": info["outer_iterations"],
+                      "launches_per_step": launches}))
+
+
 def run_ours(args):
     import torch
     import maille_b200 as mb
@@ -361,6 +385,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.only:
+        run_only(args)
     else:
         run_ours(args)
 

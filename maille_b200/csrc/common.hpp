@@ -58,6 +58,26 @@ struct Symbolic {
     double ms = 0.0;
 };
 
+// Sliced 3x3-block layout of one matrix part (see sparse.cuh): K (full rows), L (strictly
+// lower blocks) or U (strictly upper blocks, holding L^T). Slices never cross a level; inside a
+// level rows are taken by decreasing length. src maps each slot to its block in the CSR
+// pattern (-1 for padding), so the numeric values are filled by one gather per assembly.
+struct SellHost {
+    int32_t lpr = 1;
+    std::vector<int32_t> rowid;         // [nslices * 32 / lpr], -1 when empty
+    std::vector<int64_t> off{0};        // [nslices + 1] first step of each slice
+    std::vector<int32_t> col, src;      // [steps * 128]
+    std::vector<int32_t> level_slices;  // [levels + 1]
+    int64_t steps() const { return off.back(); }
+    int32_t nslices() const { return (int32_t)off.size() - 1; }
+};
+
+enum SellKind { SELL_FULL = 0, SELL_LOWER = 1, SELL_UPPER = 2 };
+
+// Builds the sliced layout of one part of the analysed pattern. lpr <= 0 picks lanes per row
+// from the mean row length.
+void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out);
+
 // Builds the symbolic analysis. conn is [n_elems * npe] in the caller's node numbering.
 bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
              const uint8_t* fixed, int ordering, Symbolic& s, Error& err);

@@ -7,111 +7,13 @@
 #include <cmath>
 
 #include "kernels.cuh"
+#include "reduce.cuh"
 
 namespace maille {
 
 // kernels launched by this library since load (graph launches add their kernel nodes)
 std::atomic<long long> g_kernel_launches{0};
 namespace {
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// Block-wide ordered sum of one value per thread; result valid in thread 0.
-__device__ __forceinline__ double block_sum(double v, double* sh) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    v = warp_sum(v);
-    __syncthreads();
-    if (lane == 0) sh[warp] = v;
-    __syncthreads();
-    double t = 0.0;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
-    return t;
-}
-
-// Writes this block's partial, returns true (in every thread) in the block that finished last.
-__device__ __forceinline__ bool publish_partial(double v, double* partials, unsigned int* ticket,
-                                                double* sh) {
-    __shared__ bool last;
-    const double t = block_sum(v, sh);
-    if (threadIdx.x == 0) {
-        partials[blockIdx.x] = t;
-        __threadfence();
-        const unsigned int k = atomicAdd(ticket, 1u);
-        last = (k == gridDim.x - 1);
-    }
-    __syncthreads();
-    return last;
-}
-
-// Ordered sum of partials[0..n) by one block (every thread returns the same value).
-__device__ __forceinline__ double gather_sum(const double* partials, int n, double* sh) {
-    __threadfence();
-    double t = 0.0;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) t += __ldcg(partials + k);
-    __shared__ double res;
-    const double s = block_sum(t, sh);
-    if (threadIdx.x == 0) res = s;
-    __syncthreads();
-    return res;
-}
-
-template <typename T>
-struct Vec16;
-template <>
-struct Vec16<double> {
-    using V = double2;
-    static constexpr int N = 2;
-    __device__ static inline double at(const V& v, int k) { return k == 0 ? v.x : v.y; }
-};
-template <>
-struct Vec16<float> {
-    using V = float4;
-    static constexpr int N = 4;
-    __device__ static inline double at(const V& v, int k) {
-        return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
-    }
-};
-
-// acc_r += sum over blocks [b0, b1) of one row of  V_b[r][c] * x[3 col_b + c].
-// The row's values are read as one flat range with lane-interleaved 128-bit loads (double2 /
-// float4), so every load instruction of the warp reads 512 contiguous bytes; a scalar head and
-// tail cover the unaligned ends.
-template <typename T>
-__device__ __forceinline__ void row_accum(const T* __restrict__ vals,
-                                          const int32_t* __restrict__ col, int64_t b0, int64_t b1,
-                                          const T* __restrict__ x, int lane, double& a0,
-                                          double& a1, double& a2) {
-    using VT = Vec16<T>;
-    constexpr int VN = VT::N;
-    const int64_t vb = 9 * b0, ve = 9 * b1;
-    int64_t va = (vb + VN - 1) / VN * VN;
-    if (va > ve) va = ve;
-    int64_t vz = ve / VN * VN;
-    if (vz < va) vz = va;
-    auto one = [&](int64_t v, double a) {
-        const int t = (int)(v - vb);
-        const int b = t / 9;
-        const int e = t - 9 * b;
-        const int r = (e * 11) >> 5;  // e / 3 for e < 9
-        const int c = e - 3 * r;
-        const double pr = a * (double)x[3 * (int64_t)__ldg(col + b0 + b) + c];
-        a0 += (r == 0) ? pr : 0.0;
-        a1 += (r == 1) ? pr : 0.0;
-        a2 += (r == 2) ? pr : 0.0;
-    };
-    if (lane < va - vb) one(vb + lane, (double)__ldg(vals + vb + lane));
-    for (int64_t v = va + (int64_t)lane * VN; v < vz; v += 32 * VN) {
-        const typename VT::V q = __ldg(reinterpret_cast<const typename VT::V*>(vals + v));
-#pragma unroll
-        for (int k = 0; k < VN; ++k) one(v + k, VT::at(q, k));
-    }
-    if (lane < ve - vz) one(vz + lane, (double)__ldg(vals + vz + lane));
-}
 
 // ---- element integration --------------------------------------------------------------------
 
@@ -417,273 +319,23 @@ __global__ void __launch_bounds__(kThreads) k_factor(Pattern pt, int32_t r0, int
     }
 }
 
-// ---- PCG kernels ----------------------------------------------------------------------------
-
-// ap = K p, one warp per block row; p . ap reduced; the last block sets alpha = rz / (p . ap)
-// (Pcg::solve, iterative.rs:223-228): curvature <= 0 or NaN -> SINGULAR.
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_spmv_pcg(Pattern pt, const T* __restrict__ K,
-                                                        const T* __restrict__ p, T* __restrict__ ap,
-                                                        PcgScalars* s, double* partials) {
-    __shared__ double sh[kWarps];
-    if (s->done) return;
-    const int lane = threadIdx.x & 31;
-    double loc = 0.0;
-    for (int32_t I = (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); I < pt.nb;
-         I += (int32_t)((gridDim.x * blockDim.x) >> 5)) {
-        double a0 = 0, a1 = 0, a2 = 0;
-        row_accum<T>(K, pt.col, pt.row_ptr[I], pt.row_ptr[I + 1], p, lane, a0, a1, a2);
-        a0 = warp_sum(a0);
-        a1 = warp_sum(a1);
-        a2 = warp_sum(a2);
-        if (lane == 0) {
-            const int64_t k = 3 * (int64_t)I;
-            const T y0 = (T)a0, y1 = (T)a1, y2 = (T)a2;
-            ap[k] = y0;
-            ap[k + 1] = y1;
-            ap[k + 2] = y2;
-            loc += (double)p[k] * (double)y0 + (double)p[k + 1] * (double)y1 + (double)p[k + 2] * (double)y2;
-        }
-    }
-    if (publish_partial(loc, partials, &s->ticket[0], sh)) {
-        const double pap = gather_sum(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            s->pap = pap;
-            s->iter += 1;
-            if (isnan(pap) || pap <= 0.0) {
-                s->status = 1;
-                s->done = 1;
-            } else {
-                s->alpha = s->rz / pap;
-            }
-            s->ticket[0] = 0;
-        }
-    }
-}
-
-// One level of the forward sweep, fused with the PCG update of its rows:
-//   x_I += alpha p_I, r_I -= alpha ap_I (iterative.rs:229-232), ||r||^2 partials,
-//   y_I = L_II^-1 (r_I - sum_{J<I} L_IJ y_J)   (Csr::precondition, iterative.rs:175-179).
-// The last level's last block checks ||r|| <= tol ||b|| (iterative.rs:233) and the cap.
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_fwd(Pattern pt, int32_t r0, int32_t r1, int level,
-                                                   int nlevels, const T* __restrict__ F, T* r, T* y,
-                                                   T* x, const T* __restrict__ p,
-                                                   const T* __restrict__ ap, PcgScalars* s,
-                                                   double* partials, double* lvl_total) {
-    __shared__ double sh[kWarps];
-    if (s->done) return;
-    const int lane = threadIdx.x & 31;
-    const double alpha = s->alpha;
-    double loc = 0.0;
-    for (int32_t I = r0 + (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); I < r1;
-         I += (int32_t)((gridDim.x * blockDim.x) >> 5)) {
-        double ri = 0.0;
-        if (lane < 3) {
-            const int64_t k = 3 * (int64_t)I + lane;
-            x[k] = (T)((double)x[k] + alpha * (double)p[k]);
-            const T rn = (T)((double)r[k] - alpha * (double)ap[k]);
-            r[k] = rn;
-            ri = (double)rn;
-            loc += ri * ri;
-        }
-        const double t0 = __shfl_sync(0xffffffffu, ri, 0);
-        const double t1 = __shfl_sync(0xffffffffu, ri, 1);
-        const double t2 = __shfl_sync(0xffffffffu, ri, 2);
-        double a0 = 0, a1 = 0, a2 = 0;
-        row_accum<T>(F, pt.col, pt.row_ptr[I], pt.diag[I], y, lane, a0, a1, a2);
-        a0 = warp_sum(a0);
-        a1 = warp_sum(a1);
-        a2 = warp_sum(a2);
-        if (lane == 0) {
-            const T* D = F + 9 * pt.diag[I];
-            const double u0 = t0 - a0, u1 = t1 - a1, u2 = t2 - a2;
-            const int64_t k = 3 * (int64_t)I;
-            y[k] = (T)((double)D[0] * u0);
-            y[k + 1] = (T)((double)D[3] * u0 + (double)D[4] * u1);
-            y[k + 2] = (T)((double)D[6] * u0 + (double)D[7] * u1 + (double)D[8] * u2);
-        }
-    }
-    if (publish_partial(loc, partials, &s->ticket[1], sh)) {
-        const double tot = gather_sum(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            lvl_total[level] = tot;
-            s->ticket[1] = 0;
-        }
-        if (level == nlevels - 1) {
-            const double rr = gather_sum(lvl_total, nlevels, sh);
-            if (threadIdx.x == 0) {
-                s->rr = rr;
-                if (sqrt(rr) <= s->tol * sqrt(s->bb)) {
-                    s->done = 1;
-                } else if (s->iter >= s->max_iter) {
-                    s->done = 1;
-                    s->status = 2;
-                }
-            }
-        }
-    }
-}
-
-// One level of the backward sweep z_I = L_II^-T (y_I - sum_{J>I} L_JI^T z_J) (in place over y,
-// Csr::precondition, iterative.rs:180-186, as a gather), with r . z partials. The last launch
-// (level 0) sets beta = rz_new / rz and rz = rz_new (iterative.rs:237-239).
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_bwd(Pattern pt, int32_t r0, int32_t r1, int level,
-                                                   int nlevels, const T* __restrict__ F,
-                                                   const T* __restrict__ r, T* z, PcgScalars* s,
-                                                   double* partials, double* lvl_total) {
-    __shared__ double sh[kWarps];
-    if (s->done) return;
-    const int lane = threadIdx.x & 31;
-    double loc = 0.0;
-    for (int32_t I = r0 + (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); I < r1;
-         I += (int32_t)((gridDim.x * blockDim.x) >> 5)) {
-        double a0 = 0, a1 = 0, a2 = 0;
-        row_accum<T>(F, pt.col, pt.diag[I] + 1, pt.row_ptr[I + 1], z, lane, a0, a1, a2);
-        a0 = warp_sum(a0);
-        a1 = warp_sum(a1);
-        a2 = warp_sum(a2);
-        if (lane == 0) {
-            const T* D = F + 9 * pt.diag[I];
-            const int64_t k = 3 * (int64_t)I;
-            const double u0 = (double)z[k] - a0, u1 = (double)z[k + 1] - a1, u2 = (double)z[k + 2] - a2;
-            const T z0 = (T)((double)D[0] * u0 + (double)D[3] * u1 + (double)D[6] * u2);
-            const T z1 = (T)((double)D[4] * u1 + (double)D[7] * u2);
-            const T z2 = (T)((double)D[8] * u2);
-            z[k] = z0;
-            z[k + 1] = z1;
-            z[k + 2] = z2;
-            loc += (double)r[k] * (double)z0 + (double)r[k + 1] * (double)z1 + (double)r[k + 2] * (double)z2;
-        }
-    }
-    if (publish_partial(loc, partials, &s->ticket[2], sh)) {
-        const double tot = gather_sum(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            lvl_total[level] = tot;
-            s->ticket[2] = 0;
-        }
-        if (level == 0) {
-            const double rz = gather_sum(lvl_total, nlevels, sh);
-            if (threadIdx.x == 0) {
-                if (s->iter == 0) {
-                    s->beta = 0.0;
-                } else {
-                    s->beta = rz / s->rz;
-                }
-                s->rz = rz;
-            }
-        }
-    }
-}
-
-// p = z + beta p (iterative.rs:240-242)
-template <typename T>
-__global__ void k_pupdate(int64_t n, const T* __restrict__ z, T* __restrict__ p, PcgScalars* s) {
-    if (s->done) return;
-    const double beta = s->beta;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-        p[k] = (T)((double)z[k] + beta * (double)p[k]);
-}
-
-__global__ void k_pcg_init(PcgScalars* s, double tol, int32_t max_iter) {
-    s->alpha = 0.0;
-    s->beta = 0.0;
-    s->rz = 0.0;
-    s->rr = 0.0;
-    s->tol = tol;
-    s->pap = 0.0;
-    s->iter = 0;
-    s->max_iter = max_iter;
-    s->status = 0;
-    s->done = (s->bb == 0.0) ? 1 : 0;  // zero right-hand side: x = 0 (iterative.rs:214-216)
-    for (int k = 0; k < 4; ++k) s->ticket[k] = 0;
-}
-
-// r = b - K u in FP64 with ||r||^2 (the refinement's outer residual).
-__global__ void __launch_bounds__(kThreads) k_residual64(Pattern pt, const double* __restrict__ K,
-                                                          const double* __restrict__ b,
-                                                          const double* __restrict__ u,
-                                                          double* __restrict__ r, double* partials,
-                                                          unsigned int* ticket, double* out_sum) {
-    __shared__ double sh[kWarps];
-    const int lane = threadIdx.x & 31;
-    double loc = 0.0;
-    for (int32_t I = (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); I < pt.nb;
-         I += (int32_t)((gridDim.x * blockDim.x) >> 5)) {
-        double a0 = 0, a1 = 0, a2 = 0;
-        row_accum<double>(K, pt.col, pt.row_ptr[I], pt.row_ptr[I + 1], u, lane, a0, a1, a2);
-        a0 = warp_sum(a0);
-        a1 = warp_sum(a1);
-        a2 = warp_sum(a2);
-        if (lane == 0) {
-            const int64_t k = 3 * (int64_t)I;
-            const double q0 = b[k] - a0, q1 = b[k + 1] - a1, q2 = b[k + 2] - a2;
-            r[k] = q0;
-            r[k + 1] = q1;
-            r[k + 2] = q2;
-            loc += q0 * q0 + q1 * q1 + q2 * q2;
-        }
-    }
-    if (publish_partial(loc, partials, ticket, sh)) {
-        const double tot = gather_sum(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            *out_sum = tot;
-            *ticket = 0;
-        }
-    }
-}
-
-template <typename T>
-__global__ void k_norm2(int64_t n, const T* __restrict__ v, double* partials,
-                        unsigned int* ticket, double* out_sum) {
-    __shared__ double sh[kWarps];
-    double loc = 0.0;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-        loc += (double)v[k] * (double)v[k];
-    if (publish_partial(loc, partials, ticket, sh)) {
-        const double tot = gather_sum(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            *out_sum = tot;
-            *ticket = 0;
-        }
-    }
-}
-
-__global__ void k_scale_to_float(int64_t n, const double* __restrict__ src,
-                                 const double* __restrict__ norm2, float* __restrict__ dst) {
-    const double inv = 1.0 / sqrt(*norm2);
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-        dst[k] = (float)(src[k] * inv);
-}
-
-__global__ void k_accumulate(int64_t n, const float* __restrict__ d, const double* __restrict__ norm2,
-                             double* __restrict__ u) {
-    const double sc = sqrt(*norm2);
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-        u[k] += sc * (double)d[k];
-}
-
-__global__ void k_to_float(int64_t n, const double* __restrict__ src, float* __restrict__ dst) {
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-        dst[k] = (float)src[k];
-}
-
 // ---- right-hand side, solution, boundary products -------------------------------------------
 
-// b_I = F_f - K_fc u_c in solver numbering, 0 at fixed DOFs of kept nodes (FreeSystem::solve,
+// b_I = F_f - K_fc u_c in solver numbering (padded: 4 entries per node), 0 at fixed DOFs of kept nodes (FreeSystem::solve,
 // model.rs:1503-1508).
 __global__ void k_build_rhs(int32_t nb, const int32_t* __restrict__ perm,
                             const uint8_t* __restrict__ fixmask, const double* __restrict__ f,
                             const double* __restrict__ coupling, double* __restrict__ b) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 3 * (int64_t)nb) return;
-    const int32_t I = (int32_t)(t / 3);
-    const int c = (int)(t - 3 * (int64_t)I);
-    const int64_t g = 3 * (int64_t)perm[I] + c;
+    if (t >= 4 * (int64_t)nb) return;
+    const int32_t I = (int32_t)(t >> 2);
+    const int c = (int)(t & 3);
     double v = 0.0;
-    if (!((fixmask[I] >> c) & 1)) v = (f ? f[g] : 0.0) - (coupling ? coupling[g] : 0.0);
-    b[t] = v;
+    if (c < 3 && !((fixmask[I] >> c) & 1)) {
+        const int64_t g = 3 * (int64_t)perm[I] + c;
+        v = (f ? f[g] : 0.0) - (coupling ? coupling[g] : 0.0);
+    }
+    b[t] = v;  // padded layout: 4 entries per node, the 4th is 0
 }
 
 // u = imposed at fixed DOFs, x at free DOFs (model.rs:581, 1509-1514)
@@ -695,7 +347,7 @@ __global__ void k_gather_u(int64_t n_nodes, const int32_t* __restrict__ inv,
     const int64_t v = g / 3;
     const int c = (int)(g - 3 * v);
     const int32_t I = inv[v];
-    u[g] = (fixed && fixed[g]) ? imposed[g] : (I >= 0 ? x[3 * (int64_t)I + c] : 0.0);
+    u[g] = (fixed && fixed[g]) ? imposed[g] : (I >= 0 ? x[4 * (int64_t)I + c] : 0.0);
 }
 
 __device__ __forceinline__ int pair_index(int npe, int a, int b) {
@@ -917,97 +569,10 @@ void launch_factor_level(const Pattern& pt, int32_t r0, int32_t r1, const double
     k_factor<<<blocks_for(rows, kWarps, INT32_MAX), kThreads, 0, st>>>(pt, r0, r1, K, F, shift, fail);
 }
 
-template <typename T>
-void launch_spmv_pcg(const Pattern& pt, const T* K, const T* p, T* ap, PcgScalars* s,
-                     double* partials, int grid, cudaStream_t st) {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_spmv_pcg<T><<<grid, kThreads, 0, st>>>(pt, K, p, ap, s, partials);
-}
-
-template <typename T>
-void launch_fwd(const Pattern& pt, int32_t r0, int32_t r1, int level, int nlevels, const T* F,
-                T* r, T* y, T* x, const T* p, const T* ap, PcgScalars* s, double* partials,
-                double* lvl_total, int grid, cudaStream_t st) {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_fwd<T><<<grid, kThreads, 0, st>>>(pt, r0, r1, level, nlevels, F, r, y, x, p, ap, s, partials,
-                                        lvl_total);
-}
-
-template <typename T>
-void launch_bwd(const Pattern& pt, int32_t r0, int32_t r1, int level, const T* F, const T* r,
-                T* z, PcgScalars* s, double* partials, double* lvl_total, int nlevels, int grid,
-                cudaStream_t st) {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_bwd<T><<<grid, kThreads, 0, st>>>(pt, r0, r1, level, nlevels, F, r, z, s, partials, lvl_total);
-}
-
-template <typename T>
-void launch_pupdate(int64_t n, const T* z, T* p, PcgScalars* s, cudaStream_t st) {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_pupdate<T><<<blocks_for(n, kThreads, 148 * 16), kThreads, 0, st>>>(n, z, p, s);
-}
-
-template void launch_spmv_pcg<double>(const Pattern&, const double*, const double*, double*,
-                                      PcgScalars*, double*, int, cudaStream_t);
-template void launch_spmv_pcg<float>(const Pattern&, const float*, const float*, float*,
-                                     PcgScalars*, double*, int, cudaStream_t);
-template void launch_fwd<double>(const Pattern&, int32_t, int32_t, int, int, const double*, double*,
-                                 double*, double*, const double*, const double*, PcgScalars*,
-                                 double*, double*, int, cudaStream_t);
-template void launch_fwd<float>(const Pattern&, int32_t, int32_t, int, int, const float*, float*,
-                                float*, float*, const float*, const float*, PcgScalars*, double*,
-                                double*, int, cudaStream_t);
-template void launch_bwd<double>(const Pattern&, int32_t, int32_t, int, const double*, const double*,
-                                 double*, PcgScalars*, double*, double*, int, int, cudaStream_t);
-template void launch_bwd<float>(const Pattern&, int32_t, int32_t, int, const float*, const float*,
-                                float*, PcgScalars*, double*, double*, int, int, cudaStream_t);
-template void launch_pupdate<double>(int64_t, const double*, double*, PcgScalars*, cudaStream_t);
-template void launch_pupdate<float>(int64_t, const float*, float*, PcgScalars*, cudaStream_t);
-
-void launch_residual64(const Pattern& pt, const double* K, const double* b, const double* u,
-                       double* r, double* partials, unsigned int* ticket, double* out_sum,
-                       int grid, cudaStream_t st) {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_residual64<<<grid, kThreads, 0, st>>>(pt, K, b, u, r, partials, ticket, out_sum);
-}
-
-void launch_norm2(int64_t n, const double* v, double* partials, unsigned int* ticket,
-                  double* out_sum, int grid, cudaStream_t st) {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_norm2<double><<<grid, kThreads, 0, st>>>(n, v, partials, ticket, out_sum);
-}
-
-void launch_norm2_f(int64_t n, const float* v, double* partials, unsigned int* ticket,
-                    double* out_sum, int grid, cudaStream_t st) {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_norm2<float><<<grid, kThreads, 0, st>>>(n, v, partials, ticket, out_sum);
-}
-
-void launch_scale_to_float(int64_t n, const double* src, const double* norm2, float* dst,
-                           cudaStream_t st) {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_scale_to_float<<<blocks_for(n, kThreads, 148 * 16), kThreads, 0, st>>>(n, src, norm2, dst);
-}
-
-void launch_accumulate(int64_t n, const float* d, const double* norm2, double* u, cudaStream_t st) {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_accumulate<<<blocks_for(n, kThreads, 148 * 16), kThreads, 0, st>>>(n, d, norm2, u);
-}
-
-void launch_to_float(int64_t n, const double* src, float* dst, cudaStream_t st) {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_to_float<<<blocks_for(n, kThreads, 148 * 32), kThreads, 0, st>>>(n, src, dst);
-}
-
-void launch_pcg_init(PcgScalars* s, double tol, int32_t max_iter, cudaStream_t st) {
-    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_pcg_init<<<1, 1, 0, st>>>(s, tol, max_iter);
-}
-
 void launch_build_rhs(int32_t nb, const int32_t* perm, const uint8_t* fixmask, const double* f,
                       const double* coupling, double* b, cudaStream_t st) {
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    k_build_rhs<<<blocks_for(3 * (int64_t)nb, kThreads, INT32_MAX), kThreads, 0, st>>>(nb, perm, fixmask, f, coupling, b);
+    k_build_rhs<<<blocks_for(4 * (int64_t)nb, kThreads, INT32_MAX), kThreads, 0, st>>>(nb, perm, fixmask, f, coupling, b);
 }
 
 void launch_gather_u(int64_t n_nodes, const int32_t* inv, const uint8_t* fixed,

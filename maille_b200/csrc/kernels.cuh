@@ -1,10 +1,11 @@
 // kernels.cuh -- sm_100a kernels of the linear-elastic solve path.
 //
 // Data layout in HBM (new = solver numbering of the kept nodes, see setup.cpp):
-//   * K and F (the IC(0) factor) share one full 3x3-block CSR pattern: row_ptr (int64), col
-//     (int32), values as 9 consecutive entries per block, row-major (AoS). F holds L below the
-//     diagonal, L^T above it (so both sweeps gather along rows) and D = L_II^-1 on the diagonal.
-//   * Vectors are [3 nb] in new numbering, DOF c of row I at 3 I + c.
+//   * K and F (the IC(0) factor) are assembled and factorised on one full 3x3-block CSR pattern:
+//     row_ptr (int64), col (int32), 9 consecutive entries per block, row-major. F holds L below
+//     the diagonal, L^T above it and D = L_II^-1 on the diagonal. The iteration kernels read
+//     copies of K, L, L^T and D in the sliced layout of sparse.cuh.
+//   * Solver vectors are padded, [4 nb] in new numbering: DOF c of row I at 4 I + c, 4th = 0.
 //   * Element matrices are kept as their node-pair blocks a <= b: Ke[(e * NP + pair) * 9 + 3 i + j]
 //     = K_e[3 a + i][3 b + j].
 // Every reduction is deterministic: fixed per-warp shuffle trees, per-block partials in fixed
@@ -23,13 +24,6 @@ constexpr int kMaxLevels = 65536;
 
 // kernels launched by this library since load (a graph launch adds its kernel nodes)
 extern std::atomic<long long> g_kernel_launches;
-
-// Device-resident scalars of one PCG run.
-struct PcgScalars {
-    double alpha, beta, rz, rr, bb, tol, pap;
-    int32_t iter, max_iter, done, status;  // status: 0 ok, 1 singular (also NaN)
-    unsigned int ticket[4];                // 0 spmv, 1 fwd, 2 bwd, 3 misc
-};
 
 // Element geometry / material inputs (old numbering).
 struct ElemIn {
@@ -56,34 +50,10 @@ void launch_assemble(const Pattern& pt, int64_t nl, const int64_t* lslot, const 
                      const uint32_t* contrib, const double* ke_up, double* K, cudaStream_t st);
 void launch_factor_level(const Pattern& pt, int32_t r0, int32_t r1, const double* K, double* F,
                         double shift, int32_t* fail, cudaStream_t st);
-template <typename T>
-void launch_spmv_pcg(const Pattern& pt, const T* K, const T* p, T* ap, PcgScalars* s,
-                     double* partials, int grid, cudaStream_t st);
-template <typename T>
-void launch_fwd(const Pattern& pt, int32_t r0, int32_t r1, int level, int nlevels, const T* F,
-                T* r, T* y, T* x, const T* p, const T* ap, PcgScalars* s, double* partials,
-                double* lvl_total, int grid, cudaStream_t st);
-template <typename T>
-void launch_bwd(const Pattern& pt, int32_t r0, int32_t r1, int level, const T* F, const T* r,
-                T* z, PcgScalars* s, double* partials, double* lvl_total, int nlevels, int grid,
-                cudaStream_t st);
-template <typename T>
-void launch_pupdate(int64_t n, const T* z, T* p, PcgScalars* s, cudaStream_t st);
-void launch_residual64(const Pattern& pt, const double* K, const double* b, const double* u,
-                       double* r, double* partials, unsigned int* ticket, double* out_sum,
-                       int grid, cudaStream_t st);
-void launch_norm2(int64_t n, const double* v, double* partials, unsigned int* ticket,
-                  double* out_sum, int grid, cudaStream_t st);
-void launch_scale_to_float(int64_t n, const double* src, const double* norm2, float* dst,
-                           cudaStream_t st);
-void launch_accumulate(int64_t n, const float* d, const double* norm2, double* u,
-                       cudaStream_t st);
-void launch_to_float(int64_t n, const double* src, float* dst, cudaStream_t st);
-void launch_norm2_f(int64_t n, const float* v, double* partials, unsigned int* ticket,
-                    double* out_sum, int grid, cudaStream_t st);
-void launch_pcg_init(PcgScalars* s, double tol, int32_t max_iter, cudaStream_t st);
+// b (padded solver numbering, 4 per node) = F_f - K_fc u_c, 0 at fixed DOFs
 void launch_build_rhs(int32_t nb, const int32_t* perm, const uint8_t* fixmask, const double* f,
                       const double* coupling, double* b, cudaStream_t st);
+// u (caller numbering) = imposed at fixed DOFs, x (padded solver numbering) elsewhere
 void launch_gather_u(int64_t n_nodes, const int32_t* inv, const uint8_t* fixed,
                      const double* imposed, const double* x, double* u, cudaStream_t st);
 void launch_elem_apply(int npe, int64_t nlist, const int32_t* list, const int32_t* conn,

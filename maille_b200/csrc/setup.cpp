@@ -134,7 +134,7 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
         err = {MAILLE_INVALID_INPUT, "empty mesh"};
         return false;
     }
-    if (n_nodes >= (int64_t(1) << 31) || n_elems * node_pairs(npe) >= (int64_t(1) << 31)) {
+    if (n_nodes >= (int64_t(1) << 30) || n_elems * node_pairs(npe) >= (int64_t(1) << 31)) {
         err = {MAILLE_INVALID_INPUT, "mesh too large for 32-bit element-pair indices"};
         return false;
     }
@@ -249,6 +249,10 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
         s.row_ptr[r + 1] = s.row_ptr[r] + (g.off[k + 1] - g.off[k]) + 1;
     }
     s.blocks = s.row_ptr[nk];
+    if (s.blocks >= (int64_t(1) << 31)) {
+        err = {MAILLE_INVALID_INPUT, "pattern too large for 32-bit block positions"};
+        return false;
+    }
     s.col.resize(s.blocks);
     s.diag.resize(nk);
     for (int32_t r = 0; r < nk; ++r) {
@@ -334,6 +338,52 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
     }
     s.ms = now_ms() - t0;
     return true;
+}
+
+void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out) {
+    out = SellHost{};
+    auto start = [&](int32_t i) { return kind == SELL_UPPER ? s.diag[i] + 1 : s.row_ptr[i]; };
+    auto end = [&](int32_t i) { return kind == SELL_LOWER ? s.diag[i] : s.row_ptr[i + 1]; };
+    if (lpr <= 0) {
+        const double total = kind == SELL_FULL ? (double)s.blocks : (double)(s.blocks - s.nb) / 2.0;
+        const double mean = total / std::max<int32_t>(1, s.nb);
+        lpr = 1;
+        while (lpr < 8 && mean / (2.0 * lpr) > 8.0) lpr *= 2;
+    }
+    out.lpr = lpr;
+    const int S = 32 / lpr, per_step = 4 * lpr;
+    out.level_slices.push_back(0);
+    std::vector<int32_t> rows;
+    for (int32_t l = 0; l < s.levels; ++l) {
+        rows.clear();
+        for (int32_t i = s.level_ptr[l]; i < s.level_ptr[l + 1]; ++i) rows.push_back(i);
+        std::stable_sort(rows.begin(), rows.end(), [&](int32_t a, int32_t b) {
+            return end(a) - start(a) > end(b) - start(b);
+        });
+        for (size_t c0 = 0; c0 < rows.size(); c0 += S) {
+            const size_t c1 = std::min(rows.size(), c0 + S);
+            int64_t maxlen = 0;
+            for (size_t k = c0; k < c1; ++k) maxlen = std::max<int64_t>(maxlen, end(rows[k]) - start(rows[k]));
+            const int64_t steps = (maxlen + per_step - 1) / per_step;
+            const int64_t g0 = out.off.back();
+            out.off.push_back(g0 + steps);
+            out.col.resize((size_t)(g0 + steps) * 128, rows[c0]);
+            out.src.resize((size_t)(g0 + steps) * 128, -1);
+            for (int r = 0; r < S; ++r) out.rowid.push_back(c0 + r < c1 ? rows[c0 + r] : -1);
+            for (size_t k = c0; k < c1; ++k) {
+                const int32_t i = rows[k];
+                const int r = (int)(k - c0);
+                for (int64_t p = start(i), b = 0; p < end(i); ++p, ++b) {
+                    const int64_t t = b / per_step, rem = b % per_step;
+                    const int64_t lane = r * lpr + rem / 4, j = rem % 4;
+                    const size_t slot = (size_t)(g0 + t) * 128 + 4 * lane + j;
+                    out.col[slot] = s.col[p];
+                    out.src[slot] = (int32_t)p;
+                }
+            }
+        }
+        out.level_slices.push_back(out.nslices());
+    }
 }
 
 // face_pressure for the tet faces (assembly.rs:650-674; face_rule tet branch 556-585; face nodes

@@ -25,6 +25,7 @@
 
 #include "common.hpp"
 #include "kernels.cuh"
+#include "sparse.cuh"
 
 using namespace maille;
 
@@ -64,17 +65,35 @@ T* dupload(const T* src, size_t n, cudaStream_t st) {
     return d;
 }
 
-// Vectors of one PCG precision.
-template <typename T>
-struct PcgVecs {
-    T *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr;
-};
-
 constexpr double kDefaultTol = 1e-12;      // iterative.rs:9
 constexpr int32_t kDefaultMaxIter = 10000;  // iterative.rs:11
 const double kShifts[6] = {0.0, 1e-3, 1e-2, 1e-1, 1.0, 10.0};  // iterative.rs:14
 
 }  // namespace
+
+// A sliced layout: host description (level slices) plus its device index arrays.
+struct SellBuf {
+    SellHost h;
+    int32_t* rowid = nullptr;
+    int64_t* off = nullptr;
+    int32_t* col = nullptr;
+    int32_t* src = nullptr;
+    SellDev dev() const { return SellDev{h.lpr, h.nslices(), rowid, off, col}; }
+    void upload(cudaStream_t st) {
+        rowid = dupload(h.rowid.data(), h.rowid.size(), st);
+        off = dupload(h.off.data(), h.off.size(), st);
+        col = dupload(h.col.data(), h.col.size(), st);
+        src = dupload(h.src.data(), h.src.size(), st);
+    }
+    void release() {
+        for (void* p : {(void*)rowid, (void*)off, (void*)col, (void*)src})
+            if (p) cudaFree(p);
+        rowid = nullptr;
+        off = nullptr;
+        col = nullptr;
+        src = nullptr;
+    }
+};
 
 struct MailleGpuHandle {
     int device = 0;
@@ -86,8 +105,7 @@ struct MailleGpuHandle {
     int precision = MAILLE_FP64;
     double tol = kDefaultTol;
     int32_t max_iter = kDefaultMaxIter;
-    double inner_tol = 1e-4;
-    int32_t max_outer = 60;
+    double delta = 0.1;  // reliable update when the FP32 residual fell by this factor
     std::vector<uint8_t> h_fixed;
     std::vector<double> h_f, h_f0, h_imposed;
     bool any_imposed = false;
@@ -104,17 +122,19 @@ struct MailleGpuHandle {
     uint32_t* contrib = nullptr;
     int64_t* inc_ptr = nullptr;
     int32_t *inc = nullptr, *belem = nullptr, *bnodes = nullptr, *elem_slot = nullptr;
-    // device: numeric
+    // device: numeric (CSR K and factor F; sliced copies for the iterations)
     double* ke = nullptr;
     double *K = nullptr, *F = nullptr;
-    float *K32 = nullptr, *F32 = nullptr;
-    PcgVecs<double> v64;
-    PcgVecs<float> v32;
-    double *rr64 = nullptr;  // outer residual (mixed)
+    SellBuf sk, sl, su;
+    double *Ks64 = nullptr, *Ls64 = nullptr, *Us64 = nullptr, *D64 = nullptr;
+    float *Ks32 = nullptr, *Ls32 = nullptr, *Us32 = nullptr, *D32 = nullptr;
+    // padded solver vectors (4 entries per block row)
+    double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr, *z64 = nullptr, *p64 = nullptr,
+           *ap64 = nullptr;
+    float *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *ap32 = nullptr;
     double *u_full = nullptr, *y_full = nullptr, *ye = nullptr, *gauss = nullptr, *vm = nullptr,
            *react = nullptr, *lambda_full = nullptr, *grad = nullptr;
     PcgScalars* scal = nullptr;
-    PcgScalars* spmv_scal = nullptr;
     PcgScalars* h_scal = nullptr;  // pinned
     double* partials = nullptr;
     double* lvl_total = nullptr;
@@ -123,8 +143,7 @@ struct MailleGpuHandle {
     unsigned int* dticket = nullptr;
     int32_t* dfail = nullptr;
     int spmv_grid = 1;
-    std::vector<int> lvl_grid;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [0] FP64, [1] FP32
+    cudaGraphExec_t graph = nullptr;  // PCG iterations of the handle's form
     int graph_iters = 8;
     long long graph_kernels = 0;
     std::atomic<int> cancel{0};
@@ -146,14 +165,14 @@ void dfree(void* p) {
 
 MailleGpuHandle::~MailleGpuHandle() {
     cudaSetDevice(device);
-    for (auto& g : graph)
-        if (g) cudaGraphExecDestroy(g);
+    if (graph) cudaGraphExecDestroy(graph);
     void* bufs[] = {coords, young, poisson, imposed, f, f0, conn, fixed, perm, inv, col, lrow, fixmask,
                     row_ptr, diag, tpos, lslot, lptr, contrib, inc_ptr, inc, belem, bnodes,
-                    elem_slot, ke, K, F, K32, F32, v64.b, v64.x, v64.r, v64.z, v64.p, v64.ap,
-                    v32.b, v32.x, v32.r, v32.z, v32.p, v32.ap, rr64, u_full, y_full, ye, gauss, vm,
-                    react, lambda_full, grad, scal, spmv_scal, partials, lvl_total, dsum, dticket, dfail};
+                    elem_slot, ke, K, F, Ks64, Ls64, Us64, D64, Ks32, Ls32, Us32, D32, b64, x64,
+                    r64, z64, p64, ap64, x32, r32, z32, p32, ap32, u_full, y_full, ye, gauss, vm,
+                    react, lambda_full, grad, scal, partials, lvl_total, dsum, dticket, dfail};
     for (void* p : bufs) dfree(p);
+    for (SellBuf* b : {&sk, &sl, &su}) b->release();
     if (h_scal) cudaFreeHost(h_scal);
     if (h_sum) cudaFreeHost(h_sum);
     for (auto& e : ev)
@@ -169,87 +188,95 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
-int grid_for_rows(int64_t rows) {
-    int64_t g = (rows + kWarps - 1) / kWarps;
+int grid_for_slices(int64_t slices) {
+    int64_t g = (slices + kWarps - 1) / kWarps;
     if (g > 148 * 8) g = 148 * 8;
     return (int)(g < 1 ? 1 : g);
 }
 
-// Kernel sequence of one PCG iteration (type T) on the handle's stream.
-template <typename T>
-void enqueue_iteration(MailleGpuHandle* h, const T* K, const T* F, PcgVecs<T>& v) {
-    const Pattern pt = h->pattern();
+bool is_mixed(const MailleGpuHandle* h) { return h->precision == MAILLE_MIXED; }
+
+// The preconditioner z = (L L^T)^-1 r: forward levels then backward levels (Csr::precondition,
+// iterative.rs:173-188), in the precision of the form.
+void enqueue_precondition(MailleGpuHandle* h) {
     const int L = h->sym.levels;
-    launch_spmv_pcg<T>(pt, K, v.p, v.ap, h->scal, h->partials, h->spmv_grid, h->st);
-    for (int l = 0; l < L; ++l)
-        launch_fwd<T>(pt, h->sym.level_ptr[l], h->sym.level_ptr[l + 1], l, L, F, v.r, v.z, v.x,
-                      v.p, v.ap, h->scal, h->partials, h->lvl_total, h->lvl_grid[l], h->st);
-    for (int l = L - 1; l >= 0; --l)
-        launch_bwd<T>(pt, h->sym.level_ptr[l], h->sym.level_ptr[l + 1], l, F, v.r, v.z, h->scal,
-                      h->partials, h->lvl_total + kMaxLevels, L, h->lvl_grid[l], h->st);
-    launch_pupdate<T>(3 * (int64_t)h->sym.nb, v.z, v.p, h->scal, h->st);
+    const int32_t nb = h->sym.nb;
+    const SellDev Ld = h->sl.dev(), Ud = h->su.dev();
+    const auto& ls = h->sl.h.level_slices;
+    const auto& us = h->su.h.level_slices;
+    double* lt = h->lvl_total;
+    if (is_mixed(h)) {
+        for (int l = 0; l < L; ++l)
+            launch_fwd<float>(Ld, ls[l], ls[l + 1], h->Ls32, h->D32, nb, h->r32, h->z32, h->scal, h->st);
+        for (int l = L - 1; l >= 0; --l)
+            launch_bwd<float>(Ud, us[l], us[l + 1], l, L, h->Us32, h->D32, nb, h->r32, h->z32,
+                              h->scal, h->partials, lt, h->st);
+        launch_pupdate<float>(nb, h->z32, h->p32, h->scal, h->st);
+    } else {
+        for (int l = 0; l < L; ++l)
+            launch_fwd<double>(Ld, ls[l], ls[l + 1], h->Ls64, h->D64, nb, h->r64, h->z64, h->scal, h->st);
+        for (int l = L - 1; l >= 0; --l)
+            launch_bwd<double>(Ud, us[l], us[l + 1], l, L, h->Us64, h->D64, nb, h->r64, h->z64,
+                               h->scal, h->partials, lt, h->st);
+        launch_pupdate<double>(nb, h->z64, h->p64, h->scal, h->st);
+    }
 }
 
-template <typename T>
-void norm2_of(MailleGpuHandle* h, const T* v, int64_t n, double* out);
-
-template <>
-void norm2_of<double>(MailleGpuHandle* h, const double* v, int64_t n, double* out) {
-    launch_norm2(n, v, h->partials, h->dticket, out, 148 * 4, h->st);
+// One PCG iteration (Pcg::solve loop body, iterative.rs:223-242).
+// Plain form: ap = K p, x/r update + stopping test, z = M^-1 r, beta, p.
+// Mixed form: the same in FP32 on the FP32 matrix and factor, plus a reliable update (x64 +=
+// x32, r64 = b - K64 x64 against the FP64 matrix, r32 = r64) on the iterations that raise it.
+void enqueue_iteration(MailleGpuHandle* h) {
+    const int32_t nb = h->sym.nb;
+    const SellDev Kd = h->sk.dev();
+    if (is_mixed(h)) {
+        launch_spmv<float>(Kd, h->Ks32, h->p32, h->ap32, h->scal, h->partials, h->spmv_grid, false, h->st);
+        launch_axpy<float>(nb, h->x32, h->r32, h->p32, h->ap32, h->scal, h->partials, true, h->st);
+        launch_upd_x(nb, h->x64, h->x32, h->scal, h->st);
+        launch_upd_r(Kd, h->Ks64, h->b64, h->x64, h->r64, h->scal, h->partials, h->spmv_grid, h->st);
+        launch_upd_cast(nb, h->r64, h->r32, h->scal, h->st);
+    } else {
+        launch_spmv<double>(Kd, h->Ks64, h->p64, h->ap64, h->scal, h->partials, h->spmv_grid, false, h->st);
+        launch_axpy<double>(nb, h->x64, h->r64, h->p64, h->ap64, h->scal, h->partials, false, h->st);
+    }
+    enqueue_precondition(h);
 }
 
-}  // namespace
-
-namespace {
-
-template <>
-void norm2_of<float>(MailleGpuHandle* h, const float* v, int64_t n, double* out) {
-    launch_norm2_f(n, v, h->partials, h->dticket, out, 148 * 4, h->st);
-}
-
-// PCG on K x = b with the IC(0) factor F (both of type T): x, r, z, p, ap of `v`.
-// Returns the MailleStatus and the iteration count.
-template <typename T>
-int32_t run_pcg(MailleGpuHandle* h, const T* K, const T* F, PcgVecs<T>& v, double tol,
-                int32_t max_iter, int32_t* iterations, double* rel_res) {
-    const int64_t n = 3 * (int64_t)h->sym.nb;
-    const int L = h->sym.levels;
-    const Pattern pt = h->pattern();
-    CK(cudaMemsetAsync(v.x, 0, n * sizeof(T), h->st));
-    CK(cudaMemsetAsync(v.p, 0, n * sizeof(T), h->st));
-    CK(cudaMemsetAsync(v.ap, 0, n * sizeof(T), h->st));
-    CK(cudaMemcpyAsync(v.r, v.b, n * sizeof(T), cudaMemcpyDeviceToDevice, h->st));
-    norm2_of<T>(h, v.b, n, &h->scal->bb);
-    launch_pcg_init(h->scal, tol, max_iter, h->st);
-    // z = M^-1 b, rz = b.z, p = z (iterative.rs:217-220): the sweeps with alpha = 0
-    for (int l = 0; l < L; ++l)
-        launch_fwd<T>(pt, h->sym.level_ptr[l], h->sym.level_ptr[l + 1], l, L, F, v.r, v.z, v.x,
-                      v.p, v.ap, h->scal, h->partials, h->lvl_total, h->lvl_grid[l], h->st);
-    for (int l = L - 1; l >= 0; --l)
-        launch_bwd<T>(pt, h->sym.level_ptr[l], h->sym.level_ptr[l + 1], l, F, v.r, v.z, h->scal,
-                      h->partials, h->lvl_total + kMaxLevels, L, h->lvl_grid[l], h->st);
-    launch_pupdate<T>(n, v.z, v.p, h->scal, h->st);
+// PCG on K x = b64 (b64 in padded solver numbering) into x64. Returns the MailleStatus.
+int32_t run_pcg(MailleGpuHandle* h, int32_t* iterations, int32_t* updates, double* rel_res) {
+    const int64_t n4 = 4 * (int64_t)h->sym.nb;
+    cudaStream_t st = h->st;
+    const bool mixed = is_mixed(h);
+    CK(cudaMemsetAsync(h->x64, 0, n4 * sizeof(double), st));
+    CK(cudaMemcpyAsync(h->r64, h->b64, n4 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    launch_norm2<double>(n4, h->b64, h->partials, h->dticket, &h->scal->bb, st);
+    launch_pcg_init(h->scal, h->tol, h->max_iter, mixed ? h->delta : 0.0, st);
+    if (mixed) {
+        for (float* q : {h->x32, h->p32, h->ap32}) CK(cudaMemsetAsync(q, 0, n4 * sizeof(float), st));
+        launch_cast(n4, h->b64, h->r32, st);
+    } else {
+        for (double* q : {h->p64, h->ap64}) CK(cudaMemsetAsync(q, 0, n4 * sizeof(double), st));
+    }
+    // z = M^-1 b, rz = b.z, p = z (iterative.rs:217-220)
+    enqueue_precondition(h);
     CK(cudaGetLastError());
-
-    const int gi = std::is_same<T, double>::value ? 0 : 1;
-    // the graph bakes in the vector and matrix pointers of this precision
-    if (!h->graph[gi]) {
+    if (!h->graph) {
         cudaGraph_t g;
         const long long before = g_kernel_launches.load();
-        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < h->graph_iters; ++k) enqueue_iteration<T>(h, K, F, v);
-        CK(cudaStreamEndCapture(h->st, &g));
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < h->graph_iters; ++k) enqueue_iteration(h);
+        CK(cudaStreamEndCapture(st, &g));
         h->graph_kernels = g_kernel_launches.load() - before;
         g_kernel_launches.store(before);  // captured, not launched
-        CK(cudaGraphInstantiate(&h->graph[gi], g, 0));
+        CK(cudaGraphInstantiate(&h->graph, g, 0));
         cudaGraphDestroy(g);
     }
     int32_t status = MAILLE_OK;
     for (;;) {
-        CK(cudaGraphLaunch(h->graph[gi], h->st));
+        CK(cudaGraphLaunch(h->graph, st));
         g_kernel_launches.fetch_add(h->graph_kernels);
-        CK(cudaMemcpyAsync(h->h_scal, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, h->st));
-        CK(cudaStreamSynchronize(h->st));
+        CK(cudaMemcpyAsync(h->h_scal, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
         const PcgScalars& s = *h->h_scal;
         if (s.done) {
             status = s.status == 1 ? MAILLE_SINGULAR : (s.status == 2 ? MAILLE_NOT_CONVERGED : MAILLE_OK);
@@ -259,14 +286,15 @@ int32_t run_pcg(MailleGpuHandle* h, const T* K, const T* F, PcgVecs<T>& v, doubl
             status = MAILLE_CANCELLED;
             break;
         }
-        if (s.iter >= max_iter) {
+        if (s.iter >= h->max_iter + 1) {  // the device test stops at the cap; this is a guard
             status = MAILLE_NOT_CONVERGED;
             break;
         }
     }
     const PcgScalars& s = *h->h_scal;
     *iterations = s.iter;
-    *rel_res = s.bb > 0 ? std::sqrt(s.rr / s.bb) : 0.0;
+    *updates = mixed ? s.updates : 1;
+    *rel_res = s.bb > 0 ? std::sqrt((mixed ? s.rr_true : s.rr) / s.bb) : 0.0;
     return status;
 }
 
@@ -284,6 +312,10 @@ bool check_problem(const MailleElasticProblem* p, Error& err) {
     }
     if (!p->coords || !p->conn || !p->young || !p->poisson) {
         err = {MAILLE_INVALID_INPUT, "coords, conn, young and poisson are required"};
+        return false;
+    }
+    if (p->precision != MAILLE_FP64 && p->precision != MAILLE_MIXED) {
+        err = {MAILLE_INVALID_INPUT, "unknown precision"};
         return false;
     }
     for (int64_t k = 0; k < 3 * p->n_nodes; ++k)
@@ -312,7 +344,7 @@ bool check_problem(const MailleElasticProblem* p, Error& err) {
     return true;
 }
 
-// Builds b (solver numbering) from the load vector on the device (h->f) and K_fc u_c.
+// b64 (padded solver numbering) from the current load vector and K_fc u_c.
 void build_rhs(MailleGpuHandle* h) {
     const double* coupling = nullptr;
     if (h->any_imposed) {
@@ -324,7 +356,7 @@ void build_rhs(MailleGpuHandle* h) {
                            h->elem_slot, h->ye, h->y_full, h->st);
         coupling = h->y_full;
     }
-    launch_build_rhs(h->sym.nb, h->perm, h->fixmask, h->f_cur, coupling, h->v64.b, h->st);
+    launch_build_rhs(h->sym.nb, h->perm, h->fixmask, h->f_cur, coupling, h->b64, h->st);
 }
 
 int32_t factorize(MailleGpuHandle* h, Error& err) {
@@ -347,23 +379,37 @@ int32_t factorize(MailleGpuHandle* h, Error& err) {
     return MAILLE_SINGULAR;
 }
 
-// Element integration + scatter-reduce assembly + IC(0) (+ FP32 copies), all on the device.
+// Element integration + scatter-reduce assembly + IC(0), then the sliced copies the
+// iterations read (FP64 for the plain form; FP32 K, L, L^T, D and the FP64 K for the mixed one).
 int32_t numeric_phase(MailleGpuHandle* h, Error& err) {
     const Symbolic& s = h->sym;
+    cudaStream_t st = h->st;
     ElemIn in{h->n_elems, h->coords, h->conn, h->young, h->poisson};
-    launch_elem_stiffness(h->npe, in, h->ke, h->st);
+    launch_elem_stiffness(h->npe, in, h->ke, st);
     launch_assemble(h->pattern(), (int64_t)s.lslot.size(), h->lslot, h->lrow, h->lptr, h->contrib,
-                    h->ke, h->K, h->st);
+                    h->ke, h->K, st);
+    launch_sell_fill<double>(h->sk.h.steps(), h->sk.src, h->K, h->Ks64, st);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(h->ev[2], h->st));
+    CK(cudaEventRecord(h->ev[2], st));
     if (factorize(h, err) != MAILLE_OK) return err.status;
-    if (h->precision == MAILLE_MIXED) {
-        launch_to_float((int64_t)s.blocks * 9, h->K, h->K32, h->st);
-        launch_to_float((int64_t)s.blocks * 9, h->F, h->F32, h->st);
-        CK(cudaGetLastError());
+    if (is_mixed(h)) {
+        launch_sell_fill<float>(h->sk.h.steps(), h->sk.src, h->K, h->Ks32, st);
+        launch_sell_fill<float>(h->sl.h.steps(), h->sl.src, h->F, h->Ls32, st);
+        launch_sell_fill<float>(h->su.h.steps(), h->su.src, h->F, h->Us32, st);
+        launch_diag_fill<float>(s.nb, h->diag, h->F, h->D32, st);
+    } else {
+        launch_sell_fill<double>(h->sl.h.steps(), h->sl.src, h->F, h->Ls64, st);
+        launch_sell_fill<double>(h->su.h.steps(), h->su.src, h->F, h->Us64, st);
+        launch_diag_fill<double>(s.nb, h->diag, h->F, h->D64, st);
     }
-    CK(cudaEventRecord(h->ev[3], h->st));
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->ev[3], st));
     return MAILLE_OK;
+}
+
+int env_int(const char* name, int dflt) {
+    const char* e = std::getenv(name);
+    return e ? std::atoi(e) : dflt;
 }
 
 int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, MailleElasticResult* res) {
@@ -379,8 +425,8 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
     h->precision = p->precision;
     h->tol = p->rel_tol > 0 ? p->rel_tol : kDefaultTol;
     h->max_iter = p->max_iter > 0 ? p->max_iter : kDefaultMaxIter;
-    if (const char* e = std::getenv("MAILLE_INNER_TOL")) h->inner_tol = std::atof(e);
-    if (const char* e = std::getenv("MAILLE_GRAPH_ITERS")) h->graph_iters = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("MAILLE_RELIABLE_DELTA")) h->delta = std::atof(e);
+    h->graph_iters = std::max(1, env_int("MAILLE_GRAPH_ITERS", h->graph_iters));
     const int64_t n3 = 3 * p->n_nodes;
     h->h_fixed.assign(n3, 0);
     if (p->fixed)
@@ -400,6 +446,9 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
                  h->sym, err))
         return fail(err);
     if (h->sym.levels >= kMaxLevels) return fail({MAILLE_INVALID_INPUT, "too many IC(0) levels"});
+    build_sell(h->sym, SELL_FULL, env_int("MAILLE_LPR_K", 0), h->sk.h);
+    build_sell(h->sym, SELL_LOWER, env_int("MAILLE_LPR_LU", 0), h->sl.h);
+    build_sell(h->sym, SELL_UPPER, env_int("MAILLE_LPR_LU", 0), h->su.h);
     const double t_setup1 = now_ms();
     try {
         int ndev = 0;
@@ -450,20 +499,25 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         std::vector<int32_t> slot(p->n_elems, -1);
         for (size_t k = 0; k < s.belem.size(); ++k) slot[s.belem[k]] = (int32_t)k;
         h->elem_slot = dupload(slot.data(), slot.size(), st);
+        for (SellBuf* b : {&h->sk, &h->sl, &h->su}) b->upload(st);
         // numeric buffers
         const int np = node_pairs(h->npe);
-        const int64_t n = 3 * (int64_t)s.nb;
+        const int64_t n4 = 4 * (int64_t)s.nb;
         h->ke = dalloc<double>((size_t)p->n_elems * np * 9);
         h->K = dalloc<double>((size_t)s.blocks * 9);
         h->F = dalloc<double>((size_t)s.blocks * 9);
-        for (double** q : {&h->v64.b, &h->v64.x, &h->v64.r, &h->v64.z, &h->v64.p, &h->v64.ap})
-            *q = dalloc<double>(n);
-        if (h->precision == MAILLE_MIXED) {
-            h->K32 = dalloc<float>((size_t)s.blocks * 9);
-            h->F32 = dalloc<float>((size_t)s.blocks * 9);
-            for (float** q : {&h->v32.b, &h->v32.x, &h->v32.r, &h->v32.z, &h->v32.p, &h->v32.ap})
-                *q = dalloc<float>(n);
-            h->rr64 = dalloc<double>(n);
+        h->Ks64 = dalloc<double>((size_t)h->sk.h.steps() * 9 * kStepSlots);
+        for (double** q : {&h->b64, &h->x64, &h->r64, &h->z64, &h->p64, &h->ap64}) *q = dalloc<double>(n4);
+        if (is_mixed(h.get())) {
+            h->Ks32 = dalloc<float>((size_t)h->sk.h.steps() * 9 * kStepSlots);
+            h->Ls32 = dalloc<float>((size_t)h->sl.h.steps() * 9 * kStepSlots);
+            h->Us32 = dalloc<float>((size_t)h->su.h.steps() * 9 * kStepSlots);
+            h->D32 = dalloc<float>((size_t)s.nb * 9);
+            for (float** q : {&h->x32, &h->r32, &h->z32, &h->p32, &h->ap32}) *q = dalloc<float>(n4);
+        } else {
+            h->Ls64 = dalloc<double>((size_t)h->sl.h.steps() * 9 * kStepSlots);
+            h->Us64 = dalloc<double>((size_t)h->su.h.steps() * 9 * kStepSlots);
+            h->D64 = dalloc<double>((size_t)s.nb * 9);
         }
         h->u_full = dalloc<double>(n3);
         h->y_full = dalloc<double>(n3);
@@ -474,17 +528,14 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         CK(cudaMallocHost(&h->h_scal, sizeof(PcgScalars)));
         CK(cudaMallocHost(&h->h_sum, 4 * sizeof(double)));
         h->partials = dalloc<double>(148 * 16);
-        h->lvl_total = dalloc<double>(2 * kMaxLevels);
+        h->lvl_total = dalloc<double>(kMaxLevels);
         h->dsum = dalloc<double>(4);
         h->dticket = dalloc<unsigned int>(1);
         CK(cudaMemsetAsync(h->dticket, 0, sizeof(unsigned int), st));
         h->dfail = dalloc<int32_t>(1);
-        h->spmv_grid = grid_for_rows(s.nb);
-        h->lvl_grid.resize(s.levels);
-        for (int l = 0; l < s.levels; ++l)
-            h->lvl_grid[l] = grid_for_rows(s.level_ptr[l + 1] - s.level_ptr[l]);
+        h->spmv_grid = grid_for_slices(h->sk.h.nslices());
         // graph size: keep a few thousand kernel nodes at most
-        const int per_iter = 2 * s.levels + 2;
+        const int per_iter = 2 * s.levels + 6;
         h->graph_iters = std::max(1, std::min(h->graph_iters, 4000 / per_iter));
         CK(cudaEventRecord(h->ev[1], st));
         if (numeric_phase(h.get(), err) != MAILLE_OK) return fail(err);
@@ -502,6 +553,17 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
     return MAILLE_OK;
 }
 
+const char* status_message(int32_t status, int32_t iters, double rel) {
+    static thread_local std::string m;
+    if (status == MAILLE_SINGULAR) m = "Singular: IC(0)-PCG met p.Ap <= 0 or NaN";
+    else if (status == MAILLE_NOT_CONVERGED)
+        m = "IterativeNotConverged: iterations " + std::to_string(iters) + ", relative residual " +
+            std::to_string(rel);
+    else if (status == MAILLE_CANCELLED) m = "Cancelled";
+    else m = "";
+    return m.c_str();
+}
+
 int32_t solve_impl(MailleGpuHandle* h, const double* f, MailleElasticResult* res) {
     if (!h) return fail({MAILLE_INVALID_INPUT, "null handle"});
     try {
@@ -509,8 +571,6 @@ int32_t solve_impl(MailleGpuHandle* h, const double* f, MailleElasticResult* res
         cudaStream_t st = h->st;
         const Symbolic& s = h->sym;
         const int64_t n3 = 3 * h->n_nodes;
-        const int64_t n = 3 * (int64_t)s.nb;
-        const double t0 = now_ms();
         if (f) {
             for (int64_t k = 0; k < n3; ++k)
                 if (!std::isfinite(f[k])) return fail({MAILLE_INVALID_INPUT, "non-finite load"});
@@ -523,49 +583,9 @@ int32_t solve_impl(MailleGpuHandle* h, const double* f, MailleElasticResult* res
         }
         CK(cudaEventRecord(h->ev[4], st));
         build_rhs(h);
-        int32_t status = MAILLE_OK, iters = 0, outer = 1;
+        int32_t iters = 0, outer = 1;
         double rel = 0.0;
-        if (h->precision == MAILLE_MIXED) {
-            // FP64 iterative refinement around an FP32 IC(0)-PCG
-            norm2_of<double>(h, h->v64.b, n, h->dsum + 1);
-            CK(cudaMemsetAsync(h->v64.x, 0, n * sizeof(double), st));
-            CK(cudaMemcpyAsync(h->h_sum + 1, h->dsum + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            const double bb = h->h_sum[1];
-            outer = 0;
-            if (bb > 0.0) {
-                for (;;) {
-                    launch_residual64(h->pattern(), h->K, h->v64.b, h->v64.x, h->rr64, h->partials,
-                                      h->dticket, h->dsum, h->spmv_grid, st);
-                    CK(cudaMemcpyAsync(h->h_sum, h->dsum, sizeof(double), cudaMemcpyDeviceToHost, st));
-                    CK(cudaStreamSynchronize(st));
-                    rel = std::sqrt(h->h_sum[0] / bb);
-                    if (!(rel == rel)) {
-                        status = MAILLE_SINGULAR;
-                        break;
-                    }
-                    if (std::sqrt(h->h_sum[0]) <= h->tol * std::sqrt(bb)) break;
-                    if (outer >= h->max_outer || iters >= h->max_iter) {
-                        status = MAILLE_NOT_CONVERGED;
-                        break;
-                    }
-                    launch_scale_to_float(n, h->rr64, h->dsum, h->v32.b, st);
-                    int32_t it = 0;
-                    double inner_rel = 0.0;
-                    const int32_t st_in = run_pcg<float>(h, h->K32, h->F32, h->v32, h->inner_tol,
-                                                         h->max_iter - iters, &it, &inner_rel);
-                    iters += it;
-                    ++outer;
-                    if (st_in == MAILLE_SINGULAR || st_in == MAILLE_CANCELLED) {
-                        status = st_in;
-                        break;
-                    }
-                    launch_accumulate(n, h->v32.x, h->dsum, h->v64.x, st);
-                }
-            }
-        } else {
-            status = run_pcg<double>(h, h->K, h->F, h->v64, h->tol, h->max_iter, &iters, &rel);
-        }
+        const int32_t status = run_pcg(h, &iters, &outer, &rel);
         CK(cudaEventRecord(h->ev[5], st));
         if (res) {
             res->iterations = iters;
@@ -579,15 +599,11 @@ int32_t solve_impl(MailleGpuHandle* h, const double* f, MailleElasticResult* res
         }
         if (status != MAILLE_OK) {
             CK(cudaStreamSynchronize(st));
-            if (status == MAILLE_SINGULAR) set_error("Singular: IC(0)-PCG met p.Ap <= 0 or NaN");
-            else if (status == MAILLE_NOT_CONVERGED)
-                set_error("IterativeNotConverged: iterations " + std::to_string(iters) +
-                          ", relative residual " + std::to_string(rel));
-            else if (status == MAILLE_CANCELLED) set_error("Cancelled");
+            set_error(status_message(status, iters, rel));
             return status;
         }
         // u in caller numbering, reactions, stresses
-        launch_gather_u(h->n_nodes, h->inv, h->fixed, h->imposed, h->v64.x, h->u_full, st);
+        launch_gather_u(h->n_nodes, h->inv, h->fixed, h->imposed, h->x64, h->u_full, st);
         CK(cudaMemsetAsync(h->react, 0, n3 * sizeof(double), st));
         if (!s.belem.empty()) {
             CK(cudaMemsetAsync(h->y_full, 0, n3 * sizeof(double), st));
@@ -632,7 +648,6 @@ int32_t solve_impl(MailleGpuHandle* h, const double* f, MailleElasticResult* res
                             if (h->h_fixed[3 * v + c]) res->reactions[3 * v + c] = -h->h_f[3 * v + c];
             }
         }
-        (void)t0;
         h->solved = true;
     } catch (const CudaFailure& e) {
         return fail({MAILLE_CUDA_ERROR, e.what});
@@ -646,64 +661,27 @@ int32_t backward_impl(MailleGpuHandle* h, const double* dJdu, double* dJdE, doub
     try {
         CK(cudaSetDevice(h->device));
         cudaStream_t st = h->st;
-        const Symbolic& s = h->sym;
         const int64_t n3 = 3 * h->n_nodes;
-        const int64_t n = 3 * (int64_t)s.nb;
         for (int64_t k = 0; k < n3; ++k)
             if (!std::isfinite(dJdu[k])) return fail({MAILLE_INVALID_INPUT, "non-finite dJ/du"});
-        // adjoint right-hand side: g at free DOFs (no coupling term: lambda_c = 0)
+        // adjoint right-hand side g at free DOFs; lambda = 0 at fixed DOFs (no coupling term)
         CK(cudaMemcpyAsync(h->y_full, dJdu, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
-        launch_build_rhs(s.nb, h->perm, h->fixmask, h->y_full, nullptr, h->v64.b, st);
-        // K is symmetric: the same PCG and factor solve K lambda = g (saved u is kept in u_full)
+        launch_build_rhs(h->sym.nb, h->perm, h->fixmask, h->y_full, nullptr, h->b64, st);
         if (!h->lambda_full) {
             h->lambda_full = dalloc<double>(n3);
             h->grad = dalloc<double>(h->n_elems);
         }
-        int32_t iters = 0;
+        // K is symmetric: the same PCG and factor solve K lambda = g (u stays in u_full)
+        int32_t iters = 0, outer = 0;
         double rel = 0.0;
-        int32_t status;
-        if (h->precision == MAILLE_MIXED) {
-            // refinement as in the forward solve
-            norm2_of<double>(h, h->v64.b, n, h->dsum + 1);
-            CK(cudaMemsetAsync(h->v64.x, 0, n * sizeof(double), st));
-            CK(cudaMemcpyAsync(h->h_sum + 1, h->dsum + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            const double bb = h->h_sum[1];
-            status = MAILLE_OK;
-            int outer = 0;
-            while (bb > 0.0) {
-                launch_residual64(h->pattern(), h->K, h->v64.b, h->v64.x, h->rr64, h->partials,
-                                  h->dticket, h->dsum, h->spmv_grid, st);
-                CK(cudaMemcpyAsync(h->h_sum, h->dsum, sizeof(double), cudaMemcpyDeviceToHost, st));
-                CK(cudaStreamSynchronize(st));
-                if (std::sqrt(h->h_sum[0]) <= h->tol * std::sqrt(bb)) break;
-                if (outer >= h->max_outer || iters >= h->max_iter) {
-                    status = MAILLE_NOT_CONVERGED;
-                    break;
-                }
-                launch_scale_to_float(n, h->rr64, h->dsum, h->v32.b, st);
-                int32_t it = 0;
-                double ir = 0;
-                const int32_t si = run_pcg<float>(h, h->K32, h->F32, h->v32, h->inner_tol,
-                                                  h->max_iter - iters, &it, &ir);
-                iters += it;
-                ++outer;
-                if (si == MAILLE_SINGULAR || si == MAILLE_CANCELLED) {
-                    status = si;
-                    break;
-                }
-                launch_accumulate(n, h->v32.x, h->dsum, h->v64.x, st);
-            }
-        } else {
-            status = run_pcg<double>(h, h->K, h->F, h->v64, h->tol, h->max_iter, &iters, &rel);
-        }
+        const int32_t status = run_pcg(h, &iters, &outer, &rel);
         if (status != MAILLE_OK) {
-            set_error("adjoint solve failed");
+            CK(cudaStreamSynchronize(st));
+            set_error(std::string("adjoint solve: ") + status_message(status, iters, rel));
             return status;
         }
-        // lambda in caller numbering (0 at fixed DOFs), then the element gradient
         CK(cudaMemsetAsync(h->y_full, 0, n3 * sizeof(double), st));
-        launch_gather_u(h->n_nodes, h->inv, h->fixed, h->y_full, h->v64.x, h->lambda_full, st);
+        launch_gather_u(h->n_nodes, h->inv, h->fixed, h->y_full, h->x64, h->lambda_full, st);
         launch_adjoint_grad(h->npe, h->n_elems, h->conn, h->ke, h->young, h->lambda_full, h->u_full,
                             h->grad, st);
         CK(cudaGetLastError());
@@ -795,21 +773,17 @@ int32_t maille_gpu_refactor(MailleGpuHandle* h, const double* young, const doubl
 int32_t maille_gpu_spmv_device(MailleGpuHandle* h, int32_t precision, int32_t count) {
     g_last_error.clear();
     if (!h || count < 0) return fail({MAILLE_INVALID_INPUT, "null handle or negative count"});
-    if (precision == MAILLE_MIXED && !h->K32)
+    if (precision == MAILLE_MIXED && !h->Ks32)
         return fail({MAILLE_INVALID_INPUT, "the handle holds no FP32 matrix"});
     try {
         CK(cudaSetDevice(h->device));
-        if (!h->spmv_scal) {
-            h->spmv_scal = dalloc<PcgScalars>(1);
-            CK(cudaMemsetAsync(h->spmv_scal, 0, sizeof(PcgScalars), h->st));
-        }
         for (int32_t k = 0; k < count; ++k) {
             if (precision == MAILLE_MIXED)
-                launch_spmv_pcg<float>(h->pattern(), h->K32, h->v32.p, h->v32.ap, h->spmv_scal,
-                                       h->partials, h->spmv_grid, h->st);
+                launch_spmv<float>(h->sk.dev(), h->Ks32, h->p32, h->ap32, h->scal, h->partials,
+                                   h->spmv_grid, true, h->st);
             else
-                launch_spmv_pcg<double>(h->pattern(), h->K, h->v64.p, h->v64.ap, h->spmv_scal,
-                                        h->partials, h->spmv_grid, h->st);
+                launch_spmv<double>(h->sk.dev(), h->Ks64, h->p64, h->ap64, h->scal, h->partials,
+                                    h->spmv_grid, true, h->st);
         }
         CK(cudaGetLastError());
     } catch (const CudaFailure& e) {
@@ -825,16 +799,11 @@ int32_t maille_gpu_multiply(MailleGpuHandle* h, const double* x, double* y) {
         CK(cudaSetDevice(h->device));
         const int64_t n3 = 3 * h->n_nodes;
         CK(cudaMemcpyAsync(h->y_full, x, n3 * sizeof(double), cudaMemcpyHostToDevice, h->st));
-        launch_build_rhs(h->sym.nb, h->perm, h->fixmask, h->y_full, nullptr, h->v64.p, h->st);
-        if (!h->spmv_scal) {
-            h->spmv_scal = dalloc<PcgScalars>(1);
-            CK(cudaMemsetAsync(h->spmv_scal, 0, sizeof(PcgScalars), h->st));
-        }
-        launch_spmv_pcg<double>(h->pattern(), h->K, h->v64.p, h->v64.ap, h->spmv_scal, h->partials,
-                                h->spmv_grid, h->st);
-        CK(cudaMemsetAsync(h->u_full, 0, n3 * sizeof(double), h->st));
+        launch_build_rhs(h->sym.nb, h->perm, h->fixmask, h->y_full, nullptr, h->p64, h->st);
+        launch_spmv<double>(h->sk.dev(), h->Ks64, h->p64, h->ap64, h->scal, h->partials,
+                            h->spmv_grid, true, h->st);
         CK(cudaMemsetAsync(h->react, 0, n3 * sizeof(double), h->st));
-        launch_gather_u(h->n_nodes, h->inv, h->fixed, h->react, h->v64.ap, h->y_full, h->st);
+        launch_gather_u(h->n_nodes, h->inv, h->fixed, h->react, h->ap64, h->y_full, h->st);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(y, h->y_full, n3 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
         CK(cudaStreamSynchronize(h->st));

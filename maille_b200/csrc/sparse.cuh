@@ -1,0 +1,74 @@
+// sparse.cuh -- sliced 3x3-block layout (SELL) and the PCG kernels that run on it.
+//
+// Layout. Rows of one level are cut into warp slices of 32/lpr rows (lpr = lanes per row); in a
+// slice every step holds 128 slots, 4 consecutive slots per lane, so a lane reads the 9 values
+// of its 4 blocks as 9 128-bit loads (float4, or two double2) and their 4 node columns as one
+// int4. Value plane k of step g is vals[(g * 9 + k) * 128 + slot]: every load instruction of the
+// warp reads 512 (FP32) or 1024 (FP64) contiguous bytes. A row's blocks are spread over its lpr
+// lanes; the lanes of a row are summed with shuffles. Rows inside a level are sorted by length
+// (descending) per layout, which keeps the padding of a slice small; rowid maps slice rows to
+// matrix rows. Vectors are padded to 4 entries per node, so the x of one block is one 16-byte
+// gather (FP32) or a 16 + 8-byte gather (FP64).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace maille {
+
+constexpr int kLaneSlots = 4;    // slots (blocks) per lane per step
+constexpr int kStepSlots = 128;  // 32 lanes x kLaneSlots
+
+struct SellDev {
+    int32_t lpr;            // lanes per row: 1, 2, 4 or 8
+    int32_t nslices;
+    const int32_t* rowid;   // [nslices * 32 / lpr] matrix row of each slice row, -1 when empty
+    const int64_t* off;     // [nslices + 1] first step of each slice
+    const int32_t* col;     // [steps * 128] node column of each slot
+};
+
+// Device-resident scalars of one PCG run.
+struct PcgScalars {
+    double alpha, beta, rz, rr, bb, tol, pap;
+    double maxr, delta, rr_true;  // reliable updates (mixed form)
+    int32_t iter, max_iter, done, status;  // status: 0 ok, 1 singular (also NaN), 2 cap reached
+    int32_t update, updates;
+    unsigned int ticket[4];
+};
+
+template <typename T>
+void launch_spmv(const SellDev& A, const T* vals, const T* p, T* ap, PcgScalars* s,
+                 double* partials, int grid, bool standalone, cudaStream_t st);
+template <typename T>
+void launch_axpy(int32_t nb, T* x, T* r, const T* p, const T* ap, PcgScalars* s,
+                 double* partials, bool mixed, cudaStream_t st);
+void launch_upd_x(int32_t nb, double* x64, float* x32, PcgScalars* s, cudaStream_t st);
+void launch_upd_r(const SellDev& A, const double* vals, const double* b, const double* x64,
+                  double* r64, PcgScalars* s, double* partials, int grid, cudaStream_t st);
+void launch_upd_cast(int32_t nb, const double* r64, float* r32, PcgScalars* s, cudaStream_t st);
+template <typename T>
+void launch_fwd(const SellDev& L, int32_t s0, int32_t s1, const T* vals, const T* D, int32_t nb,
+                const T* r, T* y, PcgScalars* s, cudaStream_t st);
+template <typename T>
+void launch_bwd(const SellDev& U, int32_t s0, int32_t s1, int level, int nlevels, const T* vals,
+                const T* D, int32_t nb, const T* r, T* z, PcgScalars* s, double* partials,
+                double* lvl_total, cudaStream_t st);
+template <typename T>
+void launch_pupdate(int32_t nb, const T* z, T* p, PcgScalars* s, cudaStream_t st);
+void launch_pcg_init(PcgScalars* s, double tol, int32_t max_iter, double delta, cudaStream_t st);
+template <typename T>
+void launch_norm2(int64_t n, const T* v, double* partials, unsigned int* ticket, double* out,
+                  cudaStream_t st);
+// r = b - A u in FP64 with ||r||^2 into *out (A: SELL FP64)
+void launch_residual64(const SellDev& A, const double* vals, const double* b, const double* u,
+                       double* r, double* partials, unsigned int* ticket, double* out, int grid,
+                       cudaStream_t st);
+// vals[slot layout] = csr[src[slot]] (9 entries per block, 0 for padding)
+template <typename T>
+void launch_sell_fill(int64_t steps, const int32_t* src, const double* csr, T* vals, cudaStream_t st);
+// D[k * nb + i] = F[diag[i] * 9 + k]
+template <typename T>
+void launch_diag_fill(int32_t nb, const int64_t* diag, const double* F, T* D, cudaStream_t st);
+void launch_cast(int64_t n, const double* a, float* b, cudaStream_t st);
+
+}  // namespace maille
