@@ -62,6 +62,7 @@ struct Symbolic {
 // lower blocks) or U (strictly upper blocks, holding L^T). Slices never cross a level; inside a
 // level rows are taken by decreasing length. src maps each slot to its block in the CSR
 // pattern (-1 for padding), so the numeric values are filled by one gather per assembly.
+// Padding slots point at column nb, a dummy node whose vector entries stay 0.
 struct SellHost {
     int32_t lpr = 1;
     std::vector<int32_t> rowid;         // [nslices * 32 / lpr], -1 when empty

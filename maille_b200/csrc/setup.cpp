@@ -347,8 +347,11 @@ void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out) {
     if (lpr <= 0) {
         const double total = kind == SELL_FULL ? (double)s.blocks : (double)(s.blocks - s.nb) / 2.0;
         const double mean = total / std::max<int32_t>(1, s.nb);
+        // K: ~4 steps of 4 slots per lane; L and U: ~1 step, which puts more and shorter
+        // slices in flight for the sweeps
         lpr = 1;
-        while (lpr < 8 && mean / (2.0 * lpr) > 8.0) lpr *= 2;
+        const double per_lane = kind == SELL_FULL ? 16.0 : 4.0;
+        while (lpr < 4 && mean / lpr > per_lane) lpr *= 2;
     }
     out.lpr = lpr;
     const int S = 32 / lpr, per_step = 4 * lpr;
@@ -367,7 +370,7 @@ void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out) {
             const int64_t steps = (maxlen + per_step - 1) / per_step;
             const int64_t g0 = out.off.back();
             out.off.push_back(g0 + steps);
-            out.col.resize((size_t)(g0 + steps) * 128, rows[c0]);
+            out.col.resize((size_t)(g0 + steps) * 128, s.nb);  // padding: the dummy zero node
             out.src.resize((size_t)(g0 + steps) * 128, -1);
             for (int r = 0; r < S; ++r) out.rowid.push_back(c0 + r < c1 ? rows[c0 + r] : -1);
             for (size_t k = c0; k < c1; ++k) {

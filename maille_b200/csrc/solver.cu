@@ -143,7 +143,14 @@ struct MailleGpuHandle {
     unsigned int* dticket = nullptr;
     int32_t* dfail = nullptr;
     int spmv_grid = 1;
-    cudaGraphExec_t graph = nullptr;  // PCG iterations of the handle's form
+    cudaGraphExec_t graph = nullptr;  // PCG iterations of the handle's form (per-level launches)
+    int persist_grid = 0;             // > 0: the persistent cooperative kernel runs the PCG
+    int persist_chunk = 64;           // iterations per persistent launch
+    int32_t *lvl_l = nullptr, *lvl_u = nullptr;
+    unsigned long long* timing = nullptr;  // per-phase ns when MAILLE_PHASE_TIMING is set
+    int32_t* claim = nullptr;              // dataflow sweeps: claim counters [2] + timeout flag
+    unsigned int* flags = nullptr;         // row-ready flags [nb + 1] (the dummy's is always set)
+    int32_t* bwd_seq = nullptr;            // U slices by level, descending
     int graph_iters = 8;
     long long graph_kernels = 0;
     std::atomic<int> cancel{0};
@@ -165,12 +172,21 @@ void dfree(void* p) {
 
 MailleGpuHandle::~MailleGpuHandle() {
     cudaSetDevice(device);
+    if (timing) {
+        unsigned long long t[8] = {0};
+        cudaMemcpy(t, timing, sizeof(t), cudaMemcpyDeviceToHost);
+        std::fprintf(stderr,
+                     "maille phase timing (ms, block 0): spmv %.3f axpy %.3f update %.3f fwd %.3f "
+                     "bwd %.3f pupdate %.3f launches %llu grid %d\n",
+                     t[0] * 1e-6, t[1] * 1e-6, t[2] * 1e-6, t[3] * 1e-6, t[4] * 1e-6, t[5] * 1e-6,
+                     t[6], persist_grid);
+    }
     if (graph) cudaGraphExecDestroy(graph);
     void* bufs[] = {coords, young, poisson, imposed, f, f0, conn, fixed, perm, inv, col, lrow, fixmask,
                     row_ptr, diag, tpos, lslot, lptr, contrib, inc_ptr, inc, belem, bnodes,
                     elem_slot, ke, K, F, Ks64, Ls64, Us64, D64, Ks32, Ls32, Us32, D32, b64, x64,
                     r64, z64, p64, ap64, x32, r32, z32, p32, ap32, u_full, y_full, ye, gauss, vm,
-                    react, lambda_full, grad, scal, partials, lvl_total, dsum, dticket, dfail};
+                    react, lambda_full, grad, scal, partials, lvl_l, lvl_u, timing, claim, flags, bwd_seq, lvl_total, dsum, dticket, dfail};
     for (void* p : bufs) dfree(p);
     for (SellBuf* b : {&sk, &sl, &su}) b->release();
     if (h_scal) cudaFreeHost(h_scal);
@@ -242,6 +258,81 @@ void enqueue_iteration(MailleGpuHandle* h) {
     enqueue_precondition(h);
 }
 
+template <typename T>
+PcgArgs<T> pcg_args(MailleGpuHandle* h, const T* Kv, const T* Lv, const T* Uv, const T* D, T* x,
+                    T* r, T* z, T* p, T* ap) {
+    PcgArgs<T> a{};
+    a.nb = h->sym.nb;
+    a.levels = h->sym.levels;
+    a.chunk = h->persist_chunk;
+    a.K = h->sk.dev();
+    a.L = h->sl.dev();
+    a.U = h->su.dev();
+    a.lvl_l = h->lvl_l;
+    a.lvl_u = h->lvl_u;
+    a.Kv = Kv;
+    a.Lv = Lv;
+    a.Uv = Uv;
+    a.D = D;
+    a.x = x;
+    a.r = r;
+    a.z = z;
+    a.p = p;
+    a.ap = ap;
+    a.K64 = h->Ks64;
+    a.b64 = h->b64;
+    a.x64 = h->x64;
+    a.r64 = h->r64;
+    a.s = h->scal;
+    a.partials = h->partials;
+    a.timing = h->timing;
+    a.claim = h->claim;
+    a.flags = h->flags;
+    a.bwd_seq = h->bwd_seq;
+    return a;
+}
+
+// The PCG with the persistent cooperative kernel: one launch for the initial preconditioning,
+// then launches of `persist_chunk` iterations until the device flags the end.
+int32_t run_pcg_persistent(MailleGpuHandle* h, int32_t* iterations, int32_t* updates, double* rel_res) {
+    cudaStream_t st = h->st;
+    const bool mixed = is_mixed(h);
+    auto launch = [&](bool init) {
+        if (mixed) {
+            auto a = pcg_args<float>(h, h->Ks32, h->Ls32, h->Us32, h->D32, h->x32, h->r32, h->z32, h->p32, h->ap32);
+            CK((launch_pcg_persistent<float, true>(a, h->persist_grid, init, st)));
+        } else {
+            auto a = pcg_args<double>(h, h->Ks64, h->Ls64, h->Us64, h->D64, h->x64, h->r64, h->z64, h->p64, h->ap64);
+            CK((launch_pcg_persistent<double, false>(a, h->persist_grid, init, st)));
+        }
+    };
+    CK(cudaMemsetAsync(h->claim, 0, 4 * sizeof(int32_t), st));
+    launch(true);
+    int32_t status = MAILLE_OK;
+    for (;;) {
+        launch(false);
+        CK(cudaMemcpyAsync(h->h_scal, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        const PcgScalars& s = *h->h_scal;
+        if (s.done) {
+            status = s.status == 1 ? MAILLE_SINGULAR
+                   : s.status == 2 ? MAILLE_NOT_CONVERGED
+                   : s.status == 3 ? MAILLE_CUDA_ERROR
+                                   : MAILLE_OK;
+            break;
+        }
+        if (h->cancel.load()) {
+            status = MAILLE_CANCELLED;
+            break;
+        }
+    }
+    const PcgScalars& s = *h->h_scal;
+    *iterations = s.iter;
+    *updates = mixed ? s.updates : 1;
+    *rel_res = s.bb > 0 ? std::sqrt((mixed ? s.rr_true : s.rr) / s.bb) : 0.0;
+    return status;
+}
+
 // PCG on K x = b64 (b64 in padded solver numbering) into x64. Returns the MailleStatus.
 int32_t run_pcg(MailleGpuHandle* h, int32_t* iterations, int32_t* updates, double* rel_res) {
     const int64_t n4 = 4 * (int64_t)h->sym.nb;
@@ -257,6 +348,7 @@ int32_t run_pcg(MailleGpuHandle* h, int32_t* iterations, int32_t* updates, doubl
     } else {
         for (double* q : {h->p64, h->ap64}) CK(cudaMemsetAsync(q, 0, n4 * sizeof(double), st));
     }
+    if (h->persist_grid > 0) return run_pcg_persistent(h, iterations, updates, rel_res);
     // z = M^-1 b, rz = b.z, p = z (iterative.rs:217-220)
     enqueue_precondition(h);
     CK(cudaGetLastError());
@@ -502,18 +594,24 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         for (SellBuf* b : {&h->sk, &h->sl, &h->su}) b->upload(st);
         // numeric buffers
         const int np = node_pairs(h->npe);
-        const int64_t n4 = 4 * (int64_t)s.nb;
+        const int64_t n4 = 4 * ((int64_t)s.nb + 1);  // + the dummy node that padding points at
         h->ke = dalloc<double>((size_t)p->n_elems * np * 9);
         h->K = dalloc<double>((size_t)s.blocks * 9);
         h->F = dalloc<double>((size_t)s.blocks * 9);
         h->Ks64 = dalloc<double>((size_t)h->sk.h.steps() * 9 * kStepSlots);
-        for (double** q : {&h->b64, &h->x64, &h->r64, &h->z64, &h->p64, &h->ap64}) *q = dalloc<double>(n4);
+        for (double** q : {&h->b64, &h->x64, &h->r64, &h->z64, &h->p64, &h->ap64}) {
+            *q = dalloc<double>(n4);
+            CK(cudaMemsetAsync(*q, 0, n4 * sizeof(double), st));
+        }
         if (is_mixed(h.get())) {
             h->Ks32 = dalloc<float>((size_t)h->sk.h.steps() * 9 * kStepSlots);
             h->Ls32 = dalloc<float>((size_t)h->sl.h.steps() * 9 * kStepSlots);
             h->Us32 = dalloc<float>((size_t)h->su.h.steps() * 9 * kStepSlots);
             h->D32 = dalloc<float>((size_t)s.nb * 9);
-            for (float** q : {&h->x32, &h->r32, &h->z32, &h->p32, &h->ap32}) *q = dalloc<float>(n4);
+            for (float** q : {&h->x32, &h->r32, &h->z32, &h->p32, &h->ap32}) {
+                *q = dalloc<float>(n4);
+                CK(cudaMemsetAsync(*q, 0, n4 * sizeof(float), st));
+            }
         } else {
             h->Ls64 = dalloc<double>((size_t)h->sl.h.steps() * 9 * kStepSlots);
             h->Us64 = dalloc<double>((size_t)h->su.h.steps() * 9 * kStepSlots);
@@ -527,13 +625,37 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         CK(cudaMemsetAsync(h->scal, 0, sizeof(PcgScalars), st));
         CK(cudaMallocHost(&h->h_scal, sizeof(PcgScalars)));
         CK(cudaMallocHost(&h->h_sum, 4 * sizeof(double)));
-        h->partials = dalloc<double>(148 * 16);
+        h->partials = dalloc<double>(4 * 148 * 8);  // >= 4 slots x the persistent grid
         h->lvl_total = dalloc<double>(kMaxLevels);
         h->dsum = dalloc<double>(4);
         h->dticket = dalloc<unsigned int>(1);
         CK(cudaMemsetAsync(h->dticket, 0, sizeof(unsigned int), st));
         h->dfail = dalloc<int32_t>(1);
         h->spmv_grid = grid_for_slices(h->sk.h.nslices());
+        h->lvl_l = dupload(h->sl.h.level_slices.data(), h->sl.h.level_slices.size(), st);
+        {
+            std::vector<int32_t> seq;
+            const auto& us = h->su.h.level_slices;
+            for (int l = s.levels - 1; l >= 0; --l)
+                for (int32_t k = us[l]; k < us[l + 1]; ++k) seq.push_back(k);
+            h->bwd_seq = dupload(seq.data(), seq.size(), st);
+            std::vector<unsigned int> fl((size_t)s.nb + 1, 0u);
+            fl[s.nb] = 0xFFFFFFFFu;
+            h->flags = dupload(fl.data(), fl.size(), st);
+            h->claim = dalloc<int32_t>(4);
+            CK(cudaMemsetAsync(h->claim, 0, 4 * sizeof(int32_t), st));
+        }
+        h->lvl_u = dupload(h->su.h.level_slices.data(), h->su.h.level_slices.size(), st);
+        if (env_int("MAILLE_PERSISTENT", 1) && h->sl.h.lpr == h->su.h.lpr) {
+            h->persist_grid = is_mixed(h.get()) ? pcg_persistent_grid<float, true>(h->sk.h.lpr, h->sl.h.lpr)
+                                                : pcg_persistent_grid<double, false>(h->sk.h.lpr, h->sl.h.lpr);
+            h->persist_grid = std::min(h->persist_grid, 148 * 8);  // partials hold 4 x 1184 blocks
+        }
+        if (env_int("MAILLE_PHASE_TIMING", 0)) {
+            h->timing = dalloc<unsigned long long>(8);
+            CK(cudaMemsetAsync(h->timing, 0, 8 * sizeof(unsigned long long), st));
+        }
+        h->persist_chunk = std::max(1, env_int("MAILLE_PERSIST_CHUNK", h->persist_chunk));
         // graph size: keep a few thousand kernel nodes at most
         const int per_iter = 2 * s.levels + 6;
         h->graph_iters = std::max(1, std::min(h->graph_iters, 4000 / per_iter));

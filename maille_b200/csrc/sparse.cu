@@ -49,33 +49,90 @@ template <typename T>
 __device__ __forceinline__ void node3_rw(const T* x, int64_t i, T& a, T& b, T& d) {
     a = x[4 * i]; b = x[4 * i + 1]; d = x[4 * i + 2];
 }
+// the 4 padded entries of node i (plain loads / stores, 128-bit for FP32, 2 x 128-bit for FP64)
+struct F4 {
+    double v[4];
+};
+__device__ __forceinline__ F4 ld4(const float* x, int64_t i) {
+    const float4 q = *reinterpret_cast<const float4*>(x + 4 * i);
+    return F4{{q.x, q.y, q.z, q.w}};
+}
+__device__ __forceinline__ F4 ld4(const double* x, int64_t i) {
+    const double2 a = *reinterpret_cast<const double2*>(x + 4 * i);
+    const double2 b = *reinterpret_cast<const double2*>(x + 4 * i + 2);
+    return F4{{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ void st4(float* x, int64_t i, const F4& f) {
+    *reinterpret_cast<float4*>(x + 4 * i) = make_float4((float)f.v[0], (float)f.v[1], (float)f.v[2], (float)f.v[3]);
+}
+__device__ __forceinline__ void st4(double* x, int64_t i, const F4& f) {
+    *reinterpret_cast<double2*>(x + 4 * i) = make_double2(f.v[0], f.v[1]);
+    *reinterpret_cast<double2*>(x + 4 * i + 2) = make_double2(f.v[2], f.v[3]);
+}
 template <typename T>
 __device__ __forceinline__ void store_node(T* x, int64_t i, T a, T b, T d) {
     x[4 * i] = a; x[4 * i + 1] = b; x[4 * i + 2] = d; x[4 * i + 3] = T(0);
 }
 
-// acc += sum over the slice steps [g0, g1) of this lane's slots: V_b x[col_b] (3x3 blocks)
+// acc += this lane's 4 slots of step g: V_b x[col_b] (3x3 blocks)
+template <typename T>
+__device__ __forceinline__ void step_accum(const T* __restrict__ vals,
+                                           const int32_t* __restrict__ col, int64_t g,
+                                           const T* __restrict__ x, int lane, T& a0, T& a1, T& a2) {
+    const int4 c4 = __ldg(reinterpret_cast<const int4*>(col + g * kStepSlots + 4 * lane));
+    const T* V = vals + g * 9 * kStepSlots + 4 * lane;
+    T v[9][4];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) load4(V + k * kStepSlots, v[k]);
+    const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        T x0, x1, x2;
+        node3(x, cc[j], x0, x1, x2);
+        a0 += v[0][j] * x0 + v[1][j] * x1 + v[2][j] * x2;
+        a1 += v[3][j] * x0 + v[4][j] * x1 + v[5][j] * x2;
+        a2 += v[6][j] * x0 + v[7][j] * x1 + v[8][j] * x2;
+    }
+}
+
+// acc += sum over the slice steps [g0, g1) of this lane's slots
 template <typename T>
 __device__ __forceinline__ void slice_accum(const T* __restrict__ vals,
                                             const int32_t* __restrict__ col, int64_t g0, int64_t g1,
                                             const T* __restrict__ x, int lane, T& a0, T& a1, T& a2) {
 #pragma unroll 2
-    for (int64_t g = g0; g < g1; ++g) {
-        const int4 c4 = __ldg(reinterpret_cast<const int4*>(col + g * kStepSlots + 4 * lane));
-        const T* V = vals + g * 9 * kStepSlots + 4 * lane;
-        T v[9][4];
+    for (int64_t g = g0; g < g1; ++g) step_accum<T>(vals, col, g, x, lane, a0, a1, a2);
+}
+
+// Slice sum split across the kSweepWarps warps of a block: warp w takes steps g0 + w,
+// g0 + w + kSweepWarps, ...; the partial sums meet in shared memory and warp 0 returns the total
+// (the other warps return 0). Summation order is fixed, so results are deterministic.
+constexpr int kSweepWarps = 8;
+template <typename T>
+__device__ __forceinline__ void slice_accum_cta(const T* __restrict__ vals,
+                                                const int32_t* __restrict__ col, int64_t g0,
+                                                int64_t g1, const T* __restrict__ x, T (*red)[32][3],
+                                                T& a0, T& a1, T& a2) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    a0 = 0;
+    a1 = 0;
+    a2 = 0;
+    for (int64_t g = g0 + w; g < g1; g += kSweepWarps) step_accum<T>(vals, col, g, x, lane, a0, a1, a2);
+    if (w > 0) {
+        red[w - 1][lane][0] = a0;
+        red[w - 1][lane][1] = a1;
+        red[w - 1][lane][2] = a2;
+    }
+    __syncthreads();
+    if (w == 0) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) load4(V + k * kStepSlots, v[k]);
-        const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            T x0, x1, x2;
-            node3(x, cc[j], x0, x1, x2);
-            a0 += v[0][j] * x0 + v[1][j] * x1 + v[2][j] * x2;
-            a1 += v[3][j] * x0 + v[4][j] * x1 + v[5][j] * x2;
-            a2 += v[6][j] * x0 + v[7][j] * x1 + v[8][j] * x2;
+        for (int k = 0; k < kSweepWarps - 1; ++k) {
+            a0 += red[k][lane][0];
+            a1 += red[k][lane][1];
+            a2 += red[k][lane][2];
         }
     }
+    __syncthreads();
 }
 
 template <typename T, int LPR>
@@ -145,14 +202,16 @@ __global__ void __launch_bounds__(kThr) k_axpy(int32_t nb, T* __restrict__ x, T*
     double loc = 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb;
          i += (int64_t)gridDim.x * blockDim.x) {
+        F4 xv = ld4(x, i), rv = ld4(r, i);
+        const F4 pv = ld4(p, i), av = ld4(ap, i);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const int64_t k = 4 * i + c;
-            x[k] = (T)((double)x[k] + alpha * (double)p[k]);
-            const T rn = (T)((double)r[k] - alpha * (double)ap[k]);
-            r[k] = rn;
-            loc += (double)rn * (double)rn;
+            xv.v[c] = (double)(T)(xv.v[c] + alpha * pv.v[c]);
+            rv.v[c] = (double)(T)(rv.v[c] - alpha * av.v[c]);
+            loc += rv.v[c] * rv.v[c];
         }
+        st4(x, i, xv);
+        st4(r, i, rv);
     }
     if (publish_partial(loc, partials, &s->ticket[1], sh)) {
         const double rr = gather_sum(partials, gridDim.x, sh);
@@ -177,10 +236,14 @@ __global__ void __launch_bounds__(kThr) k_axpy(int32_t nb, T* __restrict__ x, T*
 // reliable update, part 1: x64 += x32, x32 = 0
 __global__ void k_upd_x(int32_t nb, double* __restrict__ x64, float* __restrict__ x32, PcgScalars* s) {
     if (s->done || !s->update) return;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 4 * (int64_t)nb;
-         k += (int64_t)gridDim.x * blockDim.x) {
-        x64[k] += (double)x32[k];
-        x32[k] = 0.f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        F4 a = ld4(x64, i);
+        const F4 d = ld4(x32, i);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) a.v[c] += d.v[c];
+        st4(x64, i, a);
+        st4(x32, i, F4{{0.0, 0.0, 0.0, 0.0}});
     }
 }
 
@@ -230,36 +293,41 @@ __global__ void __launch_bounds__(kThr) k_upd_r(SellDev A, const double* __restr
 __global__ void k_upd_cast(int32_t nb, const double* __restrict__ r64, float* __restrict__ r32,
                            PcgScalars* s) {
     if (s->done || !s->update) return;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 4 * (int64_t)nb;
-         k += (int64_t)gridDim.x * blockDim.x)
-        r32[k] = (float)r64[k];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb;
+         i += (int64_t)gridDim.x * blockDim.x)
+        st4(r32, i, ld4(r64, i));
 }
 
 // One level of the forward sweep y_I = L_II^-1 (r_I - sum_{J<I} L_IJ y_J) (Csr::precondition,
-// iterative.rs:175-179, block form; D_I = L_II^-1 stored as 9 planes of nb entries).
+// iterative.rs:175-179, block form; D_I = L_II^-1 stored as 9 planes of nb entries). One block of
+// kSweepWarps warps per slice: the warps split the slice's steps, so a level with few slices still
+// keeps every SM busy.
 template <typename T, int LPR>
-__global__ void __launch_bounds__(kThr) k_fwd(SellDev Lm, int32_t s0, int32_t s1,
-                                               const T* __restrict__ vals, const T* __restrict__ D,
-                                               int32_t nb, const T* __restrict__ r, T* y,
-                                               const PcgScalars* s) {
+__global__ void __launch_bounds__(kSweepWarps * 32) k_fwd(SellDev Lm, int32_t s0, int32_t s1,
+                                                          const T* __restrict__ vals,
+                                                          const T* __restrict__ D, int32_t nb,
+                                                          const T* __restrict__ r, T* y,
+                                                          const PcgScalars* s) {
+    __shared__ T red[kSweepWarps - 1][32][3];
     if (s->done) return;
     const int lane = threadIdx.x & 31, rr = lane / LPR, q = lane % LPR;
     constexpr int S = 32 / LPR;
-    for (int32_t sl = s0 + (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); sl < s1;
-         sl += (int32_t)((gridDim.x * blockDim.x) >> 5)) {
-        T a0 = 0, a1 = 0, a2 = 0;
-        slice_accum<T>(vals, Lm.col, Lm.off[sl], Lm.off[sl + 1], y, lane, a0, a1, a2);
-        row_reduce<T, LPR>(a0, a1, a2);
-        const int32_t row = Lm.rowid[(int64_t)sl * S + rr];
-        if (q == 0 && row >= 0) {
-            T r0, r1, r2;
-            node3(r, row, r0, r1, r2);
-            const T u0 = r0 - a0, u1 = r1 - a1, u2 = r2 - a2;
-            const T* d = D + row;
-            const T y0 = d[0] * u0;
-            const T y1 = d[3 * (int64_t)nb] * u0 + d[4 * (int64_t)nb] * u1;
-            const T y2 = d[6 * (int64_t)nb] * u0 + d[7 * (int64_t)nb] * u1 + d[8 * (int64_t)nb] * u2;
-            store_node(y, row, y0, y1, y2);
+    for (int32_t sl = s0 + (int32_t)blockIdx.x; sl < s1; sl += (int32_t)gridDim.x) {
+        T a0, a1, a2;
+        slice_accum_cta<T>(vals, Lm.col, Lm.off[sl], Lm.off[sl + 1], y, red, a0, a1, a2);
+        if (threadIdx.x < 32) {
+            row_reduce<T, LPR>(a0, a1, a2);
+            const int32_t row = Lm.rowid[(int64_t)sl * S + rr];
+            if (q == 0 && row >= 0) {
+                T r0, r1, r2;
+                node3(r, row, r0, r1, r2);
+                const T u0 = r0 - a0, u1 = r1 - a1, u2 = r2 - a2;
+                const T* d = D + row;
+                const T y0 = d[0] * u0;
+                const T y1 = d[3 * (int64_t)nb] * u0 + d[4 * (int64_t)nb] * u1;
+                const T y2 = d[6 * (int64_t)nb] * u0 + d[7 * (int64_t)nb] * u1 + d[8 * (int64_t)nb] * u2;
+                store_node(y, row, y0, y1, y2);
+            }
         }
     }
 }
@@ -267,36 +335,40 @@ __global__ void __launch_bounds__(kThr) k_fwd(SellDev Lm, int32_t s0, int32_t s1
 // One level of the backward sweep z_I = L_II^-T (y_I - sum_{J>I} L_JI^T z_J), in place over y
 // (Csr::precondition, iterative.rs:180-186, as a gather on the stored upper blocks L_JI^T), with
 // r . z partials; the last launch (level 0) sets beta = rz_new / rz, rz = rz_new
-// (iterative.rs:237-239).
+// (iterative.rs:237-239). One block per slice, as in the forward sweep.
 template <typename T, int LPR>
-__global__ void __launch_bounds__(kThr) k_bwd(SellDev Um, int32_t s0, int32_t s1, int level,
-                                               int nlevels, const T* __restrict__ vals,
-                                               const T* __restrict__ D, int32_t nb,
-                                               const T* __restrict__ r, T* z, PcgScalars* s,
-                                               double* partials, double* lvl_total) {
-    __shared__ double sh[kWarp];
+__global__ void __launch_bounds__(kSweepWarps * 32) k_bwd(SellDev Um, int32_t s0, int32_t s1,
+                                                          int level, int nlevels,
+                                                          const T* __restrict__ vals,
+                                                          const T* __restrict__ D, int32_t nb,
+                                                          const T* __restrict__ r, T* z,
+                                                          PcgScalars* s, double* partials,
+                                                          double* lvl_total) {
+    __shared__ T red[kSweepWarps - 1][32][3];
+    __shared__ double sh[kSweepWarps];
     if (s->done) return;
     const int lane = threadIdx.x & 31, rr = lane / LPR, q = lane % LPR;
     constexpr int S = 32 / LPR;
     double loc = 0.0;
-    for (int32_t sl = s0 + (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); sl < s1;
-         sl += (int32_t)((gridDim.x * blockDim.x) >> 5)) {
-        T a0 = 0, a1 = 0, a2 = 0;
-        slice_accum<T>(vals, Um.col, Um.off[sl], Um.off[sl + 1], z, lane, a0, a1, a2);
-        row_reduce<T, LPR>(a0, a1, a2);
-        const int32_t row = Um.rowid[(int64_t)sl * S + rr];
-        if (q == 0 && row >= 0) {
-            T y0, y1, y2;
-            node3_rw(z, row, y0, y1, y2);
-            const T u0 = y0 - a0, u1 = y1 - a1, u2 = y2 - a2;
-            const T* d = D + row;
-            const T z0 = d[0] * u0 + d[3 * (int64_t)nb] * u1 + d[6 * (int64_t)nb] * u2;
-            const T z1 = d[4 * (int64_t)nb] * u1 + d[7 * (int64_t)nb] * u2;
-            const T z2 = d[8 * (int64_t)nb] * u2;
-            store_node(z, row, z0, z1, z2);
-            T r0, r1, r2;
-            node3(r, row, r0, r1, r2);
-            loc += (double)r0 * (double)z0 + (double)r1 * (double)z1 + (double)r2 * (double)z2;
+    for (int32_t sl = s0 + (int32_t)blockIdx.x; sl < s1; sl += (int32_t)gridDim.x) {
+        T a0, a1, a2;
+        slice_accum_cta<T>(vals, Um.col, Um.off[sl], Um.off[sl + 1], z, red, a0, a1, a2);
+        if (threadIdx.x < 32) {
+            row_reduce<T, LPR>(a0, a1, a2);
+            const int32_t row = Um.rowid[(int64_t)sl * S + rr];
+            if (q == 0 && row >= 0) {
+                T y0, y1, y2;
+                node3_rw(z, row, y0, y1, y2);
+                const T u0 = y0 - a0, u1 = y1 - a1, u2 = y2 - a2;
+                const T* d = D + row;
+                const T z0 = d[0] * u0 + d[3 * (int64_t)nb] * u1 + d[6 * (int64_t)nb] * u2;
+                const T z1 = d[4 * (int64_t)nb] * u1 + d[7 * (int64_t)nb] * u2;
+                const T z2 = d[8 * (int64_t)nb] * u2;
+                store_node(z, row, z0, z1, z2);
+                T r0, r1, r2;
+                node3(r, row, r0, r1, r2);
+                loc += (double)r0 * (double)z0 + (double)r1 * (double)z1 + (double)r2 * (double)z2;
+            }
         }
     }
     if (publish_partial(loc, partials, &s->ticket[2], sh)) {
@@ -320,9 +392,14 @@ template <typename T>
 __global__ void k_pupdate(int32_t nb, const T* __restrict__ z, T* __restrict__ p, PcgScalars* s) {
     if (s->done) return;
     const double beta = s->beta;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 4 * (int64_t)nb;
-         k += (int64_t)gridDim.x * blockDim.x)
-        p[k] = (T)((double)z[k] + beta * (double)p[k]);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const F4 zv = ld4(z, i);
+        F4 pv = ld4(p, i);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) pv.v[c] = zv.v[c] + beta * pv.v[c];
+        st4(p, i, pv);
+    }
 }
 
 __global__ void k_pcg_init(PcgScalars* s, double tol, int32_t max_iter, double delta) {
@@ -440,12 +517,12 @@ template <typename T>
 void launch_axpy(int32_t nb, T* x, T* r, const T* p, const T* ap, PcgScalars* s, double* partials,
                  bool mixed, cudaStream_t st) {
     counted();
-    k_axpy<T><<<grid_for(nb, kThr), kThr, 0, st>>>(nb, x, r, p, ap, s, partials, mixed ? 1 : 0);
+    k_axpy<T><<<grid_for(nb, kThr, 148 * 16), kThr, 0, st>>>(nb, x, r, p, ap, s, partials, mixed ? 1 : 0);
 }
 
 void launch_upd_x(int32_t nb, double* x64, float* x32, PcgScalars* s, cudaStream_t st) {
     counted();
-    k_upd_x<<<grid_for(4 * (int64_t)nb, kThr), kThr, 0, st>>>(nb, x64, x32, s);
+    k_upd_x<<<grid_for(nb, kThr, 148 * 16), kThr, 0, st>>>(nb, x64, x32, s);
 }
 
 void launch_upd_r(const SellDev& A, const double* vals, const double* b, const double* x64,
@@ -463,15 +540,15 @@ void launch_upd_r(const SellDev& A, const double* vals, const double* b, const d
 
 void launch_upd_cast(int32_t nb, const double* r64, float* r32, PcgScalars* s, cudaStream_t st) {
     counted();
-    k_upd_cast<<<grid_for(4 * (int64_t)nb, kThr), kThr, 0, st>>>(nb, r64, r32, s);
+    k_upd_cast<<<grid_for(nb, kThr, 148 * 16), kThr, 0, st>>>(nb, r64, r32, s);
 }
 
 template <typename T>
 void launch_fwd(const SellDev& L, int32_t s0, int32_t s1, const T* vals, const T* D, int32_t nb,
                 const T* r, T* y, PcgScalars* s, cudaStream_t st) {
     counted();
-    const int grid = grid_for(s1 - s0, kWarp);
-    MAILLE_LPR_SWITCH(L.lpr, k_fwd, grid, kThr, 0, st>>>(L, s0, s1, vals, D, nb, r, y, s));
+    const int grid = grid_for(s1 - s0, 1, 148 * 16);
+    MAILLE_LPR_SWITCH(L.lpr, k_fwd, grid, kSweepWarps * 32, 0, st>>>(L, s0, s1, vals, D, nb, r, y, s));
 }
 
 template <typename T>
@@ -479,14 +556,14 @@ void launch_bwd(const SellDev& U, int32_t s0, int32_t s1, int level, int nlevels
                 const T* D, int32_t nb, const T* r, T* z, PcgScalars* s, double* partials,
                 double* lvl_total, cudaStream_t st) {
     counted();
-    const int grid = grid_for(s1 - s0, kWarp);
-    MAILLE_LPR_SWITCH(U.lpr, k_bwd, grid, kThr, 0, st>>>(U, s0, s1, level, nlevels, vals, D, nb, r, z, s, partials, lvl_total));
+    const int grid = grid_for(s1 - s0, 1, 148 * 16);
+    MAILLE_LPR_SWITCH(U.lpr, k_bwd, grid, kSweepWarps * 32, 0, st>>>(U, s0, s1, level, nlevels, vals, D, nb, r, z, s, partials, lvl_total));
 }
 
 template <typename T>
 void launch_pupdate(int32_t nb, const T* z, T* p, PcgScalars* s, cudaStream_t st) {
     counted();
-    k_pupdate<T><<<grid_for(4 * (int64_t)nb, kThr, 148 * 16), kThr, 0, st>>>(nb, z, p, s);
+    k_pupdate<T><<<grid_for(nb, kThr, 148 * 16), kThr, 0, st>>>(nb, z, p, s);
 }
 
 void launch_pcg_init(PcgScalars* s, double tol, int32_t max_iter, double delta, cudaStream_t st) {

@@ -8,7 +8,8 @@
 // lanes; the lanes of a row are summed with shuffles. Rows inside a level are sorted by length
 // (descending) per layout, which keeps the padding of a slice small; rowid maps slice rows to
 // matrix rows. Vectors are padded to 4 entries per node, so the x of one block is one 16-byte
-// gather (FP32) or a 16 + 8-byte gather (FP64).
+// gather (FP32) or a 16 + 8-byte gather (FP64). Vectors hold nb + 1 nodes: node nb is a dummy
+// that stays 0 and that padding slots point at.
 #pragma once
 
 #include <cstdint>
@@ -34,6 +35,7 @@ struct PcgScalars {
     int32_t iter, max_iter, done, status;  // status: 0 ok, 1 singular (also NaN), 2 cap reached
     int32_t update, updates;
     unsigned int ticket[4];
+    unsigned int epoch;  // sweep counter of the row-ready flags; never reset (monotonic)
 };
 
 template <typename T>
@@ -70,5 +72,31 @@ void launch_sell_fill(int64_t steps, const int32_t* src, const double* csr, T* v
 template <typename T>
 void launch_diag_fill(int32_t nb, const int64_t* diag, const double* F, T* D, cudaStream_t st);
 void launch_cast(int64_t n, const double* a, float* b, cudaStream_t st);
+
+// The persistent cooperative PCG kernel (persist.cu): arguments, co-resident grid size and launch.
+template <typename T>
+struct PcgArgs {
+    int32_t nb, levels, chunk;
+    SellDev K, L, U;
+    const int32_t* lvl_l;  // [levels + 1] slice ranges of the L layout per level
+    const int32_t* lvl_u;
+    const T *Kv, *Lv, *Uv, *D;
+    T *x, *r, *z, *p, *ap;
+    const double* K64;  // mixed form: FP64 matrix, right-hand side, solution, true residual
+    const double* b64;
+    double *x64, *r64;
+    PcgScalars* s;
+    // dataflow sweeps: slice claim counters, row-ready flags ([nb + 1], monotonic epochs) and the
+    // order in which the backward sweep claims the U slices (levels descending)
+    int32_t* claim;
+    unsigned int* flags;
+    const int32_t* bwd_seq;
+    double* partials;       // [4 * grid]
+    unsigned long long* timing;  // optional [8] ns per phase (block 0): spmv, axpy, update, fwd, bwd, p
+};
+template <typename T, bool MIXED>
+int pcg_persistent_grid(int lprk, int lprlu);
+template <typename T, bool MIXED>
+cudaError_t launch_pcg_persistent(const PcgArgs<T>& a, int grid, bool init, cudaStream_t st);
 
 }  // namespace maille
