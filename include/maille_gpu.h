@@ -177,6 +177,28 @@ int32_t maille_gpu_face_pressure_loads(int64_t n_nodes, const double* coords, in
                                        const int64_t* p_elem, const int32_t* p_face,
                                        const double* p_value, double* f);
 
+/* Largest n_block_rows that maille_gpu_bsr3_spmv_dot_noalloc accepts (2^26 block rows, i.e.
+ * about 2e8 DOFs, inside the 32-bit column indices of the matrix). */
+#define MAILLE_NOALLOC_MAX_BLOCK_ROWS (INT64_C(1) << 26)
+
+/* No counterpart in the reference. For callers that cannot allocate device memory where they
+ * need the product (code running during CUDA stream capture, plugins whose host framework owns
+ * every device allocation, real-time loops): y = A x and *xy = x . y for a 3x3-block CSR matrix
+ * A held by the caller on `device` -- row_ptr [n_block_rows + 1] (int64), col [blocks] (int32
+ * block columns), vals [9 * blocks] (row-major blocks), x and y [3 * n_block_rows], xy [1], all
+ * device pointers the caller owns -- enqueued on `stream` (cudaStream_t, NULL = the legacy
+ * default stream) without waiting. It calls no cudaMalloc, cudaFree or allocating routine: the
+ * reduction's partial sums and ticket live in a fixed 8.5 KB device array inside the library,
+ * shared by all calls, so calls that overlap on the GPU race and must be ordered by the caller.
+ * The first call on a device looks up that array's address (cudaGetSymbolAddress) with the
+ * device current: make it before any stream capture. Sizes beyond
+ * MAILLE_NOALLOC_MAX_BLOCK_ROWS are rejected with MAILLE_INVALID_INPUT. The current device of
+ * the calling thread is restored on return. */
+int32_t maille_gpu_bsr3_spmv_dot_noalloc(int32_t device, int64_t n_block_rows,
+                                         const int64_t* row_ptr, const int32_t* col,
+                                         const double* vals, const double* x, double* y,
+                                         double* xy, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, "libmaille_gpu.so")
 MAILLE_OK, MAILLE_SINGULAR, MAILLE_NOT_CONVERGED, MAILLE_INVALID_INPUT, MAILLE_CUDA_ERROR, \
     MAILLE_CANCELLED = range(6)
 MAILLE_FP64, MAILLE_MIXED = 0, 1
+MAILLE_NOALLOC_MAX_BLOCK_ROWS = 1 << 26
 MAILLE_ORDER_AUTO, MAILLE_ORDER_MULTICOLOR, MAILLE_ORDER_RCM = 0, 1, 2
 
 _d = ctypes.POINTER(ctypes.c_double)
@@ -65,6 +66,10 @@ SIGNATURES = {
     "maille_gpu_multiply": ([ctypes.c_void_p, _d, _d], ctypes.c_int32),
     "maille_gpu_spmv_device": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
     "maille_gpu_kernel_launches": ([], ctypes.c_int64),
+    "maille_gpu_bsr3_spmv_dot_noalloc": ([ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                                         ctypes.c_int32),
     "maille_gpu_face_pressure_loads": ([ctypes.c_int64, _d, ctypes.c_int32, ctypes.c_int64, _i64,
                                         ctypes.c_int64, _i64, _i32, _d, _d], ctypes.c_int32),
 }

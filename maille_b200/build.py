@@ -12,7 +12,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = [os.path.join(HERE, "csrc", f) for f in ("setup.cpp", "kernels.cu", "sparse.cu", "persist.cu", "solver.cu")]
+SRC = [os.path.join(HERE, "csrc", f) for f in ("setup.cpp", "kernels.cu", "sparse.cu", "persist.cu", "solver.cu", "noalloc.cu")]
 HDR = [os.path.join(HERE, "csrc", f) for f in ("common.hpp", "kernels.cuh", "sparse.cuh", "reduce.cuh")] + [
     os.path.join(HERE, "..", "include", "maille_gpu.h")]
 LIB = os.path.join(HERE, "libmaille_gpu.so")

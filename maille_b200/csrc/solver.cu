@@ -819,6 +819,10 @@ int32_t backward_impl(MailleGpuHandle* h, const double* dJdu, double* dJdE, doub
 
 }  // namespace
 
+namespace maille {
+void set_last_error(const std::string& message) { g_last_error = message; }
+}  // namespace maille
+
 // ---- C ABI -------------------------------------------------------------------------------------
 
 extern "C" {
