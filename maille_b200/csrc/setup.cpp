@@ -11,7 +11,10 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <numeric>
+#include <thread>
 
 #include "common.hpp"
 
@@ -22,6 +25,23 @@ double now_ms() {
     return std::chrono::duration<double, std::milli>(
                std::chrono::steady_clock::now().time_since_epoch())
         .count();
+}
+
+// Runs fn(begin, end) over [0, n) split into contiguous chunks on the host's cores.
+template <typename F>
+void parallel_for(int64_t n, F&& fn) {
+    const int64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const int64_t chunks = std::min<int64_t>(hw, std::max<int64_t>(1, n / 4096));
+    if (chunks <= 1) {
+        fn(int64_t(0), n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int64_t c = 0; c < chunks; ++c) {
+        const int64_t b = n * c / chunks, e = n * (c + 1) / chunks;
+        pool.emplace_back([&fn, b, e] { fn(b, e); });
+    }
+    for (auto& t : pool) t.join();
 }
 
 struct NodeGraph {
@@ -144,6 +164,14 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
                                              " refers to unknown node " + std::to_string(conn[k])};
             return false;
         }
+    const bool stage_timing = std::getenv("MAILLE_SETUP_TIMING") != nullptr;
+    double t_stage = now_ms();
+    auto stage = [&](const char* name) {
+        if (!stage_timing) return;
+        const double t = now_ms();
+        std::fprintf(stderr, "maille setup %-12s %8.1f ms\n", name, t - t_stage);
+        t_stage = t;
+    };
     s = Symbolic{};
     s.n_nodes = n_nodes;
     s.n_elems = n_elems;
@@ -160,6 +188,7 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
         for (int64_t k = 0; k < n_elems * npe; ++k) s.inc[cur[conn[k]]++] = (int32_t)k;
     }
 
+    stage("incidence");
     // kept nodes (at least one free DOF) in original order; graph on them
     std::vector<int32_t> kept_of(N, -1), kept;
     for (int32_t v = 0; v < N; ++v) {
@@ -197,6 +226,7 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
         }
     }
 
+    stage("graph");
     // ordering over kept nodes: order[new] = kept index
     std::vector<int32_t> order = rcm(g);
     if (ordering != MAILLE_ORDER_RCM) {
@@ -207,6 +237,7 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
             return colour[a] != colour[b] ? colour[a] < colour[b] : rank[a] < rank[b];
         });
     }
+    stage("ordering");
     // levels of the lower-triangular dependency graph in that order, then group rows by level
     // (a topological renumbering leaves the IC(0) factor unchanged)
     {
@@ -242,6 +273,7 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
         s.fixmask[r] = m;
     }
 
+    stage("levels");
     // full block pattern in new numbering (neighbours + the diagonal), columns ascending
     s.row_ptr.assign(nk + 1, 0);
     for (int32_t r = 0; r < nk; ++r) {
@@ -255,70 +287,79 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
     }
     s.col.resize(s.blocks);
     s.diag.resize(nk);
-    for (int32_t r = 0; r < nk; ++r) {
-        const int32_t k = kept_of[s.perm[r]];
-        int64_t p = s.row_ptr[r];
-        s.col[p++] = r;
-        for (int64_t q = g.off[k]; q < g.off[k + 1]; ++q) s.col[p++] = s.inv[kept[g.adj[q]]];
-        std::sort(s.col.begin() + s.row_ptr[r], s.col.begin() + s.row_ptr[r + 1]);
-        s.diag[r] = std::lower_bound(s.col.begin() + s.row_ptr[r],
-                                     s.col.begin() + s.row_ptr[r + 1], r) -
-                    s.col.begin();
-    }
+    parallel_for(nk, [&](int64_t r0, int64_t r1) {
+        for (int64_t r = r0; r < r1; ++r) {
+            const int32_t k = kept_of[s.perm[r]];
+            int64_t p = s.row_ptr[r];
+            s.col[p++] = (int32_t)r;
+            for (int64_t q = g.off[k]; q < g.off[k + 1]; ++q) s.col[p++] = s.inv[kept[g.adj[q]]];
+            std::sort(s.col.begin() + s.row_ptr[r], s.col.begin() + s.row_ptr[r + 1]);
+            s.diag[r] = std::lower_bound(s.col.begin() + s.row_ptr[r],
+                                         s.col.begin() + s.row_ptr[r + 1], (int32_t)r) -
+                        s.col.begin();
+        }
+    });
     g = NodeGraph{};
     auto find = [&](int32_t i, int32_t j) -> int64_t {
         auto b = s.col.begin() + s.row_ptr[i], e = s.col.begin() + s.row_ptr[i + 1];
         auto it = std::lower_bound(b, e, j);
         return (it != e && *it == j) ? (int64_t)(it - s.col.begin()) : -1;
     };
+    stage("pattern");
     s.tpos.resize(s.blocks);
-    for (int32_t r = 0; r < nk; ++r)
-        for (int64_t p = s.row_ptr[r]; p < s.row_ptr[r + 1]; ++p) s.tpos[p] = find(s.col[p], r);
+    parallel_for(nk, [&](int64_t r0, int64_t r1) {
+        for (int64_t r = r0; r < r1; ++r)
+            for (int64_t p = s.row_ptr[r]; p < s.row_ptr[r + 1]; ++p)
+                s.tpos[p] = find(s.col[p], (int32_t)r);
+    });
 
-    // lower slots and the scatter map (counting sort by slot, element order kept inside a slot)
-    std::vector<int64_t> lidx(s.blocks, -1);
+    stage("transpose");
+    // lower slots (row by row, columns ascending) and the scatter map: for lower slot (I, J) the
+    // element node pairs that couple I and J, in element order. Built row by row from the
+    // node's incident elements (ascending), with a per-thread column -> slot map.
+    const int64_t nl0 = 0;
+    (void)nl0;
+    std::vector<int64_t> lfirst(nk + 1, 0);
+    for (int32_t r = 0; r < nk; ++r) lfirst[r + 1] = lfirst[r] + (s.diag[r] - s.row_ptr[r] + 1);
+    const int64_t nl = lfirst[nk];
+    s.lslot.resize(nl);
     for (int32_t r = 0; r < nk; ++r)
-        for (int64_t p = s.row_ptr[r]; p <= s.diag[r]; ++p) {
-            lidx[p] = (int64_t)s.lslot.size();
-            s.lslot.push_back(p);
-        }
-    const int64_t nl = (int64_t)s.lslot.size();
+        for (int64_t p = s.row_ptr[r]; p <= s.diag[r]; ++p) s.lslot[lfirst[r] + (p - s.row_ptr[r])] = p;
     const int np = node_pairs(npe);
-    std::vector<int64_t> target((size_t)n_elems * np, -1);
+    auto pair_index = [npe](int a, int b) { return a * npe - a * (a - 1) / 2 + (b - a); };
+    // visit(r, fn): fn(local slot, contribution) for every contribution of row r, element order
+    auto visit_row = [&](int32_t r, std::vector<int32_t>& slotmap, auto&& fn) {
+        for (int64_t p = s.row_ptr[r]; p <= s.diag[r]; ++p) slotmap[s.col[p]] = (int32_t)(p - s.row_ptr[r]);
+        const int32_t v = s.perm[r];
+        for (int64_t q = s.inc_ptr[v]; q < s.inc_ptr[v + 1]; ++q) {
+            const int64_t e = s.inc[q] / npe;
+            const int a = (int)(s.inc[q] - e * npe);
+            for (int b = 0; b < npe; ++b) {
+                const int32_t J = s.inv[conn[e * npe + b]];
+                if (J < 0 || J > r) continue;
+                const uint32_t k = (uint32_t)(e * np + (a <= b ? pair_index(a, b) : pair_index(b, a)));
+                fn(slotmap[J], k | (a <= b ? 0u : 0x80000000u));
+            }
+        }
+    };
     s.lptr.assign(nl + 1, 0);
-    {
-        int pa[55], pb[55], q = 0;
-        for (int a = 0; a < npe; ++a)
-            for (int b = a; b < npe; ++b) {
-                pa[q] = a;
-                pb[q] = b;
-                ++q;
-            }
-        for (int64_t e = 0; e < n_elems; ++e)
-            for (int p = 0; p < np; ++p) {
-                const int32_t I = s.inv[conn[e * npe + pa[p]]];
-                const int32_t J = s.inv[conn[e * npe + pb[p]]];
-                if (I < 0 || J < 0) continue;
-                const bool tr = I < J;
-                const int64_t pos = tr ? find(J, I) : find(I, J);
-                const int64_t ls = lidx[pos];
-                target[(size_t)e * np + p] = tr ? ~ls : ls;
-                s.lptr[ls + 1]++;
-            }
-    }
+    parallel_for(nk, [&](int64_t r0, int64_t r1) {
+        std::vector<int32_t> slotmap(nk, -1);
+        for (int64_t r = r0; r < r1; ++r)
+            visit_row((int32_t)r, slotmap, [&](int32_t ls, uint32_t) { s.lptr[lfirst[r] + ls + 1]++; });
+    });
     for (int64_t l = 0; l < nl; ++l) s.lptr[l + 1] += s.lptr[l];
     s.contrib.resize(s.lptr[nl]);
-    {
-        std::vector<int64_t> cur(s.lptr.begin(), s.lptr.end() - 1);
-        for (int64_t k = 0; k < n_elems * np; ++k) {
-            const int64_t t = target[k];
-            if (t == -1) continue;
-            const bool tr = t < 0;
-            const int64_t ls = tr ? ~t : t;
-            s.contrib[cur[ls]++] = (uint32_t)k | (tr ? 0x80000000u : 0u);
+    parallel_for(nk, [&](int64_t r0, int64_t r1) {
+        std::vector<int32_t> slotmap(nk, -1);
+        std::vector<int64_t> cur;
+        for (int64_t r = r0; r < r1; ++r) {
+            cur.assign(s.lptr.begin() + lfirst[r], s.lptr.begin() + lfirst[r + 1]);
+            visit_row((int32_t)r, slotmap, [&](int32_t ls, uint32_t c) { s.contrib[cur[ls]++] = c; });
         }
-    }
+    });
 
+    stage("scatter map");
     // elements touching a fixed DOF, and the nodes with a fixed DOF they contain
     if (fixed) {
         std::vector<uint8_t> bn(N, 0);
@@ -336,6 +377,7 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
         for (int32_t v = 0; v < N; ++v)
             if (bn[v]) s.bnodes.push_back(v);
     }
+    stage("boundary");
     s.ms = now_ms() - t0;
     return true;
 }
@@ -347,10 +389,11 @@ void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out) {
     if (lpr <= 0) {
         const double total = kind == SELL_FULL ? (double)s.blocks : (double)(s.blocks - s.nb) / 2.0;
         const double mean = total / std::max<int32_t>(1, s.nb);
-        // K: ~4 steps of 4 slots per lane; L and U: ~1 step, which puts more and shorter
-        // slices in flight for the sweeps
+        // K: one lane per row unless rows are very long (least padding; the SpMV has slices to
+        // spare); L and U: about one step per row, which puts more and shorter slices in flight
+        // for the dataflow sweeps (measured on Tet10 40^3: K 1 / L,U 4 lanes per row is best)
         lpr = 1;
-        const double per_lane = kind == SELL_FULL ? 16.0 : 4.0;
+        const double per_lane = kind == SELL_FULL ? 32.0 : 4.0;
         while (lpr < 4 && mean / lpr > per_lane) lpr *= 2;
     }
     out.lpr = lpr;

@@ -19,6 +19,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -538,9 +539,15 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
                  h->sym, err))
         return fail(err);
     if (h->sym.levels >= kMaxLevels) return fail({MAILLE_INVALID_INPUT, "too many IC(0) levels"});
-    build_sell(h->sym, SELL_FULL, env_int("MAILLE_LPR_K", 0), h->sk.h);
-    build_sell(h->sym, SELL_LOWER, env_int("MAILLE_LPR_LU", 0), h->sl.h);
-    build_sell(h->sym, SELL_UPPER, env_int("MAILLE_LPR_LU", 0), h->su.h);
+    {
+        // the three sliced layouts are independent: build them side by side
+        const int lk = env_int("MAILLE_LPR_K", 0), llu = env_int("MAILLE_LPR_LU", 0);
+        std::thread tk([&] { build_sell(h->sym, SELL_FULL, lk, h->sk.h); });
+        std::thread tl([&] { build_sell(h->sym, SELL_LOWER, llu, h->sl.h); });
+        build_sell(h->sym, SELL_UPPER, llu, h->su.h);
+        tk.join();
+        tl.join();
+    }
     const double t_setup1 = now_ms();
     try {
         int ndev = 0;
