@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost section")
+    ap.add_argument("--adjoint-cells", type=int, default=48)
     ap.add_argument("--only", choices=["mixed", "plain"], default=None,
                     help="profiling mode: time one form only (no reference solve, e2e or CPU); "
                          "prints a short line, not the benchmark line")
@@ -155,6 +157,49 @@ def time_handle(torch, h, steps, warmup, L):
     end.synchronize()
     launches = (L.maille_gpu_kernel_launches() - k0) / steps
     return start.elapsed_time(end) / steps, info, launches
+
+
+def adjoint_section(torch, mb, mg, L, cells, tol, steps, warmup, device):
+    """Adjoint compliance on the Tet4 SIMP cube (cells^3, E = 210000 rho^3): one forward step
+    (element integration, assembly, IC(0), PCG, reactions and stresses, device-resident) against
+    one backward() (adjoint PCG with the same factor + the element gradient kernel + the gradient
+    download), both with CUDA events on the library's stream; the gradient is checked against the
+    oracle's full-size values when the golden summary for this size exists."""
+    from maille_b200._lib import MAILLE_FP64, ptr, _d
+    p, rho = mg.simp_tet4(cells)
+    h = mb.SolverHandle(solve_model(mb, p, MAILLE_FP64, tol, device), device=device)
+    try:
+        ms_fwd, info, _ = time_handle(torch, h, steps, warmup, L)
+        fld = h.solve()
+        g = np.ascontiguousarray(h._f)
+        dJdE = np.zeros(p.n_elems)
+        stream = torch.cuda.ExternalStream(h.stream)
+        for _ in range(warmup):
+            assert L.maille_gpu_backward(h._h, ptr(g, _d), ptr(dJdE, _d), None) == 0
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(steps):
+            s = L.maille_gpu_backward(h._h, ptr(g, _d), ptr(dJdE, _d), None)
+            if s != 0:
+                raise RuntimeError("backward failed: " + L.maille_gpu_last_error().decode())
+        end.record(stream)
+        end.synchronize()
+        ms_bwd = start.elapsed_time(end) / steps
+    finally:
+        h.close()
+    grad = dJdE * 3 * 210000.0 * rho ** 2
+    out = {"workload": f"simp_tet4_{cells}^3_compliance", "free_dofs": p.free_dofs,
+           "elements": p.n_elems, "tol": tol, "forward_ms": ms_fwd, "backward_ms": ms_bwd,
+           "backward_over_forward": ms_bwd / ms_fwd, "target": 1.5,
+           "iterations": info["iterations"], "compliance": float(g @ fld.displacements)}
+    path = os.path.join(ROOT, "tests", "golden", f"simp{cells}_oracle_gradient.json")
+    if os.path.exists(path):
+        ref = json.load(open(path))
+        el = np.array(ref["elements"])
+        out["grad_rel_err_vs_oracle"] = float(np.linalg.norm(grad[el] - np.array(ref["grad"]))
+                                              / np.linalg.norm(ref["grad"]))
+    return out
 
 
 def spmv_roofline(torch, h, L, precision, blocks, nb, reps=50):
@@ -361,6 +406,11 @@ def run_ours(args):
                                                       "ms_factor", "ms_solve", "ms_post",
                                                       "ms_download")}}
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_section(torch, mb, mg, L, args.adjoint_cells, args.tol, args.steps,
+                                  args.warmup, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         need, path = oracle_iterations(args.tol)
@@ -396,6 +446,7 @@ def run_ours(args):
                  "ms_per_launch": ms32,
                  "fp64": {"achieved": gbs64, "frac": gbs64 / hbm, "bytes_per_launch": bytes64,
                           "ms_per_launch": ms64}},
+        "adjoint": adjoint,
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
     }
     print(json.dumps(line))

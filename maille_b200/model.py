@@ -346,6 +346,22 @@ class SolverHandle:
         _raise_for(s)
         return dJdE, lam
 
+    def refactor(self, young=None, poisson=None):
+        """New per-element materials on the same mesh and constraints: element integration,
+        assembly and IC(0) again, reusing the ordering and scatter map."""
+        ne = self.model.mesh.conn.shape[0]
+        ya = None if young is None else np.ascontiguousarray(young, np.float64).ravel()
+        pa = None if poisson is None else np.ascontiguousarray(poisson, np.float64).ravel()
+        for a in (ya, pa):
+            if a is not None and a.size != ne:
+                raise MailleError("InvalidInput", f"{a.size} material values for {ne} elements")
+        s = self._L.maille_gpu_refactor(self._h, ptr(ya, _lib._d), ptr(pa, _lib._d))
+        _raise_for(s)
+        if ya is not None:
+            self.model.mesh.young = ya.copy()
+        if pa is not None:
+            self.model.mesh.poisson = pa.copy()
+
     def cancel(self, flag: bool = True):
         self._L.maille_gpu_cancel(self._h, 1 if flag else 0)
 

@@ -5,6 +5,7 @@ bench.py's cpu_baseline / reference legs. The product package (maille_b200) neve
 """
 from __future__ import annotations
 
+import copy
 import ctypes
 import os
 import subprocess
@@ -60,6 +61,9 @@ def lib():
         L.oracle_model_solve.restype = ctypes.c_int
         L.oracle_energy.argtypes = [ctypes.c_int64, _d, ctypes.c_int, ctypes.c_int64, _i64, _d, _d, _d]
         L.oracle_energy.restype = ctypes.c_double
+        L.oracle_element_bilinear.argtypes = [ctypes.c_int64, _d, ctypes.c_int, ctypes.c_int64, _i64,
+                                               _d, _d, _d, _d, _d]
+        L.oracle_element_bilinear.restype = None
         L.oracle_nodal_stresses.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int64, _i64, _d, _d]
         _lib = L
     return _lib
@@ -195,6 +199,34 @@ def energy(prob, v):
     return lib().oracle_energy(coords.shape[0], _p(coords, _d), conn.shape[1], conn.shape[0],
                                _p(conn, _i64), _p(_c(prob.young, np.float64), _d),
                                _p(_c(prob.poisson, np.float64), _d), _p(vv, _d))
+
+
+def element_bilinear(prob, a, b):
+    """a_e^T K_e b_e for every element (K_e of the element's own E and nu)."""
+    coords = _c(prob.coords, np.float64)
+    conn = _c(prob.conn, np.int64)
+    out = np.zeros(conn.shape[0])
+    lib().oracle_element_bilinear(coords.shape[0], _p(coords, _d), conn.shape[1], conn.shape[0],
+                                  _p(conn, _i64), _p(_c(prob.young, np.float64), _d),
+                                  _p(_c(prob.poisson, np.float64), _d), _p(_c(a, np.float64), _d),
+                                  _p(_c(b, np.float64), _d), _p(out, _d))
+    return out
+
+
+def adjoint_gradient(prob, u, dJdu, tol: float = 1e-13, max_iter: int = 100000):
+    """dJ/dE_e of a linear static solve u for an objective with gradient dJdu: the adjoint system
+    K_ff lambda_f = (dJ/du)_f solved by the oracle's IC(0)-PCG (lambda = 0 on fixed DOFs, no
+    pressure, no imposed values), then -lambda_e^T K_e u_e / E_e. Returns (gradient, lambda, info)."""
+    adj = copy.copy(prob)
+    adj.loads = np.ascontiguousarray(dJdu, np.float64).reshape(prob.loads.shape)
+    adj.imposed = np.zeros_like(prob.imposed)
+    adj.p_elem = np.zeros(0, np.int64)
+    adj.p_face = np.zeros(0, np.int32)
+    adj.p_value = np.zeros(0)
+    res = model_solve(adj, solver=2, tol=tol, max_iter=max_iter)
+    lam = res["u"]
+    grad = -element_bilinear(prob, lam, u) / np.asarray(prob.young, np.float64)
+    return grad, lam, res
 
 
 def nodal_stresses(prob, gauss):

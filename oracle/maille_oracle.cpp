@@ -987,6 +987,34 @@ double oracle_energy(int64_t n_nodes, const double* coords, int npe, int64_t n_e
     return total;
 }
 
+// Per element a_e^T K_e b_e (K_e from solid_stiffness, element.rs:223-243). With a = lambda (the
+// adjoint solution) and b = u it gives the adjoint sensitivity dJ/dE_e = -lambda_e^T K_e u_e / E_e,
+// since K_e is linear in E_e; the reference has no gradients, so this is the oracle's restatement
+// of that formula on top of its own element matrices.
+void oracle_element_bilinear(int64_t n_nodes, const double* coords, int npe, int64_t n_elems,
+                             const int64_t* conn, const double* young, const double* poisson,
+                             const double* a, const double* b, double* out) {
+    SolidMesh mesh{(size_t)n_nodes, (size_t)n_elems, npe, coords, conn, young, poisson};
+    const int m = 3 * npe;
+    Vec ke((size_t)m * m);
+    for (size_t e = 0; e < mesh.n_elems; ++e) {
+        mesh.stiffness(e, ke.data());
+        double ae[30], be[30];
+        for (int l = 0; l < m; ++l) {
+            const size_t d = 3 * (size_t)conn[e * npe + l / 3] + l % 3;
+            ae[l] = a[d];
+            be[l] = b[d];
+        }
+        double total = 0.0;
+        for (int r = 0; r < m; ++r) {
+            double s = 0.0;
+            for (int c = 0; c < m; ++c) s += ke[(size_t)r * m + c] * be[c];
+            total += ae[r] * s;
+        }
+        out[e] = total;
+    }
+}
+
 // nodal_stresses / smooth, results.rs:137-230: Gauss values extrapolated to the element nodes
 // (TET4_EXTRAPOLATION 98, TET10_EXTRAPOLATION 118-132) and averaged. gauss: n_elems*ngp*9 as
 // written above; out: n_nodes*6 (sxx, syy, szz, txy, tyz, txz).
