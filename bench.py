@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost section")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched section")
+    ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--adjoint-cells", type=int, default=48)
     ap.add_argument("--only", choices=["mixed", "plain"], default=None,
                     help="profiling mode: time one form only (no reference solve, e2e or CPU); "
@@ -199,6 +201,105 @@ def adjoint_section(torch, mb, mg, L, cells, tol, steps, warmup, device):
         el = np.array(ref["elements"])
         out["grad_rel_err_vs_oracle"] = float(np.linalg.norm(grad[el] - np.array(ref["grad"]))
                                               / np.linalg.norm(ref["grad"]))
+    return out
+
+
+def batched_section(torch, mb, mg, L, count, tol, steps, warmup, device, rank=0, world=1):
+    """Batched Tet4 workload (`count` cubes of side 6..24, 8 traction load cases each; this rank's
+    LPT share under torchrun): one step = element integration + assembly + IC(0) of every
+    instance and the PCG of every instance and load case (device-resident inputs, CUDA events on
+    the batch stream), FP64 and mixed. Against it, the same work as per-instance launches: one
+    single-model handle per instance, refactor + 8 solves each (loads uploaded per solve, each
+    solve also computing its reactions and stresses, as the single-model API does)."""
+    import ctypes as C
+    from maille_b200 import batch as mbatch
+    from maille_b200._lib import MAILLE_FP64, MAILLE_MIXED, BatchResult
+    probs, loads = mg.batched_tet4(count=count)
+    mine = mbatch.partition_lpt([mbatch.instance_cost(p) for p in probs], world)[rank]
+    probs = [probs[k] for k in mine]
+    loads = [loads[k] for k in mine]
+    n_rhs = loads[0].shape[1]
+    free = sum(p.free_dofs for p in probs)
+    out = {"workload": f"batched_tet4_{count}x{n_rhs}rhs", "instances": len(probs), "load_cases": n_rhs,
+           "free_dofs": free, "tol": tol}
+
+    def time_batch(precision):
+        b = mb.BatchSolver(probs, loads, tol=tol, precision=precision, device=device)
+        try:
+            first = b.solve()  # runs the autotuner (or hits the cache)
+            stream = torch.cuda.ExternalStream(b.stream)
+            res = BatchResult()
+            for _ in range(warmup):
+                L.maille_gpu_batch_refactor(b._h, None, None)
+                L.maille_gpu_batch_solve(b._h, None, C.byref(res))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            k0 = L.maille_gpu_kernel_launches()
+            e0.record(stream)
+            for _ in range(steps):
+                if L.maille_gpu_batch_refactor(b._h, None, None) != 0:
+                    raise RuntimeError(L.maille_gpu_last_error().decode())
+                s = L.maille_gpu_batch_solve(b._h, None, C.byref(res))
+                if s != 0:
+                    raise RuntimeError(L.maille_gpu_last_error().decode())
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            launches = (L.maille_gpu_kernel_launches() - k0) / steps
+            return ms, first, res, launches
+        finally:
+            b.close()
+
+    for name, prec in (("fp64", MAILLE_FP64), ("mixed", MAILLE_MIXED)):
+        ms, first, res, launches = time_batch(prec)
+        out[name] = {"ms_per_step": ms, "value": free * n_rhs / (ms / 1e3),
+                     "unit": "DOF*load_cases/s", "max_iterations": res.max_iterations,
+                     "mean_iterations": float(first.iterations.mean()),
+                     "ms_solve": res.ms_solve, "autotuned_ms": first.info["ms_tune"],
+                     "config": {"rhs_per_lane": res.rhs_per_lane, "lanes_per_row": res.lanes_per_row,
+                                "threads": res.threads, "task_slices": res.task_slices},
+                     "kernel_launches_per_step": launches}
+        if name == "fp64":
+            u_fp64 = first.displacements
+        else:
+            err = max(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+                      for a, b in zip(first.displacements, u_fp64))
+            out[name]["max_rel_diff_vs_fp64"] = err
+
+    # per-instance launches of the single-model path: refactor + one solve per load case
+    handles = []
+    try:
+        for p in probs:
+            m = mb.Model.from_arrays(p.coords, p.conn, p.young, p.poisson, p.fixed, p.imposed, None)
+            m.with_solver(mb.SolverKind.ITERATIVE).with_tolerance(tol)
+            handles.append(mb.SolverHandle(m, device=device))
+        cols = [[np.ascontiguousarray(l[:, j]) for j in range(n_rhs)] for l in loads]
+        from maille_b200._lib import ElasticResult, ptr, _d
+
+        def one_pass():
+            for h, cs in zip(handles, cols):
+                if L.maille_gpu_refactor(h._h, None, None) != 0:
+                    raise RuntimeError(L.maille_gpu_last_error().decode())
+                for c in cs:
+                    r = ElasticResult()
+                    if L.maille_gpu_solve(h._h, ptr(c, _d), C.byref(r)) != 0:
+                        raise RuntimeError(L.maille_gpu_last_error().decode())
+        one_pass()
+        torch.cuda.synchronize()
+        k0 = L.maille_gpu_kernel_launches()
+        t0 = time.perf_counter()
+        one_pass()
+        torch.cuda.synchronize()
+        ms_pi = (time.perf_counter() - t0) * 1e3
+        out["per_instance"] = {"ms_per_step": ms_pi, "value": free * n_rhs / (ms_pi / 1e3),
+                               "unit": "DOF*load_cases/s",
+                               "kernel_launches_per_step": L.maille_gpu_kernel_launches() - k0,
+                               "timing": "host wall clock around synchronous per-instance calls"}
+    finally:
+        for h in handles:
+            h.close()
+    for name in ("fp64", "mixed"):
+        out[f"speedup_{name}_vs_per_instance"] = out["per_instance"]["ms_per_step"] / out[name]["ms_per_step"]
     return out
 
 
@@ -406,6 +507,11 @@ def run_ours(args):
                                                       "ms_factor", "ms_solve", "ms_post",
                                                       "ms_download")}}
 
+    batched = None
+    if not args.no_batched:
+        batched = batched_section(torch, mb, mg, L, args.batch_count, args.tol, args.steps,
+                                  args.warmup, local, rank, world)
+
     adjoint = None
     if not args.no_adjoint:
         adjoint = adjoint_section(torch, mb, mg, L, args.adjoint_cells, args.tol, args.steps,
@@ -446,6 +552,7 @@ def run_ours(args):
                  "ms_per_launch": ms32,
                  "fp64": {"achieved": gbs64, "frac": gbs64 / hbm, "bytes_per_launch": bytes64,
                           "ms_per_launch": ms64}},
+        "batched": batched,
         "adjoint": adjoint,
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
     }

@@ -177,6 +177,89 @@ int32_t maille_gpu_face_pressure_loads(int64_t n_nodes, const double* coords, in
                                        const int64_t* p_elem, const int32_t* p_face,
                                        const double* p_value, double* f);
 
+/* ---- Batched solves ------------------------------------------------------------------------
+ * No counterpart in the reference, whose Model::solve (model.rs:548-610) takes one mesh and one
+ * load vector: a host program with many independent models (or one model and several load cases)
+ * calls Model::solve once per model and load case. The batch entry points take many Tet4/Tet10
+ * models of uneven size, each with the same number of load cases, and solve them all in one
+ * persistent kernel over the packed block-diagonal matrix (per-instance offsets): block PCG over
+ * the right-hand sides of each instance (the matrix and factor are read once for all load
+ * cases), per-instance convergence masks, the solve captured as a CUDA graph. The lane layout,
+ * block size and task packing are chosen by an autotuner at the first solve and cached per
+ * matrix shape for the process (environment MAILLE_AUTOTUNE_CACHE = a file keeps them across
+ * processes). Each instance follows its own Model::solve contract: IC(0)-PCG to
+ * ||r|| <= rel_tol ||b|| per load case, u = imposed values at fixed DOFs. */
+
+/* Largest number of load cases per instance. */
+#define MAILLE_BATCH_MAX_RHS 8
+
+typedef struct {
+    int32_t n_instances;
+    int32_t nodes_per_elem;      /* 4 or 10, every instance */
+    int32_t n_rhs;               /* load cases per instance, 1..MAILLE_BATCH_MAX_RHS */
+    const int64_t* node_offset;  /* [n_instances + 1] instance k owns nodes [node_offset[k],
+                                    node_offset[k + 1]) of the packed node arrays */
+    const int64_t* elem_offset;  /* [n_instances + 1] and elements [elem_offset[k], ...) */
+    const double* coords;        /* [3 total_nodes] */
+    const int64_t* conn;         /* [total_elems * nodes_per_elem] node ids LOCAL to the
+                                    instance (0 .. its node count - 1) */
+    const double* young;         /* [total_elems] */
+    const double* poisson;       /* [total_elems] */
+    const uint8_t* fixed;        /* [3 total_nodes] */
+    const double* imposed;       /* [3 total_nodes] imposed values at fixed DOFs, or NULL */
+    const double* f;             /* [n_rhs][3 total_nodes] load cases (load case j of instance k
+                                    at f[j * 3 total_nodes + 3 node_offset[k] ...]), or NULL */
+    double rel_tol;              /* <= 0 selects 1e-12 */
+    int32_t max_iter;            /* per instance; <= 0 selects 10000 */
+    int32_t precision;           /* MaillePrecision */
+    int32_t device;
+} MailleBatchProblem;
+
+typedef struct {
+    double* u;                   /* [n_rhs][3 total_nodes] displacements, or NULL */
+    int32_t* iterations;         /* [n_instances * n_rhs] iterations each load case took, or NULL */
+    double* rel_residual;        /* [n_instances * n_rhs] final ||r|| / ||b||, or NULL */
+    int32_t* status;             /* [n_instances] MailleStatus of each instance, or NULL */
+    /* filled by the library */
+    int32_t max_iterations;      /* iterations of the slowest instance */
+    int32_t levels;
+    int64_t free_dofs;           /* over all instances (per load case) */
+    int64_t block_rows;
+    int64_t blocks;
+    int32_t lanes_per_row;       /* autotuned: lanes sharing one row (load-case groups x sub-lanes) */
+    int32_t rhs_per_lane;        /* autotuned: load cases one lane carries */
+    int32_t threads;             /* autotuned: threads per block */
+    int32_t task_slices;         /* autotuned: slices per vector task */
+    int32_t autotuned;           /* 1 when this call ran the tuner, 0 when the cache served it */
+    double ms_setup, ms_upload, ms_assembly, ms_factor, ms_tune, ms_solve, ms_download;
+} MailleBatchResult;
+
+typedef struct MailleGpuBatch MailleGpuBatch;
+
+/* One-shot: create + solve + destroy. Returns MAILLE_OK when every instance converged, else the
+ * first failing instance's status (per-instance statuses in result->status). */
+int32_t maille_gpu_batched_solve(const MailleBatchProblem* problem, MailleBatchResult* result);
+
+/* Packing + symbolic analysis + upload + element integration + assembly + IC(0) of all
+ * instances. */
+int32_t maille_gpu_batch_create(const MailleBatchProblem* problem, MailleGpuBatch** out);
+
+/* Solves every instance for every load case (f as in the problem, NULL = the problem's). */
+int32_t maille_gpu_batch_solve(MailleGpuBatch* b, const double* f, MailleBatchResult* result);
+
+/* New per-element materials ([total_elems] each, NULL keeps the current ones): element
+ * integration, assembly and IC(0) again on the same packing. */
+int32_t maille_gpu_batch_refactor(MailleGpuBatch* b, const double* young, const double* poisson);
+
+/* Raise (1) or clear (0) the batch's cancel flag; the running kernel polls it once per PCG
+ * pass and the solve returns MAILLE_CANCELLED. Safe to call from another thread. */
+void maille_gpu_batch_cancel(MailleGpuBatch* b, int32_t flag);
+
+/* CUDA stream of the batch, for event timing by the caller. */
+void* maille_gpu_batch_stream(MailleGpuBatch* b);
+
+void maille_gpu_batch_destroy(MailleGpuBatch* b);
+
 /* Largest n_block_rows that maille_gpu_bsr3_spmv_dot_noalloc accepts (2^26 block rows, i.e.
  * about 2e8 DOFs, inside the 32-bit column indices of the matrix). */
 #define MAILLE_NOALLOC_MAX_BLOCK_ROWS (INT64_C(1) << 26)

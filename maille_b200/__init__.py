@@ -8,3 +8,4 @@ from .model import (Bc, Dof, Field, ITERATIVE_FROM, Load, MailleError, Material,
 from ._lib import MAILLE_FP64, MAILLE_MIXED, MAILLE_ORDER_AUTO, MAILLE_ORDER_MULTICOLOR, MAILLE_ORDER_RCM  # noqa: F401
 
 __version__ = "0.1.0"
+from .batch import BatchField, BatchSolver, partition_lpt, solve_sharded  # noqa: F401,E402

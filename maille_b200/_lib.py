@@ -48,6 +48,33 @@ class ElasticResult(ctypes.Structure):
     ]
 
 
+MAILLE_BATCH_MAX_RHS = 8
+
+
+class BatchProblem(ctypes.Structure):
+    _fields_ = [
+        ("n_instances", ctypes.c_int32), ("nodes_per_elem", ctypes.c_int32),
+        ("n_rhs", ctypes.c_int32), ("node_offset", _i64), ("elem_offset", _i64),
+        ("coords", _d), ("conn", _i64), ("young", _d), ("poisson", _d), ("fixed", _u8),
+        ("imposed", _d), ("f", _d), ("rel_tol", ctypes.c_double), ("max_iter", ctypes.c_int32),
+        ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+    ]
+
+
+class BatchResult(ctypes.Structure):
+    _fields_ = [
+        ("u", _d), ("iterations", _i32), ("rel_residual", _d), ("status", _i32),
+        ("max_iterations", ctypes.c_int32), ("levels", ctypes.c_int32),
+        ("free_dofs", ctypes.c_int64), ("block_rows", ctypes.c_int64), ("blocks", ctypes.c_int64),
+        ("lanes_per_row", ctypes.c_int32), ("rhs_per_lane", ctypes.c_int32),
+        ("threads", ctypes.c_int32), ("task_slices", ctypes.c_int32), ("autotuned", ctypes.c_int32),
+        ("ms_setup", ctypes.c_double), ("ms_upload", ctypes.c_double),
+        ("ms_assembly", ctypes.c_double), ("ms_factor", ctypes.c_double),
+        ("ms_tune", ctypes.c_double), ("ms_solve", ctypes.c_double),
+        ("ms_download", ctypes.c_double),
+    ]
+
+
 # every symbol include/maille_gpu.h declares, with its ctypes signature
 SIGNATURES = {
     "maille_gpu_last_error": ([], ctypes.c_char_p),
@@ -72,6 +99,15 @@ SIGNATURES = {
                                          ctypes.c_int32),
     "maille_gpu_face_pressure_loads": ([ctypes.c_int64, _d, ctypes.c_int32, ctypes.c_int64, _i64,
                                         ctypes.c_int64, _i64, _i32, _d, _d], ctypes.c_int32),
+    "maille_gpu_batched_solve": ([ctypes.POINTER(BatchProblem), ctypes.POINTER(BatchResult)],
+                                 ctypes.c_int32),
+    "maille_gpu_batch_create": ([ctypes.POINTER(BatchProblem), ctypes.POINTER(ctypes.c_void_p)],
+                                ctypes.c_int32),
+    "maille_gpu_batch_solve": ([ctypes.c_void_p, _d, ctypes.POINTER(BatchResult)], ctypes.c_int32),
+    "maille_gpu_batch_refactor": ([ctypes.c_void_p, _d, _d], ctypes.c_int32),
+    "maille_gpu_batch_cancel": ([ctypes.c_void_p, ctypes.c_int32], None),
+    "maille_gpu_batch_stream": ([ctypes.c_void_p], ctypes.c_void_p),
+    "maille_gpu_batch_destroy": ([ctypes.c_void_p], None),
 }
 
 _lib = None

@@ -1,0 +1,965 @@
+// batch.cu -- the batched solve driver and its C ABI (maille_gpu_batch_* in
+// include/maille_gpu.h).
+//
+// create: the instances are packed into one mesh (node ids offset by the instance's first node),
+//   analysed once (setup.cpp: the union graph has one component per instance, so the RCM visit,
+//   the colouring and hence the levels of every instance are those it would get alone), uploaded,
+//   integrated, assembled and factorised with the same kernels as a single model. Rows of one
+//   instance couple only to rows of the same instance: the packed matrix is block diagonal.
+// solve: right-hand sides of all load cases, then ONE persistent kernel (batch_kernels.cu) that
+//   runs the PCG of every instance and load case to the end; the RHS build, the state reset,
+//   the PCG kernel and the gather of u are captured once as a CUDA graph and replayed.
+// autotune: the first solve of a shape times a few passes of every candidate lane layout
+//   (load cases per lane, sub-lanes per row), block size and task packing, keeps the fastest
+//   and caches it per matrix shape (process-wide table behind a mutex, optionally a file).
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "batch.cuh"
+#include "common.hpp"
+#include "cuda_host.hpp"
+#include "kernels.cuh"
+#include "sparse.cuh"
+
+using namespace maille;
+
+namespace {
+
+struct BatchConfig {
+    int Q = 0, SUB = 1, threads = 256, task = 8;
+    bool valid() const { return Q > 0; }
+};
+
+struct BLayout {
+    BSellHost h;
+    int32_t *rowid = nullptr, *col = nullptr, *src = nullptr, *inst = nullptr;
+    int64_t* off = nullptr;
+    void upload(cudaStream_t st) {
+        rowid = dupload(h.rowid.data(), h.rowid.size(), st);
+        col = dupload(h.col.data(), h.col.size(), st);
+        src = dupload(h.src.data(), h.src.size(), st);
+        inst = dupload(h.inst.data(), h.inst.size(), st);
+        off = dupload(h.off.data(), h.off.size(), st);
+    }
+    void release() {
+        for (void* p : {(void*)rowid, (void*)col, (void*)src, (void*)inst, (void*)off}) dfree(p);
+        rowid = col = src = inst = nullptr;
+        off = nullptr;
+    }
+    BSellDev dev() const { return BSellDev{h.nslices(), rowid, off, col, inst}; }
+};
+
+std::mutex g_tune_mutex;
+std::map<std::string, BatchConfig> g_tune_cache;
+bool g_tune_file_loaded = false;
+
+const char* tune_file() { return std::getenv("MAILLE_AUTOTUNE_CACHE"); }
+
+void load_tune_file_locked() {
+    if (g_tune_file_loaded) return;
+    g_tune_file_loaded = true;
+    const char* path = tune_file();
+    if (!path) return;
+    std::ifstream in(path);
+    std::string key;
+    BatchConfig c;
+    while (in >> key >> c.Q >> c.SUB >> c.threads >> c.task)
+        if (c.valid()) g_tune_cache[key] = c;
+}
+
+void store_tune_locked(const std::string& key, const BatchConfig& c) {
+    g_tune_cache[key] = c;
+    if (const char* path = tune_file()) {
+        std::ofstream out(path, std::ios::app);
+        out << key << ' ' << c.Q << ' ' << c.SUB << ' ' << c.threads << ' ' << c.task << '\n';
+    }
+}
+
+}  // namespace
+
+struct MailleGpuBatch {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[8] = {};
+    int32_t n_inst = 0, npe = 0, n_rhs = 0, R = 0, precision = MAILLE_FP64, max_iter = kDefaultMaxIter;
+    double tol = kDefaultTol, delta = 0.1;
+    int64_t n_nodes = 0, n_elems = 0;
+    std::vector<int64_t> node_off, elem_off;
+    std::vector<uint8_t> h_fixed;
+    std::vector<double> h_imposed, h_f0;
+    bool any_imposed = false;
+    Symbolic sym;
+    std::vector<int32_t> row_inst;
+    // device: inputs (packed numbering)
+    double *coords = nullptr, *young = nullptr, *poisson = nullptr, *imposed = nullptr, *f0 = nullptr,
+           *f = nullptr;
+    const double* f_cur = nullptr;
+    int32_t* conn = nullptr;
+    uint8_t* fixed = nullptr;
+    // device: symbolic
+    int32_t *perm = nullptr, *inv = nullptr, *col = nullptr, *lrow = nullptr, *inc = nullptr,
+            *belem = nullptr, *bnodes = nullptr, *elem_slot = nullptr;
+    uint8_t* fixmask = nullptr;
+    int64_t *row_ptr = nullptr, *diag = nullptr, *tpos = nullptr, *lslot = nullptr, *lptr = nullptr,
+            *inc_ptr = nullptr;
+    uint32_t* contrib = nullptr;
+    // device: numeric (CSR), coupling scratch
+    double *ke = nullptr, *K = nullptr, *F = nullptr, *y_full = nullptr, *ye = nullptr;
+    double shift = 0.0;
+    // configuration-dependent: layouts, values, task tables, reduction slots
+    BatchConfig cfg;
+    BLayout lk, ll, lu;
+    void *Kv = nullptr, *Lv = nullptr, *Uv = nullptr, *D = nullptr;
+    double* K64 = nullptr;
+    int32_t *task_off = nullptr, *task_inst = nullptr, *inst_task = nullptr, *uslot = nullptr,
+            *inst_uslot = nullptr, *bwd_seq = nullptr;
+    int32_t ntasks = 0;
+    double *part_k = nullptr, *part_u = nullptr;
+    int grid = 0;
+    // vectors [(nb + 1) R 3]
+    void *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr;
+    double *b = nullptr, *x64 = nullptr, *r64 = nullptr;
+    double* u_out = nullptr;  // [n_rhs 3 N]
+    // state
+    BatchState state{};
+    std::vector<void*> state_bufs;
+    unsigned int* tickets = nullptr;
+    unsigned int* flags = nullptr;
+    int32_t* h_cancel = nullptr;  // mapped pinned host memory
+    int32_t* d_cancel = nullptr;
+    unsigned long long* timing = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    const double* graph_f = nullptr;  // load buffer the graph was captured with
+    bool graph_tried = false;
+    long long graph_kernels = 0;
+    std::vector<int32_t> h_iter, h_col_iter, h_status;
+    std::vector<double> h_rr, h_bb;
+    std::vector<int32_t> h_ctrl;
+
+    bool mixed() const { return precision == MAILLE_MIXED; }
+    BatchShape shape() const { return BatchShape{R, cfg.Q, cfg.SUB}; }
+    Pattern pattern() const { return Pattern{sym.nb, row_ptr, col, diag, tpos, fixmask}; }
+    size_t vec_len() const { return ((size_t)sym.nb + 1) * R * 3; }
+    void release_config() {
+        for (BLayout* l : {&lk, &ll, &lu}) l->release();
+        for (void* q : {Kv, Lv, Uv, D, (void*)K64, (void*)task_off, (void*)task_inst, (void*)inst_task,
+                        (void*)uslot, (void*)inst_uslot, (void*)bwd_seq, (void*)part_k, (void*)part_u})
+            dfree(q);
+        Kv = Lv = Uv = D = nullptr;
+        K64 = nullptr;
+        task_off = task_inst = inst_task = uslot = inst_uslot = bwd_seq = nullptr;
+        part_k = part_u = nullptr;
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        graph_tried = false;
+    }
+    ~MailleGpuBatch() {
+        cudaSetDevice(device);
+        if (timing) {
+            unsigned long long t[8] = {0};
+            cudaMemcpy(t, timing, sizeof(t), cudaMemcpyDeviceToHost);
+            std::fprintf(stderr,
+                         "maille batch phase timing (ms, block 0): spmv %.3f update %.3f residual %.3f "
+                         "fwd %.3f bwd %.3f pupdate %.3f init %.3f launches %llu grid %d\n",
+                         t[0] * 1e-6, t[1] * 1e-6, t[2] * 1e-6, t[3] * 1e-6, t[4] * 1e-6, t[5] * 1e-6,
+                         t[7] * 1e-6, t[6], grid);
+        }
+        release_config();
+        void* bufs[] = {coords, young, poisson, imposed, f0, f, conn, fixed, perm, inv, col, lrow, inc,
+                        belem, bnodes, elem_slot, fixmask, row_ptr, diag, tpos, lslot, lptr, inc_ptr,
+                        contrib, ke, K, F, y_full, ye, x, r, z, p, ap, b, x64, r64, u_out, tickets,
+                        flags, timing};
+        for (void* q : bufs) dfree(q);
+        for (void* q : state_bufs) dfree(q);
+        if (h_cancel) cudaFreeHost(h_cancel);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+namespace {
+
+int32_t fail(const Error& e) {
+    set_last_error(e.message);
+    return e.status;
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+int env_int(const char* name, int dflt) {
+    const char* e = std::getenv(name);
+    return e ? std::atoi(e) : dflt;
+}
+
+int pad_rhs(int n) { return n <= 2 ? 2 : (n <= 4 ? 4 : 8); }
+
+bool check_batch(const MailleBatchProblem* p, Error& err) {
+    if (!p) {
+        err = {MAILLE_INVALID_INPUT, "null problem"};
+        return false;
+    }
+    if (p->n_instances <= 0 || !p->node_offset || !p->elem_offset) {
+        err = {MAILLE_INVALID_INPUT, "n_instances, node_offset and elem_offset are required"};
+        return false;
+    }
+    if (p->n_rhs < 1 || p->n_rhs > MAILLE_BATCH_MAX_RHS) {
+        err = {MAILLE_INVALID_INPUT, "n_rhs must be in 1.." + std::to_string(MAILLE_BATCH_MAX_RHS)};
+        return false;
+    }
+    if (p->nodes_per_elem != 4 && p->nodes_per_elem != 10) {
+        err = {MAILLE_INVALID_INPUT, "nodes_per_elem must be 4 or 10"};
+        return false;
+    }
+    if (!p->coords || !p->conn || !p->young || !p->poisson) {
+        err = {MAILLE_INVALID_INPUT, "coords, conn, young and poisson are required"};
+        return false;
+    }
+    if (p->precision != MAILLE_FP64 && p->precision != MAILLE_MIXED) {
+        err = {MAILLE_INVALID_INPUT, "unknown precision"};
+        return false;
+    }
+    if (p->node_offset[0] != 0 || p->elem_offset[0] != 0) {
+        err = {MAILLE_INVALID_INPUT, "offsets must start at 0"};
+        return false;
+    }
+    for (int32_t k = 0; k < p->n_instances; ++k) {
+        const int64_t nn = p->node_offset[k + 1] - p->node_offset[k];
+        const int64_t ne = p->elem_offset[k + 1] - p->elem_offset[k];
+        if (nn <= 0 || ne <= 0) {
+            err = {MAILLE_INVALID_INPUT, "instance " + std::to_string(k) + " has no nodes or no elements"};
+            return false;
+        }
+        for (int64_t e = p->elem_offset[k] * p->nodes_per_elem; e < p->elem_offset[k + 1] * p->nodes_per_elem; ++e)
+            if (p->conn[e] < 0 || p->conn[e] >= nn) {
+                err = {MAILLE_INVALID_INPUT, "instance " + std::to_string(k) + ": element " +
+                                                 std::to_string(e / p->nodes_per_elem - p->elem_offset[k]) +
+                                                 " refers to unknown node " + std::to_string(p->conn[e])};
+                return false;
+            }
+    }
+    const int64_t N = p->node_offset[p->n_instances], E = p->elem_offset[p->n_instances];
+    for (int64_t k = 0; k < 3 * N; ++k)
+        if (!std::isfinite(p->coords[k])) {
+            err = {MAILLE_INVALID_INPUT, "non-finite coordinate at node " + std::to_string(k / 3)};
+            return false;
+        }
+    for (int64_t e = 0; e < E; ++e)
+        if (!std::isfinite(p->young[e]) || !std::isfinite(p->poisson[e]) || p->young[e] <= 0.0 ||
+            p->poisson[e] <= -1.0 || p->poisson[e] >= 0.5) {
+            err = {MAILLE_INVALID_INPUT, "invalid material of element " + std::to_string(e)};
+            return false;
+        }
+    if (p->f)
+        for (int64_t k = 0; k < 3 * N * p->n_rhs; ++k)
+            if (!std::isfinite(p->f[k])) {
+                err = {MAILLE_INVALID_INPUT, "non-finite load at entry " + std::to_string(k)};
+                return false;
+            }
+    return true;
+}
+
+int32_t factorize(MailleGpuBatch* b, Error& err, int32_t* dfail) {
+    const Pattern pt = b->pattern();
+    for (double shift : kShifts) {
+        CK(cudaMemsetAsync(dfail, 0, sizeof(int32_t), b->st));
+        for (int l = 0; l < b->sym.levels; ++l)
+            launch_factor_level(pt, b->sym.level_ptr[l], b->sym.level_ptr[l + 1], b->K, b->F, shift, dfail,
+                                b->st);
+        CK(cudaGetLastError());
+        int32_t failed = 0;
+        CK(cudaMemcpyAsync(&failed, dfail, sizeof(int32_t), cudaMemcpyDeviceToHost, b->st));
+        CK(cudaStreamSynchronize(b->st));
+        if (!failed) {
+            b->shift = shift;
+            return MAILLE_OK;
+        }
+    }
+    err = {MAILLE_SINGULAR, "IC(0) failed with every diagonal shift (Singular)"};
+    return MAILLE_SINGULAR;
+}
+
+// element integration + assembly + IC(0) on the packed mesh (CSR K and F)
+int32_t numeric(MailleGpuBatch* b, Error& err) {
+    const Symbolic& s = b->sym;
+    ElemIn in{b->n_elems, b->coords, b->conn, b->young, b->poisson};
+    launch_elem_stiffness(b->npe, in, b->ke, b->st);
+    launch_assemble(b->pattern(), (int64_t)s.lslot.size(), b->lslot, b->lrow, b->lptr, b->contrib, b->ke, b->K,
+                    b->st);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(b->ev[6], b->st));
+    int32_t* dfail = dalloc<int32_t>(1);
+    const int32_t status = factorize(b, err, dfail);
+    cudaFree(dfail);
+    CK(cudaEventRecord(b->ev[7], b->st));
+    return status;
+}
+
+// values of the current configuration's layouts from K and F
+void fill_values(MailleGpuBatch* b) {
+    const int ss = b->lk.h.slots();
+    if (b->mixed()) {
+        launch_bsell_fill<float>(b->lk.h.steps(), ss, b->lk.src, b->K, (float*)b->Kv, b->st);
+        launch_bsell_fill<float>(b->ll.h.steps(), ss, b->ll.src, b->F, (float*)b->Lv, b->st);
+        launch_bsell_fill<float>(b->lu.h.steps(), ss, b->lu.src, b->F, (float*)b->Uv, b->st);
+        launch_diag_fill<float>(b->sym.nb, b->diag, b->F, (float*)b->D, b->st);
+        launch_bsell_fill<double>(b->lk.h.steps(), ss, b->lk.src, b->K, b->K64, b->st);
+    } else {
+        launch_bsell_fill<double>(b->lk.h.steps(), ss, b->lk.src, b->K, (double*)b->Kv, b->st);
+        launch_bsell_fill<double>(b->ll.h.steps(), ss, b->ll.src, b->F, (double*)b->Lv, b->st);
+        launch_bsell_fill<double>(b->lu.h.steps(), ss, b->lu.src, b->F, (double*)b->Uv, b->st);
+        launch_diag_fill<double>(b->sym.nb, b->diag, b->F, (double*)b->D, b->st);
+    }
+    CK(cudaGetLastError());
+}
+
+// Builds and uploads the layouts, task tables and reduction slots of configuration c, fills the
+// values, resets the row-ready flags for the configuration's group count, sizes the grid.
+bool apply_config(MailleGpuBatch* b, const BatchConfig& c, Error& err) {
+    const BatchShape shp{b->R, c.Q, c.SUB};
+    if (!batch_shape_supported(shp)) {
+        err = {MAILLE_INVALID_INPUT, "unsupported batch lane layout"};
+        return false;
+    }
+    const bool same_layout = b->cfg.valid() && b->cfg.Q == c.Q && b->cfg.SUB == c.SUB;
+    cudaStream_t st = b->st;
+    if (!same_layout) {
+        b->release_config();
+        const int rows = shp.rows();
+        std::thread tk([&] { build_bsell(b->sym, SELL_FULL, rows, c.SUB, b->row_inst, b->lk.h); });
+        std::thread tl([&] { build_bsell(b->sym, SELL_LOWER, rows, c.SUB, b->row_inst, b->ll.h); });
+        build_bsell(b->sym, SELL_UPPER, rows, c.SUB, b->row_inst, b->lu.h);
+        tk.join();
+        tl.join();
+        for (BLayout* l : {&b->lk, &b->ll, &b->lu}) l->upload(st);
+        const size_t ek = (size_t)b->lk.h.steps() * 9 * shp.slots(), el = (size_t)b->ll.h.steps() * 9 * shp.slots(),
+                     eu = (size_t)b->lu.h.steps() * 9 * shp.slots();
+        if (b->mixed()) {
+            b->Kv = dalloc<float>(ek);
+            b->Lv = dalloc<float>(el);
+            b->Uv = dalloc<float>(eu);
+            b->D = dalloc<float>((size_t)b->sym.nb * 9);
+            b->K64 = dalloc<double>(ek);
+        } else {
+            b->Kv = dalloc<double>(ek);
+            b->Lv = dalloc<double>(el);
+            b->Uv = dalloc<double>(eu);
+            b->D = dalloc<double>((size_t)b->sym.nb * 9);
+        }
+        // U slices: reduction slot in instance-major order; backward order by level, descending
+        const int32_t nu = b->lu.h.nslices();
+        std::vector<int32_t> count(b->n_inst + 1, 0), uslot(nu), seq;
+        for (int32_t k = 0; k < nu; ++k) count[b->lu.h.inst[k] + 1]++;
+        for (int32_t i = 0; i < b->n_inst; ++i) count[i + 1] += count[i];
+        {
+            std::vector<int32_t> cur(count.begin(), count.end() - 1);
+            for (int32_t k = 0; k < nu; ++k) uslot[k] = cur[b->lu.h.inst[k]]++;
+        }
+        const auto& ls = b->lu.h.level_slices;
+        for (int l = b->sym.levels - 1; l >= 0; --l)
+            for (int32_t k = ls[l]; k < ls[l + 1]; ++k) seq.push_back(k);
+        b->uslot = dupload(uslot.data(), uslot.size(), st);
+        b->inst_uslot = dupload(count.data(), count.size(), st);
+        b->bwd_seq = dupload(seq.data(), seq.size(), st);
+        b->part_u = dalloc<double>((size_t)std::max(1, nu) * b->R);
+        fill_values(b);
+        // flags: rows 0 .. nb-1 of every group not ready, the dummy row always ready
+        const int G = shp.groups();
+        std::vector<unsigned int> fl(((size_t)b->sym.nb + 1) * 8, 0u);
+        for (int gi = 0; gi < G; ++gi) fl[(size_t)b->sym.nb * G + gi] = 0xFFFFFFFFu;
+        CK(cudaMemcpyAsync(b->flags, fl.data(), fl.size() * sizeof(unsigned int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(b->state.ctrl + 4, 0, sizeof(int32_t), st));
+        CK(cudaStreamSynchronize(st));  // the host vectors above go out of scope
+    } else {
+        for (void* q : {(void*)b->task_off, (void*)b->task_inst, (void*)b->inst_task, (void*)b->part_k}) dfree(q);
+        b->task_off = b->task_inst = b->inst_task = nullptr;
+        b->part_k = nullptr;
+        if (b->graph) cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        b->graph_tried = false;
+    }
+    // vector tasks: runs of at most c.task consecutive K slices of one instance
+    {
+        std::vector<int32_t> toff{0}, tinst, itask(b->n_inst + 1, 0);
+        const int32_t nk = b->lk.h.nslices();
+        int32_t k = 0;
+        while (k < nk) {
+            const int32_t inst = b->lk.h.inst[k];
+            int32_t e = k + 1;
+            while (e < nk && e - k < c.task && b->lk.h.inst[e] == inst) ++e;
+            toff.push_back(e);
+            tinst.push_back(inst);
+            itask[inst + 1]++;
+            k = e;
+        }
+        for (int32_t i = 0; i < b->n_inst; ++i) itask[i + 1] += itask[i];
+        b->ntasks = (int32_t)tinst.size();
+        b->task_off = dupload(toff.data(), toff.size(), st);
+        b->task_inst = dupload(tinst.data(), tinst.size(), st);
+        b->inst_task = dupload(itask.data(), itask.size(), st);
+        b->part_k = dalloc<double>((size_t)std::max(1, b->ntasks) * b->R);
+        CK(cudaStreamSynchronize(st));
+    }
+    b->cfg = c;
+    b->grid = b->mixed() ? batch_grid<float, float, true>(shp, c.threads) : batch_grid<double, double, false>(shp, c.threads);
+    if (b->grid <= 0) {
+        err = {MAILLE_CUDA_ERROR, "the batched PCG kernel cannot be resident with " + std::to_string(c.threads) +
+                                      " threads per block"};
+        return false;
+    }
+    return true;
+}
+
+template <typename M, typename T>
+BatchArgs<M, T> batch_args(MailleGpuBatch* b) {
+    BatchArgs<M, T> a{};
+    a.nb = b->sym.nb;
+    a.n_inst = b->n_inst;
+    a.n_rhs = b->n_rhs;
+    a.max_iter = b->max_iter;
+    a.tol2 = b->tol * b->tol;
+    a.delta2 = b->delta * b->delta;
+    a.K = b->lk.dev();
+    a.L = b->ll.dev();
+    a.U = b->lu.dev();
+    a.ntasks = b->ntasks;
+    a.task_off = b->task_off;
+    a.task_inst = b->task_inst;
+    a.inst_task = b->inst_task;
+    a.uslot = b->uslot;
+    a.inst_uslot = b->inst_uslot;
+    a.bwd_seq = b->bwd_seq;
+    a.Kv = (const M*)b->Kv;
+    a.Lv = (const M*)b->Lv;
+    a.Uv = (const M*)b->Uv;
+    a.D = (const M*)b->D;
+    a.x = (T*)b->x;
+    a.r = (T*)b->r;
+    a.z = (T*)b->z;
+    a.p = (T*)b->p;
+    a.ap = (T*)b->ap;
+    a.K64 = b->K64;
+    a.b = b->b;
+    a.x64 = b->x64;
+    a.r64 = b->r64;
+    a.st = b->state;
+    a.part_k = b->part_k;
+    a.part_u = b->part_u;
+    a.tickets = b->tickets;
+    a.flags = b->flags;
+    a.cancel = b->d_cancel;
+    a.timing = b->timing;
+    return a;
+}
+
+// reset + persistent PCG of `passes` passes (the kernel stops earlier when every instance has)
+void enqueue_pcg(MailleGpuBatch* b, int passes) {
+    launch_batch_reset(b->state.ctrl, b->n_inst, b->tickets, 3 * (int64_t)b->n_inst, b->st);
+    const BatchShape shp = b->shape();
+    if (b->mixed()) {
+        CK((launch_batch_pcg<float, float, true>(shp, batch_args<float, float>(b), b->grid, b->cfg.threads, passes, b->st)));
+    } else {
+        CK((launch_batch_pcg<double, double, false>(shp, batch_args<double, double>(b), b->grid, b->cfg.threads, passes,
+                                                     b->st)));
+    }
+}
+
+// b = F_j - K_fc u_c for every load case, in the batched vector layout
+void enqueue_rhs(MailleGpuBatch* b) {
+    const double* coupling = nullptr;
+    const Symbolic& s = b->sym;
+    const int64_t n3 = 3 * b->n_nodes;
+    if (b->any_imposed) {
+        CK(cudaMemsetAsync(b->y_full, 0, n3 * sizeof(double), b->st));
+        launch_elem_apply(b->npe, (int64_t)s.belem.size(), b->belem, b->conn, b->ke, b->imposed, b->ye, b->st);
+        launch_node_gather(b->npe, (int64_t)s.bnodes.size(), b->bnodes, b->inc_ptr, b->inc, b->elem_slot, b->ye,
+                           b->y_full, b->st);
+        coupling = b->y_full;
+    }
+    launch_batch_rhs(s.nb, b->R, b->n_rhs, n3, b->perm, b->fixmask, b->f_cur, coupling, b->b, b->st);
+}
+
+void enqueue_gather(MailleGpuBatch* b) {
+    launch_batch_gather(b->n_nodes, b->R, b->n_rhs, b->inv, b->fixed, b->imposed, b->mixed() ? b->x64 : (double*)b->x,
+                        b->mixed() ? (const float*)b->x : nullptr, b->u_out, b->st);
+}
+
+std::vector<BatchConfig> candidates(int R, bool mixed) {
+    std::vector<BatchConfig> out;
+    std::vector<std::pair<int, int>> qs;
+    if (R == 8) qs = {{8, 1}, {8, 2}, {4, 1}, {4, 2}, {2, 1}};
+    else if (R == 4) qs = {{4, 1}, {4, 2}, {2, 1}};
+    else qs = {{2, 1}, {2, 2}, {1, 1}};
+    for (auto [q, sub] : qs)
+        for (int threads : {128, 256})
+            for (int task : {4, 16}) out.push_back(BatchConfig{q, sub, threads, task});
+    (void)mixed;
+    return out;
+}
+
+std::string shape_key(const MailleGpuBatch* b) {
+    std::ostringstream k;
+    k << "npe" << b->npe << "_R" << b->R << "_p" << b->precision << "_inst" << b->n_inst << "_nb" << b->sym.nb
+      << "_blk" << b->sym.blocks;
+    return k.str();
+}
+
+// Picks the configuration: the cached one for this shape, or the fastest of the candidates
+// over a few PCG passes (times with events on the batch stream). Returns true when it tuned.
+bool choose_config(MailleGpuBatch* b, Error& err, bool& tuned) {
+    tuned = false;
+    const std::string key = shape_key(b);
+    BatchConfig forced;
+    forced.Q = env_int("MAILLE_BATCH_Q", 0);
+    if (forced.Q > 0) {
+        forced.SUB = env_int("MAILLE_BATCH_SUB", 1);
+        forced.threads = env_int("MAILLE_BATCH_THREADS", 256);
+        forced.task = env_int("MAILLE_BATCH_TASK", 8);
+        return apply_config(b, forced, err);
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        load_tune_file_locked();
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) return apply_config(b, it->second, err);
+    }
+    const int passes = std::max(2, env_int("MAILLE_TUNE_PASSES", 6));
+    float best = 1e30f;
+    BatchConfig best_cfg;
+    std::vector<BatchConfig> cands = candidates(b->R, b->mixed());
+    // layouts first (fewest rebuilds): candidates are grouped by (Q, SUB)
+    for (const BatchConfig& c : cands) {
+        if (!apply_config(b, c, err)) return false;
+        enqueue_rhs(b);
+        enqueue_pcg(b, 1);  // warm-up: first pass of this kernel
+        CK(cudaEventRecord(b->ev[0], b->st));
+        enqueue_pcg(b, passes);
+        CK(cudaEventRecord(b->ev[1], b->st));
+        CK(cudaEventSynchronize(b->ev[1]));
+        int32_t ctrl[5] = {0};
+        CK(cudaMemcpy(ctrl, b->state.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost));
+        if (ctrl[2] != 0) {
+            err = {MAILLE_CUDA_ERROR, "batched PCG: a sweep wait timed out while tuning"};
+            return false;
+        }
+        const float ms = elapsed(b->ev[0], b->ev[1]);
+        if (ms < best) {
+            best = ms;
+            best_cfg = c;
+        }
+    }
+    if (!apply_config(b, best_cfg, err)) return false;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        store_tune_locked(key, best_cfg);
+    }
+    tuned = true;
+    return true;
+}
+
+int32_t create_batch(const MailleBatchProblem* p, MailleGpuBatch** out) {
+    Error err{MAILLE_OK, ""};
+    if (!out) return fail({MAILLE_INVALID_INPUT, "null handle pointer"});
+    *out = nullptr;
+    if (!check_batch(p, err)) return fail(err);
+    auto b = std::make_unique<MailleGpuBatch>();
+    b->device = p->device;
+    b->n_inst = p->n_instances;
+    b->npe = p->nodes_per_elem;
+    b->n_rhs = p->n_rhs;
+    b->R = pad_rhs(p->n_rhs);
+    b->precision = p->precision;
+    b->tol = p->rel_tol > 0 ? p->rel_tol : kDefaultTol;
+    b->max_iter = p->max_iter > 0 ? p->max_iter : kDefaultMaxIter;
+    if (const char* e = std::getenv("MAILLE_RELIABLE_DELTA")) b->delta = std::atof(e);
+    b->node_off.assign(p->node_offset, p->node_offset + p->n_instances + 1);
+    b->elem_off.assign(p->elem_offset, p->elem_offset + p->n_instances + 1);
+    b->n_nodes = b->node_off.back();
+    b->n_elems = b->elem_off.back();
+    const int64_t n3 = 3 * b->n_nodes;
+    b->h_fixed.assign(n3, 0);
+    if (p->fixed)
+        for (int64_t k = 0; k < n3; ++k) b->h_fixed[k] = p->fixed[k] ? 1 : 0;
+    b->h_imposed.assign(n3, 0.0);
+    if (p->imposed)
+        for (int64_t k = 0; k < n3; ++k)
+            if (b->h_fixed[k]) {
+                if (!std::isfinite(p->imposed[k])) return fail({MAILLE_INVALID_INPUT, "non-finite imposed value"});
+                b->h_imposed[k] = p->imposed[k];
+                b->any_imposed = b->any_imposed || p->imposed[k] != 0.0;
+            }
+    b->h_f0.assign((size_t)n3 * b->n_rhs, 0.0);
+    if (p->f) std::memcpy(b->h_f0.data(), p->f, b->h_f0.size() * sizeof(double));
+
+    // the packed mesh: node ids offset by the instance's first node
+    const double t0 = now_ms();
+    std::vector<int64_t> conn((size_t)b->n_elems * b->npe);
+    for (int32_t k = 0; k < b->n_inst; ++k)
+        for (int64_t e = b->elem_off[k] * b->npe; e < b->elem_off[k + 1] * b->npe; ++e)
+            conn[e] = p->conn[e] + b->node_off[k];
+    if (!analyse(b->n_nodes, b->npe, b->n_elems, conn.data(), b->h_fixed.data(), MAILLE_ORDER_MULTICOLOR, b->sym,
+                 err))
+        return fail(err);
+    const Symbolic& s = b->sym;
+    if (s.levels >= kMaxLevels) return fail({MAILLE_INVALID_INPUT, "too many IC(0) levels"});
+    b->row_inst.resize(s.nb);
+    {
+        std::vector<int32_t> node_inst(b->n_nodes);
+        for (int32_t k = 0; k < b->n_inst; ++k)
+            for (int64_t v = b->node_off[k]; v < b->node_off[k + 1]; ++v) node_inst[v] = k;
+        std::vector<int64_t> rows(b->n_inst, 0);
+        for (int32_t r = 0; r < s.nb; ++r) {
+            b->row_inst[r] = node_inst[s.perm[r]];
+            rows[b->row_inst[r]]++;
+        }
+        for (int32_t k = 0; k < b->n_inst; ++k)
+            if (rows[k] == 0) return fail({MAILLE_INVALID_INPUT, "instance " + std::to_string(k) + ": every DOF is fixed"});
+    }
+    const double t1 = now_ms();
+    try {
+        int ndev = 0;
+        CK(cudaGetDeviceCount(&ndev));
+        if (p->device < 0 || p->device >= ndev)
+            return fail({MAILLE_CUDA_ERROR, "no CUDA device " + std::to_string(p->device)});
+        CK(cudaSetDevice(p->device));
+        CK(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+        for (auto& e : b->ev) CK(cudaEventCreate(&e));
+        cudaStream_t st = b->st;
+        CK(cudaEventRecord(b->ev[4], st));
+        std::vector<int32_t> conn32(conn.size());
+        for (size_t k = 0; k < conn.size(); ++k) conn32[k] = (int32_t)conn[k];
+        b->coords = dupload(p->coords, n3, st);
+        b->conn = dupload(conn32.data(), conn32.size(), st);
+        b->young = dupload(p->young, b->n_elems, st);
+        b->poisson = dupload(p->poisson, b->n_elems, st);
+        b->imposed = dupload(b->h_imposed.data(), n3, st);
+        b->fixed = dupload(b->h_fixed.data(), n3, st);
+        b->f0 = dupload(b->h_f0.data(), b->h_f0.size(), st);
+        b->f = dalloc<double>(b->h_f0.size());
+        b->f_cur = b->f0;
+        b->perm = dupload(s.perm.data(), s.perm.size(), st);
+        b->inv = dupload(s.inv.data(), s.inv.size(), st);
+        b->fixmask = dupload(s.fixmask.data(), s.fixmask.size(), st);
+        b->row_ptr = dupload(s.row_ptr.data(), s.row_ptr.size(), st);
+        b->col = dupload(s.col.data(), s.col.size(), st);
+        b->diag = dupload(s.diag.data(), s.diag.size(), st);
+        b->tpos = dupload(s.tpos.data(), s.tpos.size(), st);
+        std::vector<int32_t> lrow(s.lslot.size());
+        {
+            size_t q = 0;
+            for (int32_t r = 0; r < s.nb; ++r)
+                for (int64_t pp = s.row_ptr[r]; pp <= s.diag[r]; ++pp) lrow[q++] = r;
+        }
+        b->lslot = dupload(s.lslot.data(), s.lslot.size(), st);
+        b->lrow = dupload(lrow.data(), lrow.size(), st);
+        b->lptr = dupload(s.lptr.data(), s.lptr.size(), st);
+        b->contrib = dupload(s.contrib.data(), s.contrib.size(), st);
+        b->inc_ptr = dupload(s.inc_ptr.data(), s.inc_ptr.size(), st);
+        b->inc = dupload(s.inc.data(), s.inc.size(), st);
+        b->belem = dupload(s.belem.data(), s.belem.size(), st);
+        b->bnodes = dupload(s.bnodes.data(), s.bnodes.size(), st);
+        std::vector<int32_t> slot(b->n_elems, -1);
+        for (size_t k = 0; k < s.belem.size(); ++k) slot[s.belem[k]] = (int32_t)k;
+        b->elem_slot = dupload(slot.data(), slot.size(), st);
+        b->ke = dalloc<double>((size_t)b->n_elems * node_pairs(b->npe) * 9);
+        b->K = dalloc<double>((size_t)s.blocks * 9);
+        b->F = dalloc<double>((size_t)s.blocks * 9);
+        b->y_full = dalloc<double>(n3);
+        b->ye = dalloc<double>(std::max<size_t>(1, s.belem.size()) * 3 * b->npe);
+        const size_t nv = b->vec_len();
+        const size_t tsz = b->mixed() ? sizeof(float) : sizeof(double);
+        for (void** q : {&b->x, &b->r, &b->z, &b->p, &b->ap}) {
+            CK(cudaMalloc(q, nv * tsz));
+            CK(cudaMemsetAsync(*q, 0, nv * tsz, st));
+        }
+        b->b = dalloc<double>(nv);
+        if (b->mixed()) {
+            b->x64 = dalloc<double>(nv);
+            b->r64 = dalloc<double>(nv);
+            CK(cudaMemsetAsync(b->x64, 0, nv * sizeof(double), st));
+            CK(cudaMemsetAsync(b->r64, 0, nv * sizeof(double), st));
+        }
+        b->u_out = dalloc<double>((size_t)n3 * b->n_rhs);
+        // state arrays
+        const size_t ncol = (size_t)b->n_inst * b->R;
+        auto dd = [&](double*& q, size_t n) {
+            q = dalloc<double>(n);
+            CK(cudaMemsetAsync(q, 0, n * sizeof(double), st));
+            b->state_bufs.push_back(q);
+        };
+        auto di = [&](int32_t*& q, size_t n) {
+            q = dalloc<int32_t>(n);
+            CK(cudaMemsetAsync(q, 0, n * sizeof(int32_t), st));
+            b->state_bufs.push_back(q);
+        };
+        auto du = [&](uint32_t*& q, size_t n) {
+            q = dalloc<uint32_t>(n);
+            CK(cudaMemsetAsync(q, 0, n * sizeof(uint32_t), st));
+            b->state_bufs.push_back(q);
+        };
+        BatchState& S = b->state;
+        dd(S.alpha, ncol);
+        dd(S.beta, ncol);
+        dd(S.rz, ncol);
+        dd(S.rr, ncol);
+        dd(S.bb, ncol);
+        dd(S.maxr2, ncol);
+        di(S.iter, b->n_inst);
+        di(S.col_iter, ncol);
+        di(S.status, b->n_inst);
+        di(S.updates, b->n_inst);
+        du(S.done, b->n_inst);
+        du(S.flagged, b->n_inst);
+        di(S.ctrl, 8);
+        b->tickets = dalloc<unsigned int>(3 * (size_t)b->n_inst);
+        CK(cudaMemsetAsync(b->tickets, 0, 3 * (size_t)b->n_inst * sizeof(unsigned int), st));
+        b->flags = dalloc<unsigned int>(((size_t)s.nb + 1) * 8);
+        CK(cudaHostAlloc(&b->h_cancel, sizeof(int32_t), cudaHostAllocMapped));
+        *b->h_cancel = 0;
+        CK(cudaHostGetDevicePointer((void**)&b->d_cancel, b->h_cancel, 0));
+        if (env_int("MAILLE_PHASE_TIMING", 0)) {
+            b->timing = dalloc<unsigned long long>(8);
+            CK(cudaMemsetAsync(b->timing, 0, 8 * sizeof(unsigned long long), st));
+        }
+        CK(cudaEventRecord(b->ev[5], st));
+        if (numeric(b.get(), err) != MAILLE_OK) return fail(err);
+        CK(cudaStreamSynchronize(st));
+        b->h_ctrl.assign(8, 0);
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+    b->sym.ms = t1 - t0;
+    *out = b.release();
+    return MAILLE_OK;
+}
+
+int32_t solve_batch(MailleGpuBatch* b, const double* f, MailleBatchResult* res) {
+    if (!b) return fail({MAILLE_INVALID_INPUT, "null batch"});
+    Error err{MAILLE_OK, ""};
+    try {
+        CK(cudaSetDevice(b->device));
+        cudaStream_t st = b->st;
+        const int64_t n3 = 3 * b->n_nodes;
+        const size_t nf = (size_t)n3 * b->n_rhs;
+        double ms_tune = 0.0;
+        bool tuned = false;
+        if (!b->cfg.valid()) {
+            const double t0 = now_ms();
+            b->f_cur = b->f0;
+            if (!choose_config(b, err, tuned)) return fail(err);
+            ms_tune = now_ms() - t0;
+        }
+        CK(cudaEventRecord(b->ev[0], st));
+        if (f) {
+            for (size_t k = 0; k < nf; ++k)
+                if (!std::isfinite(f[k])) return fail({MAILLE_INVALID_INPUT, "non-finite load"});
+            CK(cudaMemcpyAsync(b->f, f, nf * sizeof(double), cudaMemcpyHostToDevice, st));
+            b->f_cur = b->f;
+        } else {
+            b->f_cur = b->f0;
+        }
+        if (b->graph && b->f_cur != b->graph_f) {
+            // the graph reads the load buffer it was captured with
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+            b->graph_tried = false;
+        }
+        CK(cudaEventRecord(b->ev[1], st));
+        const int passes = b->max_iter + 2;
+        if (!b->graph && !b->graph_tried && env_int("MAILLE_BATCH_GRAPH", 1)) {
+            b->graph_tried = true;
+            cudaGraph_t gph = nullptr;
+            const long long before = g_kernel_launches.load();
+            if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                bool ok = true;
+                try {
+                    enqueue_rhs(b);
+                    enqueue_pcg(b, passes);
+                    enqueue_gather(b);
+                } catch (const CudaFailure&) {
+                    ok = false;
+                }
+                const cudaError_t e = cudaStreamEndCapture(st, &gph);
+                if (ok && e == cudaSuccess && gph && cudaGraphInstantiate(&b->graph, gph, 0) == cudaSuccess) {
+                    b->graph_kernels = g_kernel_launches.load() - before;
+                    b->graph_f = b->f_cur;
+                } else {
+                    b->graph = nullptr;
+                }
+                if (gph) cudaGraphDestroy(gph);
+            }
+            g_kernel_launches.store(before);  // captured, not launched
+            cudaGetLastError();
+        }
+        if (b->graph) {
+            CK(cudaGraphLaunch(b->graph, st));
+            g_kernel_launches.fetch_add(b->graph_kernels);
+        } else {
+            enqueue_rhs(b);
+            enqueue_pcg(b, passes);
+            enqueue_gather(b);
+        }
+        CK(cudaEventRecord(b->ev[2], st));
+        const size_t ncol = (size_t)b->n_inst * b->R;
+        b->h_iter.resize(b->n_inst);
+        b->h_col_iter.resize(ncol);
+        b->h_status.resize(b->n_inst);
+        b->h_rr.resize(ncol);
+        b->h_bb.resize(ncol);
+        CK(cudaMemcpyAsync(b->h_ctrl.data(), b->state.ctrl, 8 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(b->h_iter.data(), b->state.iter, b->n_inst * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(b->h_col_iter.data(), b->state.col_iter, ncol * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(b->h_status.data(), b->state.status, b->n_inst * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(b->h_rr.data(), b->state.rr, ncol * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(b->h_bb.data(), b->state.bb, ncol * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (res && res->u) CK(cudaMemcpyAsync(res->u, b->u_out, nf * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(b->ev[3], st));
+        CK(cudaStreamSynchronize(st));
+        int32_t status = MAILLE_OK;
+        if (b->h_ctrl[2] != 0) {
+            set_last_error("batched PCG: a sweep wait timed out (status kept on the device)");
+            status = MAILLE_CUDA_ERROR;
+        } else if (b->h_ctrl[3] != 0) {
+            set_last_error("Cancelled");
+            status = MAILLE_CANCELLED;
+        }
+        int32_t max_it = 0;
+        for (int32_t i = 0; i < b->n_inst; ++i) {
+            max_it = std::max(max_it, b->h_iter[i]);
+            if (status == MAILLE_OK && b->h_status[i] != 0) {
+                status = b->h_status[i] == 1 ? MAILLE_SINGULAR : MAILLE_NOT_CONVERGED;
+                set_last_error("instance " + std::to_string(i) +
+                               (status == MAILLE_SINGULAR ? ": Singular (p.Ap <= 0 or NaN)"
+                                                          : ": IterativeNotConverged"));
+            }
+        }
+        if (status == MAILLE_OK && b->h_ctrl[0] != 0) {
+            set_last_error("batched PCG stopped with unfinished instances");
+            status = MAILLE_NOT_CONVERGED;
+        }
+        if (res) {
+            for (int32_t i = 0; i < b->n_inst; ++i) {
+                if (res->status) res->status[i] = b->h_status[i] == 1 ? MAILLE_SINGULAR
+                                                  : b->h_status[i] == 2 ? MAILLE_NOT_CONVERGED
+                                                                        : MAILLE_OK;
+                for (int32_t c = 0; c < b->n_rhs; ++c) {
+                    const size_t s = (size_t)i * b->R + c;
+                    const int32_t ci = b->h_col_iter[s];
+                    if (res->iterations) res->iterations[(size_t)i * b->n_rhs + c] = ci >= 0 ? ci : b->h_iter[i];
+                    if (res->rel_residual)
+                        res->rel_residual[(size_t)i * b->n_rhs + c] =
+                            b->h_bb[s] > 0 ? std::sqrt(b->h_rr[s] / b->h_bb[s]) : 0.0;
+                }
+            }
+            res->max_iterations = max_it;
+            res->levels = b->sym.levels;
+            res->free_dofs = b->sym.free_dofs;
+            res->block_rows = b->sym.nb;
+            res->blocks = b->sym.blocks;
+            res->rhs_per_lane = b->cfg.Q;
+            res->lanes_per_row = (b->R / b->cfg.Q) * b->cfg.SUB;
+            res->threads = b->cfg.threads;
+            res->task_slices = b->cfg.task;
+            res->autotuned = tuned ? 1 : 0;
+            res->ms_tune = ms_tune;
+            res->ms_solve = elapsed(b->ev[1], b->ev[2]);
+            res->ms_download = elapsed(b->ev[2], b->ev[3]);
+            res->ms_upload = elapsed(b->ev[0], b->ev[1]);
+        }
+        return status;
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+}
+
+int32_t refactor_batch(MailleGpuBatch* b, const double* young, const double* poisson) {
+    if (!b) return fail({MAILLE_INVALID_INPUT, "null batch"});
+    for (const double* a : {young, poisson})
+        if (a)
+            for (int64_t e = 0; e < b->n_elems; ++e)
+                if (!std::isfinite(a[e])) return fail({MAILLE_INVALID_INPUT, "non-finite material"});
+    if (young)
+        for (int64_t e = 0; e < b->n_elems; ++e)
+            if (young[e] <= 0) return fail({MAILLE_INVALID_INPUT, "invalid material of element " + std::to_string(e)});
+    if (poisson)
+        for (int64_t e = 0; e < b->n_elems; ++e)
+            if (poisson[e] <= -1.0 || poisson[e] >= 0.5)
+                return fail({MAILLE_INVALID_INPUT, "invalid material of element " + std::to_string(e)});
+    Error err{MAILLE_OK, ""};
+    try {
+        CK(cudaSetDevice(b->device));
+        if (young) CK(cudaMemcpyAsync(b->young, young, b->n_elems * sizeof(double), cudaMemcpyHostToDevice, b->st));
+        if (poisson)
+            CK(cudaMemcpyAsync(b->poisson, poisson, b->n_elems * sizeof(double), cudaMemcpyHostToDevice, b->st));
+        if (numeric(b, err) != MAILLE_OK) return fail(err);
+        if (b->cfg.valid()) fill_values(b);
+        CK(cudaStreamSynchronize(b->st));
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+    return MAILLE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t maille_gpu_batch_create(const MailleBatchProblem* problem, MailleGpuBatch** out) {
+    set_last_error("");
+    return create_batch(problem, out);
+}
+
+int32_t maille_gpu_batch_solve(MailleGpuBatch* b, const double* f, MailleBatchResult* result) {
+    set_last_error("");
+    return solve_batch(b, f, result);
+}
+
+int32_t maille_gpu_batch_refactor(MailleGpuBatch* b, const double* young, const double* poisson) {
+    set_last_error("");
+    return refactor_batch(b, young, poisson);
+}
+
+void maille_gpu_batch_cancel(MailleGpuBatch* b, int32_t flag) {
+    if (b && b->h_cancel) *(volatile int32_t*)b->h_cancel = flag ? 1 : 0;
+}
+
+void* maille_gpu_batch_stream(MailleGpuBatch* b) { return b ? (void*)b->st : nullptr; }
+
+void maille_gpu_batch_destroy(MailleGpuBatch* b) { delete b; }
+
+int32_t maille_gpu_batched_solve(const MailleBatchProblem* problem, MailleBatchResult* result) {
+    set_last_error("");
+    MailleGpuBatch* b = nullptr;
+    int32_t s = create_batch(problem, &b);
+    if (s != MAILLE_OK) return s;
+    s = solve_batch(b, nullptr, result);
+    if (result) {
+        // create's phases (its events are not reused by the solve)
+        result->ms_setup = b->sym.ms;
+        result->ms_upload += elapsed(b->ev[4], b->ev[5]);
+        result->ms_assembly = elapsed(b->ev[5], b->ev[6]);
+        result->ms_factor = elapsed(b->ev[6], b->ev[7]);
+    }
+    maille_gpu_batch_destroy(b);
+    return s;
+}
+
+}  // extern "C"

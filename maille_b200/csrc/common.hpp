@@ -75,6 +75,29 @@ struct SellHost {
 
 enum SellKind { SELL_FULL = 0, SELL_LOWER = 1, SELL_UPPER = 2 };
 
+// Sliced layout of the batched solver (block-diagonal system of many instances, several
+// right-hand sides). A slice holds `rows` rows of ONE instance (and, for L and U, of one level);
+// each row's blocks are spread over `sub` lanes of 4 slots per step, so a step holds
+// rows * sub * 4 slots: value plane k of step g at vals[(g * 9 + k) * slots + slot], columns at
+// col[g * slots + slot]. K slices are ordered instance-major; L and U slices level-major, and
+// inside a level instance by instance. Padding slots point at the dummy node nb.
+struct BSellHost {
+    int rows = 4, sub = 1;
+    int slots() const { return rows * sub * 4; }
+    std::vector<int32_t> rowid;         // [nslices * rows], -1 when empty
+    std::vector<int64_t> off{0};        // [nslices + 1] first step of each slice
+    std::vector<int32_t> col, src;      // [steps * slots]
+    std::vector<int32_t> inst;          // [nslices] instance of the slice
+    std::vector<int32_t> level_slices;  // [levels + 1] (L and U)
+    int64_t steps() const { return off.back(); }
+    int32_t nslices() const { return (int32_t)off.size() - 1; }
+};
+
+// Builds the batched layout of one part of the analysed pattern; group[row] is the row's
+// instance (rows of one instance must form one connected block of the matrix).
+void build_bsell(const Symbolic& s, SellKind kind, int rows, int sub, const std::vector<int32_t>& group,
+                 BSellHost& out);
+
 // Builds the sliced layout of one part of the analysed pattern. lpr <= 0 picks lanes per row
 // from the mean row length.
 void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out);

@@ -1,0 +1,54 @@
+// cuda_host.hpp -- host-side CUDA helpers shared by the handle and batch drivers: error
+// checking that throws to the C ABI boundary, device allocation and upload, a wall clock.
+#pragma once
+
+#include <chrono>
+#include <string>
+
+#include <cuda_runtime.h>
+
+namespace maille {
+
+struct CudaFailure {
+    std::string what;
+};
+
+#define CK(call)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            throw ::maille::CudaFailure{std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+inline double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+template <typename T>
+T* dalloc(size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    CK(cudaMalloc(&p, n * sizeof(T)));
+    return static_cast<T*>(p);
+}
+
+template <typename T>
+T* dupload(const T* src, size_t n, cudaStream_t st) {
+    T* d = dalloc<T>(n);
+    if (n && src) CK(cudaMemcpyAsync(d, src, n * sizeof(T), cudaMemcpyHostToDevice, st));
+    return d;
+}
+
+inline void dfree(void* p) {
+    if (p) cudaFree(p);
+}
+
+constexpr double kDefaultTol = 1e-12;      // iterative.rs:9
+constexpr int32_t kDefaultMaxIter = 10000;  // iterative.rs:11
+constexpr double kShifts[6] = {0.0, 1e-3, 1e-2, 1e-1, 1.0, 10.0};  // iterative.rs:14
+
+void set_last_error(const std::string& message);
+
+}  // namespace maille

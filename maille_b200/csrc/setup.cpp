@@ -432,6 +432,60 @@ void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out) {
     }
 }
 
+void build_bsell(const Symbolic& s, SellKind kind, int rows, int sub, const std::vector<int32_t>& group,
+                 BSellHost& out) {
+    out = BSellHost{};
+    out.rows = rows;
+    out.sub = sub;
+    const int slots = out.slots(), per_step = 4 * sub;
+    auto start = [&](int32_t i) { return kind == SELL_UPPER ? s.diag[i] + 1 : s.row_ptr[i]; };
+    auto end = [&](int32_t i) { return kind == SELL_LOWER ? s.diag[i] : s.row_ptr[i + 1]; };
+    auto emit = [&](std::vector<int32_t>& rs) {
+        // rows of one group: by decreasing length, `rows` per slice
+        std::stable_sort(rs.begin(), rs.end(), [&](int32_t a, int32_t b) {
+            return end(a) - start(a) > end(b) - start(b);
+        });
+        for (size_t c0 = 0; c0 < rs.size(); c0 += rows) {
+            const size_t c1 = std::min(rs.size(), c0 + rows);
+            int64_t maxlen = 0;
+            for (size_t k = c0; k < c1; ++k) maxlen = std::max<int64_t>(maxlen, end(rs[k]) - start(rs[k]));
+            const int64_t steps = (maxlen + per_step - 1) / per_step;
+            const int64_t g0 = out.off.back();
+            out.off.push_back(g0 + steps);
+            out.inst.push_back(group[rs[c0]]);
+            out.col.resize((size_t)(g0 + steps) * slots, s.nb);
+            out.src.resize((size_t)(g0 + steps) * slots, -1);
+            for (int r = 0; r < rows; ++r) out.rowid.push_back(c0 + r < c1 ? rs[c0 + r] : -1);
+            for (size_t k = c0; k < c1; ++k) {
+                const int32_t i = rs[k];
+                const int r = (int)(k - c0);
+                for (int64_t p = start(i), b = 0; p < end(i); ++p, ++b) {
+                    const int64_t t = b / per_step, rem = b % per_step;
+                    const size_t slot = (size_t)(g0 + t) * slots + 4 * (r * sub + rem / 4) + rem % 4;
+                    out.col[slot] = s.col[p];
+                    out.src[slot] = (int32_t)p;
+                }
+            }
+        }
+    };
+    // rows bucketed by group, keeping row order inside a group
+    const int32_t ngroups = group.empty() ? 0 : *std::max_element(group.begin(), group.end()) + 1;
+    std::vector<std::vector<int32_t>> bucket(ngroups);
+    if (kind == SELL_FULL) {
+        for (int32_t i = 0; i < s.nb; ++i) bucket[group[i]].push_back(i);
+        for (auto& b : bucket) emit(b);
+        return;
+    }
+    out.level_slices.push_back(0);
+    for (int32_t l = 0; l < s.levels; ++l) {
+        for (auto& b : bucket) b.clear();
+        for (int32_t i = s.level_ptr[l]; i < s.level_ptr[l + 1]; ++i) bucket[group[i]].push_back(i);
+        for (auto& b : bucket)
+            if (!b.empty()) emit(b);
+        out.level_slices.push_back(out.nslices());
+    }
+}
+
 // face_pressure for the tet faces (assembly.rs:650-674; face_rule tet branch 556-585; face nodes
 // from Element::face_positions, mesh.rs:184-198; TRIANGLE_3 / TRIANGLE_6 rules).
 bool face_pressure_loads(int64_t n_nodes, const double* coords, int npe, int64_t n_elems,

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include "common.hpp"
+#include "cuda_host.hpp"
 #include "kernels.cuh"
 #include "sparse.cuh"
 
@@ -33,42 +34,6 @@ using namespace maille;
 namespace {
 
 thread_local std::string g_last_error;
-
-double now_ms() {
-    return std::chrono::duration<double, std::milli>(
-               std::chrono::steady_clock::now().time_since_epoch())
-        .count();
-}
-
-struct CudaFailure {
-    std::string what;
-};
-
-#define CK(call)                                                                             \
-    do {                                                                                     \
-        cudaError_t e_ = (call);                                                             \
-        if (e_ != cudaSuccess)                                                               \
-            throw CudaFailure{std::string(#call) + ": " + cudaGetErrorString(e_)};           \
-    } while (0)
-
-template <typename T>
-T* dalloc(size_t n) {
-    void* p = nullptr;
-    if (n == 0) n = 1;
-    CK(cudaMalloc(&p, n * sizeof(T)));
-    return static_cast<T*>(p);
-}
-
-template <typename T>
-T* dupload(const T* src, size_t n, cudaStream_t st) {
-    T* d = dalloc<T>(n);
-    if (n && src) CK(cudaMemcpyAsync(d, src, n * sizeof(T), cudaMemcpyHostToDevice, st));
-    return d;
-}
-
-constexpr double kDefaultTol = 1e-12;      // iterative.rs:9
-constexpr int32_t kDefaultMaxIter = 10000;  // iterative.rs:11
-const double kShifts[6] = {0.0, 1e-3, 1e-2, 1e-1, 1.0, 10.0};  // iterative.rs:14
 
 }  // namespace
 
@@ -162,14 +127,6 @@ struct MailleGpuHandle {
     }
     ~MailleGpuHandle();
 };
-
-namespace {
-
-void dfree(void* p) {
-    if (p) cudaFree(p);
-}
-
-}  // namespace
 
 MailleGpuHandle::~MailleGpuHandle() {
     cudaSetDevice(device);

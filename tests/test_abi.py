@@ -46,12 +46,15 @@ def test_version_and_device_count_need_no_gpu(lib):
     assert lib.maille_gpu_device_count() >= 0
 
 
+STRUCTS = (("MailleElasticProblem", _lib.ElasticProblem), ("MailleElasticResult", _lib.ElasticResult),
+           ("MailleBatchProblem", _lib.BatchProblem), ("MailleBatchResult", _lib.BatchResult))
+
+
 def test_struct_layouts_match_the_header(tmp_path):
     """Field offsets of the ctypes structs equal those gcc computes from include/maille_gpu.h."""
     import subprocess
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "maille_gpu.h"', "int main(void) {"]
-    for cname, py in (("MailleElasticProblem", _lib.ElasticProblem),
-                      ("MailleElasticResult", _lib.ElasticResult)):
+    for cname, py in STRUCTS:
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
         for fname, _ in py._fields_:
             lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
@@ -62,8 +65,7 @@ def test_struct_layouts_match_the_header(tmp_path):
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
     got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
-    for cname, py in (("MailleElasticProblem", _lib.ElasticProblem),
-                      ("MailleElasticResult", _lib.ElasticResult)):
+    for cname, py in STRUCTS:
         assert got[(cname, "size")] == ctypes.sizeof(py)
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
