@@ -260,6 +260,64 @@ void* maille_gpu_batch_stream(MailleGpuBatch* b);
 
 void maille_gpu_batch_destroy(MailleGpuBatch* b);
 
+/* ---- Large strain: neo-Hookean Tet4, quasi-static Newton, adjoint ----------------------------
+ * Replaces, for a Tet4 model with Kinematics::Large and Hyperelasticity::NeoHookean on every
+ * element, Model::solve_quasi_static (model.rs:720-806) over Step::quasi_static(1, increments)
+ * with the linear amplitude (0,0)-(1,1): each increment is Newton-Raphson to F_int(u) = lambda F
+ * with imposed values lambda * imposed (equilibrium, model.rs:923-1022: relative residual
+ * ||r_free|| / scale <= newton_tol after at least two residuals, at most newton_max_iter, the
+ * increment halved up to 5 times when Newton fails, advance, model.rs:820-870), each linear step
+ * K_ff du_f = -r_f - K_fc du_c solved by this library's assembly + IC(0)-PCG. The element
+ * response is large_strain_response (finite_strain.rs:119-214) with the neo-Hookean law
+ * (finite_strain.rs:40-86), lambda and mu = lame(E, nu) per element (finite_strain.rs:30-35).
+ * Follower pressures, contacts and plasticity are not part of this path.
+ *
+ * backward (no counterpart in the reference): for J = sum_k dJdR[k] . R_k, R_k the reactions of
+ * increment k (F_int - lambda F at fixed DOFs), the reverse pass recomputes the tangent at each
+ * increment's checkpointed displacements, solves K_ff m_f = -K_fc g_c with the same PCG and
+ * accumulates dJ/dmu_e and dJ/dlambda_e = w_e . dF_int,e/dp_e, w = (g_c, m_f). */
+typedef struct {
+    int64_t n_nodes;
+    const double* coords;     /* [3 n_nodes] */
+    int64_t n_elems;
+    const int64_t* conn;      /* [n_elems * 4] Tet4 */
+    const double* young;      /* [n_elems] E per element (lambda, mu = lame(E, nu)) */
+    const double* poisson;    /* [n_elems] */
+    const uint8_t* fixed;     /* [3 n_nodes] */
+    const double* imposed;    /* [3 n_nodes] imposed values at the end of the step */
+    const double* f;          /* [3 n_nodes] external loads at the end of the step, or NULL */
+    int32_t increments;       /* equal increments of the step (> 0) */
+    double newton_tol;        /* <= 0 selects 1e-8 (model.rs:1220) */
+    int32_t newton_max_iter;  /* <= 0 selects 25 (model.rs:1222) */
+    double rel_tol;           /* PCG tolerance, <= 0 selects 1e-12 */
+    int32_t max_iter;         /* PCG iterations, <= 0 selects 10000 */
+    int32_t precision;        /* MaillePrecision of the PCG */
+    int32_t device;
+} MailleLargeStrainProblem;
+
+typedef struct {
+    double* u;                  /* [increments][3 n_nodes] converged displacements, or NULL */
+    double* reactions;          /* [increments][3 n_nodes] F_int - lambda F at fixed DOFs, or NULL */
+    int32_t* newton_iterations; /* [increments] residuals of the last equilibrium, or NULL */
+    int32_t* cuts;              /* [increments] interval halvings, or NULL */
+    int64_t newton_total;       /* filled: Newton iterations over the step */
+    int64_t pcg_total;          /* filled: PCG iterations over the step */
+    double ms_total;
+} MailleLargeStrainResult;
+
+typedef struct MailleGpuLargeStrain MailleGpuLargeStrain;
+
+int32_t maille_gpu_large_strain_create(const MailleLargeStrainProblem* problem, MailleGpuLargeStrain** out);
+/* Runs the whole step; the per-increment displacements stay on the device as checkpoints. */
+int32_t maille_gpu_large_strain_run(MailleGpuLargeStrain* s, MailleLargeStrainResult* result);
+/* dJdR [increments][3 n_nodes] (read at fixed DOFs) -> dJdmu [n_elems], dJdlambda [n_elems] or NULL */
+int32_t maille_gpu_large_strain_backward(MailleGpuLargeStrain* s, const double* dJdR, double* dJdmu,
+                                         double* dJdlambda);
+/* New per-element E and nu (NULL keeps them); the next run starts from rest. */
+int32_t maille_gpu_large_strain_set_materials(MailleGpuLargeStrain* s, const double* young,
+                                              const double* poisson);
+void maille_gpu_large_strain_destroy(MailleGpuLargeStrain* s);
+
 /* Largest n_block_rows that maille_gpu_bsr3_spmv_dot_noalloc accepts (2^26 block rows, i.e.
  * about 2e8 DOFs, inside the 32-bit column indices of the matrix). */
 #define MAILLE_NOALLOC_MAX_BLOCK_ROWS (INT64_C(1) << 26)

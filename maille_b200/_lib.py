@@ -75,6 +75,23 @@ class BatchResult(ctypes.Structure):
     ]
 
 
+class LargeStrainProblem(ctypes.Structure):
+    _fields_ = [
+        ("n_nodes", ctypes.c_int64), ("coords", _d), ("n_elems", ctypes.c_int64), ("conn", _i64),
+        ("young", _d), ("poisson", _d), ("fixed", _u8), ("imposed", _d), ("f", _d),
+        ("increments", ctypes.c_int32), ("newton_tol", ctypes.c_double),
+        ("newton_max_iter", ctypes.c_int32), ("rel_tol", ctypes.c_double),
+        ("max_iter", ctypes.c_int32), ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+    ]
+
+
+class LargeStrainResult(ctypes.Structure):
+    _fields_ = [
+        ("u", _d), ("reactions", _d), ("newton_iterations", _i32), ("cuts", _i32),
+        ("newton_total", ctypes.c_int64), ("pcg_total", ctypes.c_int64), ("ms_total", ctypes.c_double),
+    ]
+
+
 # every symbol include/maille_gpu.h declares, with its ctypes signature
 SIGNATURES = {
     "maille_gpu_last_error": ([], ctypes.c_char_p),
@@ -108,6 +125,12 @@ SIGNATURES = {
     "maille_gpu_batch_cancel": ([ctypes.c_void_p, ctypes.c_int32], None),
     "maille_gpu_batch_stream": ([ctypes.c_void_p], ctypes.c_void_p),
     "maille_gpu_batch_destroy": ([ctypes.c_void_p], None),
+    "maille_gpu_large_strain_create": ([ctypes.POINTER(LargeStrainProblem), ctypes.POINTER(ctypes.c_void_p)],
+                                       ctypes.c_int32),
+    "maille_gpu_large_strain_run": ([ctypes.c_void_p, ctypes.POINTER(LargeStrainResult)], ctypes.c_int32),
+    "maille_gpu_large_strain_backward": ([ctypes.c_void_p, _d, _d, _d], ctypes.c_int32),
+    "maille_gpu_large_strain_set_materials": ([ctypes.c_void_p, _d, _d], ctypes.c_int32),
+    "maille_gpu_large_strain_destroy": ([ctypes.c_void_p], None),
 }
 
 _lib = None

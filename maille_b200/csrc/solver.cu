@@ -26,6 +26,7 @@
 
 #include "common.hpp"
 #include "cuda_host.hpp"
+#include "handle.hpp"
 #include "kernels.cuh"
 #include "sparse.cuh"
 
@@ -36,97 +37,6 @@ namespace {
 thread_local std::string g_last_error;
 
 }  // namespace
-
-// A sliced layout: host description (level slices) plus its device index arrays.
-struct SellBuf {
-    SellHost h;
-    int32_t* rowid = nullptr;
-    int64_t* off = nullptr;
-    int32_t* col = nullptr;
-    int32_t* src = nullptr;
-    SellDev dev() const { return SellDev{h.lpr, h.nslices(), rowid, off, col}; }
-    void upload(cudaStream_t st) {
-        rowid = dupload(h.rowid.data(), h.rowid.size(), st);
-        off = dupload(h.off.data(), h.off.size(), st);
-        col = dupload(h.col.data(), h.col.size(), st);
-        src = dupload(h.src.data(), h.src.size(), st);
-    }
-    void release() {
-        for (void* p : {(void*)rowid, (void*)off, (void*)col, (void*)src})
-            if (p) cudaFree(p);
-        rowid = nullptr;
-        off = nullptr;
-        col = nullptr;
-        src = nullptr;
-    }
-};
-
-struct MailleGpuHandle {
-    int device = 0;
-    cudaStream_t st = nullptr;
-    cudaEvent_t ev[8] = {};
-    Symbolic sym;
-    int npe = 0;
-    int64_t n_nodes = 0, n_elems = 0;
-    int precision = MAILLE_FP64;
-    double tol = kDefaultTol;
-    int32_t max_iter = kDefaultMaxIter;
-    double delta = 0.1;  // reliable update when the FP32 residual fell by this factor
-    std::vector<uint8_t> h_fixed;
-    std::vector<double> h_f, h_f0, h_imposed;
-    bool any_imposed = false;
-    // device: inputs (caller numbering)
-    double *coords = nullptr, *young = nullptr, *poisson = nullptr, *imposed = nullptr, *f = nullptr,
-           *f0 = nullptr;  // f: loads of the current solve, f0: the problem's loads
-    const double* f_cur = nullptr;
-    int32_t* conn = nullptr;
-    uint8_t* fixed = nullptr;
-    // device: symbolic
-    int32_t *perm = nullptr, *inv = nullptr, *col = nullptr, *lrow = nullptr;
-    uint8_t* fixmask = nullptr;
-    int64_t *row_ptr = nullptr, *diag = nullptr, *tpos = nullptr, *lslot = nullptr, *lptr = nullptr;
-    uint32_t* contrib = nullptr;
-    int64_t* inc_ptr = nullptr;
-    int32_t *inc = nullptr, *belem = nullptr, *bnodes = nullptr, *elem_slot = nullptr;
-    // device: numeric (CSR K and factor F; sliced copies for the iterations)
-    double* ke = nullptr;
-    double *K = nullptr, *F = nullptr;
-    SellBuf sk, sl, su;
-    double *Ks64 = nullptr, *Ls64 = nullptr, *Us64 = nullptr, *D64 = nullptr;
-    float *Ks32 = nullptr, *Ls32 = nullptr, *Us32 = nullptr, *D32 = nullptr;
-    // padded solver vectors (4 entries per block row)
-    double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr, *z64 = nullptr, *p64 = nullptr,
-           *ap64 = nullptr;
-    float *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *ap32 = nullptr;
-    double *u_full = nullptr, *y_full = nullptr, *ye = nullptr, *gauss = nullptr, *vm = nullptr,
-           *react = nullptr, *lambda_full = nullptr, *grad = nullptr;
-    PcgScalars* scal = nullptr;
-    PcgScalars* h_scal = nullptr;  // pinned
-    double* partials = nullptr;
-    double* lvl_total = nullptr;
-    double* dsum = nullptr;        // [4] misc sums
-    double* h_sum = nullptr;       // pinned [4]
-    unsigned int* dticket = nullptr;
-    int32_t* dfail = nullptr;
-    int spmv_grid = 1;
-    cudaGraphExec_t graph = nullptr;  // PCG iterations of the handle's form (per-level launches)
-    int persist_grid = 0;             // > 0: the persistent cooperative kernel runs the PCG
-    int persist_chunk = 64;           // iterations per persistent launch
-    int32_t *lvl_l = nullptr, *lvl_u = nullptr;
-    unsigned long long* timing = nullptr;  // per-phase ns when MAILLE_PHASE_TIMING is set
-    int32_t* claim = nullptr;              // dataflow sweeps: claim counters [2] + timeout flag
-    unsigned int* flags = nullptr;         // row-ready flags [nb + 1] (the dummy's is always set)
-    int32_t* bwd_seq = nullptr;            // U slices by level, descending
-    int graph_iters = 8;
-    long long graph_kernels = 0;
-    std::atomic<int> cancel{0};
-    double shift = 0.0;
-    bool solved = false;
-    Pattern pattern() const {
-        return Pattern{sym.nb, row_ptr, col, diag, tpos, fixmask};
-    }
-    ~MailleGpuHandle();
-};
 
 MailleGpuHandle::~MailleGpuHandle() {
     cudaSetDevice(device);
@@ -431,11 +341,17 @@ int32_t factorize(MailleGpuHandle* h, Error& err) {
 
 // Element integration + scatter-reduce assembly + IC(0), then the sliced copies the
 // iterations read (FP64 for the plain form; FP32 K, L, L^T, D and the FP64 K for the mixed one).
+int32_t assemble_factor(MailleGpuHandle* h, Error& err);
+
 int32_t numeric_phase(MailleGpuHandle* h, Error& err) {
+    ElemIn in{h->n_elems, h->coords, h->conn, h->young, h->poisson};
+    launch_elem_stiffness(h->npe, in, h->ke, h->st);
+    return assemble_factor(h, err);
+}
+
+int32_t assemble_factor(MailleGpuHandle* h, Error& err) {
     const Symbolic& s = h->sym;
     cudaStream_t st = h->st;
-    ElemIn in{h->n_elems, h->coords, h->conn, h->young, h->poisson};
-    launch_elem_stiffness(h->npe, in, h->ke, st);
     launch_assemble(h->pattern(), (int64_t)s.lslot.size(), h->lslot, h->lrow, h->lptr, h->contrib,
                     h->ke, h->K, st);
     launch_sell_fill<double>(h->sk.h.steps(), h->sk.src, h->K, h->Ks64, st);
@@ -785,6 +701,17 @@ int32_t backward_impl(MailleGpuHandle* h, const double* dJdu, double* dJdE, doub
 
 namespace maille {
 void set_last_error(const std::string& message) { g_last_error = message; }
+int32_t handle_create(const MailleElasticProblem* p, MailleGpuHandle** out, MailleElasticResult* res) {
+    return create_impl(p, out, res);
+}
+int32_t handle_assemble_factor(MailleGpuHandle* h, Error& err) { return assemble_factor(h, err); }
+void handle_build_rhs(MailleGpuHandle* h) { build_rhs(h); }
+int32_t handle_run_pcg(MailleGpuHandle* h, int32_t* iterations, int32_t* updates, double* rel_res) {
+    return run_pcg(h, iterations, updates, rel_res);
+}
+const char* handle_status_message(int32_t status, int32_t iters, double rel) {
+    return status_message(status, iters, rel);
+}
 }  // namespace maille
 
 // ---- C ABI -------------------------------------------------------------------------------------

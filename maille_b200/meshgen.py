@@ -234,6 +234,33 @@ def batched_tet4(count: int = 256, lo: int = 6, hi: int = 24, load_cases: int = 
     return problems, rhs
 
 
+def large_strain_block(cells=(64, 16, 16), size=(4.0, 1.0, 1.0), tip: float = -0.4,
+                       lam: float = 120000.0, mu_range=(60000.0, 100000.0)):
+    """Large-strain neo-Hookean Tet4 block (size mm, cells x 6 tets): mu_e uniform in mu_range
+    (seeded), lambda fixed, converted per element to E = mu (3 lambda + 2 mu) / (lambda + mu) and
+    nu = lambda / (2 (lambda + mu)) (Material takes E and nu; lame() gives mu and lambda back).
+    The x = 0 face is clamped; every node of the x = size_x face has its z displacement imposed
+    to `tip` (reached at the end of the ramp). Returns (Problem, mu, tip z-DOFs)."""
+    nodes, tets = box_grid(cells, size)
+    n_el = tets.shape[0]
+    mu = mu_range[0] + (mu_range[1] - mu_range[0]) * uniform(stream=6, count=n_el)
+    young = mu * (3.0 * lam + 2.0 * mu) / (lam + mu)
+    poisson = lam / (2.0 * (lam + mu))
+    n = nodes.shape[0]
+    fixed = np.zeros(3 * n, np.uint8)
+    imposed = np.zeros(3 * n)
+    root = np.nonzero(np.abs(nodes[:, 0]) < 1e-12)[0]
+    for c in range(3):
+        fixed[3 * root + c] = 1
+    end = np.nonzero(np.abs(nodes[:, 0] - size[0]) < 1e-12)[0]
+    fixed[3 * end + 2] = 1
+    imposed[3 * end + 2] = tip
+    prob = Problem(coords=nodes, conn=tets, young=young, poisson=poisson, fixed=fixed,
+                   imposed=imposed, loads=np.zeros(3 * n),
+                   name=f"neo_hookean_tet4_{cells[0]}x{cells[1]}x{cells[2]}")
+    return prob, mu, 3 * end + 2
+
+
 def traction_loads(prob: Problem, axis: int, value: float, traction: np.ndarray) -> np.ndarray:
     """Nodal loads of constant tractions t (L, 3) on the mesh faces lying on x[axis] = value:
     f_a = t * integral of N_a over the face (linear faces: area / 3 per vertex). Returns (3N, L)."""

@@ -64,6 +64,16 @@ def lib():
         L.oracle_element_bilinear.argtypes = [ctypes.c_int64, _d, ctypes.c_int, ctypes.c_int64, _i64,
                                                _d, _d, _d, _d, _d]
         L.oracle_element_bilinear.restype = None
+        L.oracle_large_strain_run.argtypes = [ctypes.c_int64, _d, ctypes.c_int64, _i64, _d, _d, _u8, _d, _d,
+                                              ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                              ctypes.c_int64, _d, _d, _i32, _i32, _d]
+        L.oracle_large_strain_run.restype = ctypes.c_int
+        L.oracle_large_strain_gradient.argtypes = [ctypes.c_int64, _d, ctypes.c_int64, _i64, _d, _d, _u8,
+                                                   ctypes.c_int, _d, _d, ctypes.c_double, ctypes.c_int64,
+                                                   _d, _d]
+        L.oracle_large_strain_gradient.restype = ctypes.c_int
+        L.oracle_neo_hookean_tet4.argtypes = [_d, ctypes.c_double, ctypes.c_double, _d, _d, _d, _d, _d]
+        L.oracle_neo_hookean_tet4.restype = ctypes.c_int
         L.oracle_nodal_stresses.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int64, _i64, _d, _d]
         _lib = L
     return _lib
@@ -227,6 +237,52 @@ def adjoint_gradient(prob, u, dJdu, tol: float = 1e-13, max_iter: int = 100000):
     lam = res["u"]
     grad = -element_bilinear(prob, lam, u) / np.asarray(prob.young, np.float64)
     return grad, lam, res
+
+
+def neo_hookean_tet4(coords, lam, mu, ue):
+    """One neo-Hookean Tet4 response: (status, fe [12], ke [12, 12], dfe/dmu, dfe/dlambda)."""
+    fe, ke, dm, dl = np.zeros(12), np.zeros((12, 12)), np.zeros(12), np.zeros(12)
+    s = lib().oracle_neo_hookean_tet4(_p(_c(coords, np.float64), _d), lam, mu, _p(_c(ue, np.float64), _d),
+                                      _p(fe, _d), _p(ke, _d), _p(dm, _d), _p(dl, _d))
+    return s, fe, ke, dm, dl
+
+
+def large_strain_run(prob, increments: int = 10, newton_tol: float = 1e-8, newton_max: int = 25,
+                     pcg_tol: float = 1e-12, pcg_max: int = 10000):
+    """Model::solve_quasi_static of a neo-Hookean Tet4 Problem (Kinematics::Large, linear ramp of
+    the loads and imposed values over `increments` equal increments). Returns a dict: status,
+    u_hist (increments, 3N) checkpoints, reactions (increments, 3N), newton (increments,), cuts,
+    newton_total, pcg_total, wall_s."""
+    coords = _c(prob.coords, np.float64)
+    conn = _c(prob.conn, np.int64)
+    n = coords.size
+    uh = np.zeros((increments, n))
+    rh = np.zeros((increments, n))
+    it = np.zeros(increments, np.int32)
+    cuts = np.zeros(increments, np.int32)
+    info = np.zeros(2)
+    t0 = time.perf_counter()
+    s = lib().oracle_large_strain_run(
+        coords.shape[0], _p(coords, _d), conn.shape[0], _p(conn, _i64), _p(_c(prob.young, np.float64), _d),
+        _p(_c(prob.poisson, np.float64), _d), _p(_c(prob.fixed, np.uint8), _u8),
+        _p(_c(prob.imposed, np.float64), _d), _p(_c(prob.loads, np.float64), _d), increments, newton_tol,
+        newton_max, pcg_tol, pcg_max, _p(uh, _d), _p(rh, _d), _p(it, _i32), _p(cuts, _i32), _p(info, _d))
+    return dict(status=s, u_hist=uh, reactions=rh, newton=it, cuts=cuts, newton_total=int(info[0]),
+                pcg_total=int(info[1]), wall_s=time.perf_counter() - t0)
+
+
+def large_strain_gradient(prob, u_hist, dJdR, pcg_tol: float = 1e-12, pcg_max: int = 10000):
+    """dJ/dmu_e and dJ/dlambda_e of J = sum_k dJdR[k] . R_k over the checkpoints u_hist."""
+    coords = _c(prob.coords, np.float64)
+    conn = _c(prob.conn, np.int64)
+    gm = np.zeros(conn.shape[0])
+    gl = np.zeros(conn.shape[0])
+    uh = _c(u_hist, np.float64)
+    s = lib().oracle_large_strain_gradient(
+        coords.shape[0], _p(coords, _d), conn.shape[0], _p(conn, _i64), _p(_c(prob.young, np.float64), _d),
+        _p(_c(prob.poisson, np.float64), _d), _p(_c(prob.fixed, np.uint8), _u8), uh.shape[0], _p(uh, _d),
+        _p(_c(dJdR, np.float64), _d), pcg_tol, pcg_max, _p(gm, _d), _p(gl, _d))
+    return s, gm, gl
 
 
 def nodal_stresses(prob, gauss):

@@ -692,6 +692,296 @@ struct SolidMesh {
     }
 };
 
+// --- large strain: src/finite_strain.rs, model.rs:720-1022 -------------------------------------
+
+// lame, finite_strain.rs:30-35
+void lame(double young, double nu, double& lambda, double& mu) {
+    lambda = young * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    mu = young / (2.0 * (1.0 + nu));
+}
+
+// mul / transpose / det / inverse, finite_strain.rs:89-117 (sums are left folds)
+void mul3(const double a[3][3], const double b[3][3], double o[3][3]) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s = a[i][0] * b[0][j];
+            s = s + a[i][1] * b[1][j];
+            s = s + a[i][2] * b[2][j];
+            o[i][j] = s;
+        }
+}
+double det3(const double a[3][3]) {
+    return a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) - a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+           a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+}
+void inv3(const double a[3][3], double o[3][3]) {
+    const double d = det3(a);
+    auto cof = [&](int i, int j) {
+        const int r0 = (i + 1) % 3, r1 = (i + 2) % 3, c0 = (j + 1) % 3, c1 = (j + 2) % 3;
+        return a[r0][c0] * a[r1][c1] - a[r0][c1] * a[r1][c0];
+    };
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) o[i][j] = cof(j, i) / d;
+}
+
+// large_strain_response (finite_strain.rs:119-214) with LargeStrainLaw::NeoHookean
+// (finite_strain.rs:40-86) on a Tet4 (solid_gauss with TETRA_1, element.rs:338-357): internal
+// force fe [12], tangent ke [12 x 12] row-major, and the derivatives of fe with respect to mu and
+// lambda at fixed u (dS/dmu = I - C^-1, dS/dlambda = ln J C^-1 from the same law; the reference
+// has no gradients). Returns false when J <= 0 makes the law non-finite.
+bool neo_hookean_tet4(const double c[4][3], double lambda, double mu, const double* ue, double* fe, double* ke,
+                      double* dfe_dmu, double* dfe_dlambda) {
+    double n[10], dn[10][3], dn_dx[10][3];
+    const TetGP& gp = TETRA_1[0];
+    tet_shape(4, gp.xi, gp.eta, gp.zeta, n, dn);
+    const double weight = gp.w * std::fabs(mapping3d(4, c, dn, dn_dx));
+    double f[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int a = 0; a < 4; ++a)
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) f[i][j] += ue[3 * a + i] * dn_dx[a][j];
+    double ft[3][3], cc[3][3], inv[3][3], s[3][3], pk1[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) ft[i][j] = f[j][i];
+    mul3(ft, f, cc);
+    const double log_j = std::log(det3(f));
+    inv3(cc, inv);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) s[i][j] = mu * ((i == j ? 1.0 : 0.0) - inv[i][j]) + lambda * log_j * inv[i][j];
+    mul3(f, s, pk1);
+    static thread_local double mod[3][3][3][3], A[3][3][3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k)
+                for (int l = 0; l < 3; ++l)
+                    mod[i][j][k][l] = lambda * inv[i][j] * inv[k][l] +
+                                      (mu - lambda * log_j) * (inv[i][k] * inv[j][l] + inv[i][l] * inv[j][k]);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k)
+                for (int l = 0; l < 3; ++l) {
+                    double material = 0.0;
+                    for (int ii = 0; ii < 3; ++ii)
+                        for (int kk = 0; kk < 3; ++kk) material += f[i][ii] * mod[ii][j][kk][l] * f[k][kk];
+                    const double geometric = i == k ? s[j][l] : 0.0;
+                    A[i][j][k][l] = geometric + material;
+                }
+    std::fill(fe, fe + 12, 0.0);
+    std::fill(ke, ke + 144, 0.0);
+    for (int na = 0; na < 4; ++na) {
+        const double* ga = dn_dx[na];
+        for (int i = 0; i < 3; ++i) {
+            const int row = 3 * na + i;
+            double fr = pk1[i][0] * ga[0];
+            fr = fr + pk1[i][1] * ga[1];
+            fr = fr + pk1[i][2] * ga[2];
+            fe[row] += weight * fr;
+            for (int nb = 0; nb < 4; ++nb) {
+                const double* gb = dn_dx[nb];
+                for (int k = 0; k < 3; ++k) {
+                    double v = 0.0;
+                    for (int j = 0; j < 3; ++j)
+                        for (int l = 0; l < 3; ++l) v += ga[j] * A[i][j][k][l] * gb[l];
+                    ke[row * 12 + 3 * nb + k] += weight * v;
+                }
+            }
+        }
+    }
+    if (dfe_dmu || dfe_dlambda) {
+        double ds_mu[3][3], ds_la[3][3], dp_mu[3][3], dp_la[3][3];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                ds_mu[i][j] = (i == j ? 1.0 : 0.0) - inv[i][j];
+                ds_la[i][j] = log_j * inv[i][j];
+            }
+        mul3(f, ds_mu, dp_mu);
+        mul3(f, ds_la, dp_la);
+        for (int na = 0; na < 4; ++na)
+            for (int i = 0; i < 3; ++i) {
+                const double* ga = dn_dx[na];
+                if (dfe_dmu) dfe_dmu[3 * na + i] = weight * (dp_mu[i][0] * ga[0] + dp_mu[i][1] * ga[1] + dp_mu[i][2] * ga[2]);
+                if (dfe_dlambda)
+                    dfe_dlambda[3 * na + i] = weight * (dp_la[i][0] * ga[0] + dp_la[i][1] * ga[1] + dp_la[i][2] * ga[2]);
+            }
+    }
+    return std::isfinite(log_j);
+}
+
+// The topology part of FreeSystem::new (model.rs:1449-1466): free numbering, RCM rank and the
+// lower CSR profile. The reference rebuilds it at every Newton iteration (model.rs:1011) from
+// the same pattern; it is built once here, with the same result.
+struct FreeTopology {
+    IVec free, rank;
+    size_t count = 0;
+    Csr pattern;
+};
+
+FreeTopology free_topology(size_t n_elems, const int64_t* conn, const uint8_t* fixed, size_t n) {
+    FreeTopology t;
+    t.free.assign(n, NONE);
+    for (size_t g = 0; g < n; ++g)
+        if (!fixed[g]) t.free[g] = t.count++;
+    IVec eoff(n_elems + 1, 0), eidx;
+    for (size_t e = 0; e < n_elems; ++e) {
+        for (int l = 0; l < 12; ++l) {
+            const size_t g = 3 * (size_t)conn[e * 4 + l / 3] + l % 3;
+            if (t.free[g] != NONE) eidx.push_back(t.free[g]);
+        }
+        eoff[e + 1] = eidx.size();
+    }
+    Graph graph = graph_from_elements(t.count, eoff, eidx);
+    IVec order = reverse_cuthill_mckee(graph);
+    t.rank.assign(t.count, 0);
+    for (size_t r = 0; r < t.count; ++r) t.rank[order[r]] = r;
+    t.pattern = Csr::zeros(graph, order, t.rank);
+    return t;
+}
+
+struct LargeStrainMesh {
+    size_t n_nodes, n_elems;
+    const double* coords;
+    const int64_t* conn;
+    Vec lambda, mu;  // per element, from lame(E, nu) as large_strain_law does (assembly.rs:55-61)
+    void coords_of(size_t e, double c[4][3]) const {
+        for (int a = 0; a < 4; ++a)
+            for (int k = 0; k < 3; ++k) c[a][k] = coords[3 * conn[e * 4 + a] + k];
+    }
+};
+
+// FreeSystem::new (values) + FreeSystem::solve (model.rs:1442-1516) with the iterative factor:
+// K_ff x_f = f_f - K_fc u_c, written into u at free DOFs. `tangents` holds 144 values per element.
+int free_solve(const FreeTopology& t, const LargeStrainMesh& m, const Vec& tangents, const Vec& f, Vec& u,
+               double pcg_tol, size_t pcg_max, size_t& pcg_iters) {
+    Csr k = t.pattern;
+    std::fill(k.values.begin(), k.values.end(), 0.0);
+    Vec coupling(t.count, 0.0);
+    for (size_t e = 0; e < m.n_elems; ++e) {
+        const double* ke = &tangents[e * 144];
+        for (int r = 0; r < 12; ++r) {
+            const size_t gi = 3 * (size_t)m.conn[e * 4 + r / 3] + r % 3;
+            const size_t a = t.free[gi];
+            if (a == NONE) continue;
+            for (int c = 0; c < 12; ++c) {
+                const size_t gj = 3 * (size_t)m.conn[e * 4 + c / 3] + c % 3;
+                const size_t b = t.free[gj];
+                if (b != NONE) {
+                    if (t.rank[b] <= t.rank[a]) k.add(t.rank[a], t.rank[b], ke[r * 12 + c]);
+                } else {
+                    coupling[t.rank[a]] += ke[r * 12 + c] * u[gj];
+                }
+            }
+        }
+    }
+    Vec rhs(t.count);
+    for (size_t q = 0; q < t.count; ++q) rhs[q] = -coupling[q];
+    for (size_t g = 0; g < t.free.size(); ++g)
+        if (t.free[g] != NONE) rhs[t.rank[t.free[g]]] += f[g];
+    Vec x;
+    SolveStats st;
+    const int status = pcg_solve(k, rhs, pcg_tol, pcg_max, x, st);
+    pcg_iters += st.iterations;
+    if (status != OK) return status;
+    for (size_t g = 0; g < t.free.size(); ++g)
+        if (t.free[g] != NONE) u[g] = x[t.rank[t.free[g]]];
+    return OK;
+}
+
+// Element responses at u: internal force (internal_force, model.rs:1241-1249) and tangents.
+bool responses(const LargeStrainMesh& m, const Vec& u, Vec& internal, Vec& tangents) {
+    internal.assign(3 * m.n_nodes, 0.0);
+    tangents.resize(m.n_elems * 144);
+    bool finite = true;
+    for (size_t e = 0; e < m.n_elems; ++e) {
+        double c[4][3], ue[12], fe[12];
+        m.coords_of(e, c);
+        for (int l = 0; l < 12; ++l) ue[l] = u[3 * (size_t)m.conn[e * 4 + l / 3] + l % 3];
+        finite = neo_hookean_tet4(c, m.lambda[e], m.mu[e], ue, fe, &tangents[e * 144], nullptr, nullptr) && finite;
+        for (int l = 0; l < 12; ++l) internal[3 * (size_t)m.conn[e * 4 + l / 3] + l % 3] += fe[l];
+    }
+    return finite;
+}
+
+constexpr double NEWTON_TOLERANCE = 1e-8;  // model.rs:1220
+constexpr size_t NEWTON_ITERATIONS = 25;   // model.rs:1222
+constexpr int MAX_CUTS = 5;                // model.rs:1224
+
+struct QuasiStatic {
+    const LargeStrainMesh& m;
+    const FreeTopology& t;
+    const uint8_t* fixed;
+    const double* imposed;
+    const double* loads;
+    double newton_tol, pcg_tol;
+    size_t newton_max, pcg_max;
+    size_t pcg_iters = 0, newton_total = 0;
+    Vec u;
+    double scale = 0.0;
+
+    // equilibrium, model.rs:923-1022 (no contacts, no follower pressures): Newton-Raphson to
+    // F_int(u) = lambda F with imposed values lambda * imposed. Returns the status; on success
+    // `reactions` = F_int - lambda F at fixed DOFs and `iterations` = residuals computed.
+    int equilibrium(Vec& uu, double lam, double& sc, Vec& reactions, size_t& iterations) {
+        const size_t n = uu.size();
+        Vec internal, tangents, residual(n), external(n);
+        size_t count = 0;
+        for (;;) {
+            responses(m, uu, internal, tangents);
+            for (size_t g = 0; g < n; ++g) {
+                external[g] = lam * (loads ? loads[g] : 0.0);
+                residual[g] = internal[g] - external[g];
+            }
+            double ni = 0.0, ne = 0.0, nf = 0.0;
+            for (size_t g = 0; g < n; ++g) {
+                ni += internal[g] * internal[g];
+                ne += external[g] * external[g];
+                if (!fixed[g]) nf += residual[g] * residual[g];
+            }
+            sc = std::max(std::max(sc, std::sqrt(ni)), std::sqrt(ne));
+            const double free = std::sqrt(nf);
+            const double relative = sc > 0.0 ? free / sc : free;
+            if (!std::isfinite(relative)) return NOT_CONVERGED;
+            ++count;
+            ++newton_total;
+            if (count > 1 && relative <= newton_tol) {
+                reactions.assign(n, 0.0);
+                for (size_t g = 0; g < n; ++g)
+                    if (fixed[g]) reactions[g] = residual[g];
+                iterations = count;
+                return OK;
+            }
+            if (count > newton_max) return NOT_CONVERGED;
+            Vec du(n, 0.0), minus(n);
+            for (size_t g = 0; g < n; ++g) {
+                if (fixed[g]) du[g] = lam * imposed[g] - uu[g];
+                minus[g] = -residual[g];
+            }
+            const int st = free_solve(t, m, tangents, minus, du, pcg_tol, pcg_max, pcg_iters);
+            if (st != OK) return st;
+            for (size_t g = 0; g < n; ++g) uu[g] += du[g];
+        }
+    }
+
+    // advance, model.rs:820-870: Newton from the committed state, halving the interval up to
+    // MAX_CUTS times when Newton fails or meets a non-positive-definite tangent.
+    int advance(double t0, double t1, int cuts, Vec& reactions, size_t& iterations, int& cut_count) {
+        Vec trial = u;
+        double sc = scale;
+        const int st = equilibrium(trial, t1, sc, reactions, iterations);  // amplitude lambda(t) = t
+        if (st == OK) {
+            u = trial;
+            scale = sc;
+            return OK;
+        }
+        if ((st == NOT_CONVERGED || st == SINGULAR) && cuts < MAX_CUTS) {
+            const double middle = (t0 + t1) / 2.0;
+            ++cut_count;
+            const int a = advance(t0, middle, cuts + 1, reactions, iterations, cut_count);
+            if (a != OK) return a;
+            return advance(middle, t1, cuts + 1, reactions, iterations, cut_count);
+        }
+        return st;
+    }
+};
+
 }  // namespace
 
 // ============================================================================================
@@ -1041,6 +1331,106 @@ void oracle_nodal_stresses(int64_t n_nodes, int npe, int64_t n_elems, const int6
     for (int64_t k = 0; k < n_nodes; ++k)
         for (int c = 0; c < 6; ++c)
             out[k * 6 + c] = sum[k * 6 + c] / (double)std::max<size_t>(count[k], 1);
+}
+
+
+// Model::solve_quasi_static (model.rs:720-806) of a neo-Hookean Tet4 model in large strain
+// (Kinematics::Large, Step::quasi_static(1, increments), linear amplitude (0,0)-(1,1), loads and
+// imposed values scaled by lambda(t) = t), with IC(0)-PCG inner solves to pcg_tol. Per increment:
+// the converged displacements (the checkpoints, [increments][3 n_nodes]), the reactions
+// F_int - lambda F at fixed DOFs ([increments][3 n_nodes]), the Newton iterations of the last
+// equilibrium and the cuts. info: [0] total Newton iterations, [1] total PCG iterations.
+int oracle_large_strain_run(int64_t n_nodes, const double* coords, int64_t n_elems, const int64_t* conn,
+                            const double* young, const double* poisson, const uint8_t* fixed,
+                            const double* imposed, const double* loads, int increments, double newton_tol,
+                            int newton_max, double pcg_tol, int64_t pcg_max, double* u_hist, double* r_hist,
+                            int32_t* newton_iters, int32_t* cuts, double* info) {
+    LargeStrainMesh m{(size_t)n_nodes, (size_t)n_elems, coords, conn, {}, {}};
+    m.lambda.resize(m.n_elems);
+    m.mu.resize(m.n_elems);
+    for (size_t e = 0; e < m.n_elems; ++e) lame(young[e], poisson[e], m.lambda[e], m.mu[e]);
+    const size_t n = 3 * (size_t)n_nodes;
+    FreeTopology t = free_topology(m.n_elems, conn, fixed, n);
+    QuasiStatic qs{m, t, fixed, imposed, loads, newton_tol > 0 ? newton_tol : NEWTON_TOLERANCE,
+                   pcg_tol > 0 ? pcg_tol : TOLERANCE, newton_max > 0 ? (size_t)newton_max : NEWTON_ITERATIONS,
+                   pcg_max > 0 ? (size_t)pcg_max : MAX_ITERATIONS, 0, 0, Vec(n, 0.0), 0.0};
+    const double dt = 1.0 / increments;
+    for (int inc = 1; inc <= increments; ++inc) {
+        const double time = inc * dt;
+        Vec reactions;
+        size_t iterations = 0;
+        int cut_count = 0;
+        const int st = qs.advance(time - dt, time, 0, reactions, iterations, cut_count);
+        if (st != OK) return st;
+        std::copy(qs.u.begin(), qs.u.end(), u_hist + (size_t)(inc - 1) * n);
+        std::copy(reactions.begin(), reactions.end(), r_hist + (size_t)(inc - 1) * n);
+        newton_iters[inc - 1] = (int32_t)iterations;
+        cuts[inc - 1] = cut_count;
+    }
+    if (info) {
+        info[0] = (double)qs.newton_total;
+        info[1] = (double)qs.pcg_iters;
+    }
+    return OK;
+}
+
+// Adjoint of increment reactions: for J = sum_k dJdR[k] . R_k (R_k the reactions of increment k,
+// weights read at fixed DOFs), dJ/dmu_e and dJ/dlambda_e (per element Lame parameters of the
+// neo-Hookean law). Reverse pass over the checkpoints u_hist: at each increment with a nonzero
+// weight g the tangent at u_k is recomputed, K_ff m_f = -K_fc g_c is solved with the same
+// IC(0)-PCG, and w = (g_c, m_f) gives dJ_k/dp_e = w_e . dfe/dp_e. The reference has no
+// gradients: this restates the adjoint on its equilibrium equations.
+int oracle_large_strain_gradient(int64_t n_nodes, const double* coords, int64_t n_elems, const int64_t* conn,
+                                 const double* young, const double* poisson, const uint8_t* fixed,
+                                 int increments, const double* u_hist, const double* dJdR, double pcg_tol,
+                                 int64_t pcg_max, double* dJdmu, double* dJdlambda) {
+    LargeStrainMesh m{(size_t)n_nodes, (size_t)n_elems, coords, conn, {}, {}};
+    m.lambda.resize(m.n_elems);
+    m.mu.resize(m.n_elems);
+    for (size_t e = 0; e < m.n_elems; ++e) lame(young[e], poisson[e], m.lambda[e], m.mu[e]);
+    const size_t n = 3 * (size_t)n_nodes;
+    FreeTopology t = free_topology(m.n_elems, conn, fixed, n);
+    std::fill(dJdmu, dJdmu + n_elems, 0.0);
+    if (dJdlambda) std::fill(dJdlambda, dJdlambda + n_elems, 0.0);
+    size_t pcg_iters = 0;
+    for (int k = increments - 1; k >= 0; --k) {
+        const double* g = dJdR + (size_t)k * n;
+        bool any = false;
+        for (size_t q = 0; q < n; ++q) any = any || (fixed[q] && g[q] != 0.0);
+        if (!any) continue;
+        Vec uk(u_hist + (size_t)k * n, u_hist + (size_t)(k + 1) * n), internal, tangents;
+        responses(m, uk, internal, tangents);
+        Vec w(n, 0.0), zero(n, 0.0);
+        for (size_t q = 0; q < n; ++q)
+            if (fixed[q]) w[q] = g[q];
+        const int st = free_solve(t, m, tangents, zero, w, pcg_tol > 0 ? pcg_tol : TOLERANCE,
+                                  pcg_max > 0 ? (size_t)pcg_max : MAX_ITERATIONS, pcg_iters);
+        if (st != OK) return st;
+        for (size_t e = 0; e < m.n_elems; ++e) {
+            double c[4][3], ue[12], fe[12], ke[144], dmu[12], dla[12];
+            m.coords_of(e, c);
+            for (int l = 0; l < 12; ++l) ue[l] = uk[3 * (size_t)conn[e * 4 + l / 3] + l % 3];
+            neo_hookean_tet4(c, m.lambda[e], m.mu[e], ue, fe, ke, dmu, dla);
+            double sm = 0.0, sl = 0.0;
+            for (int l = 0; l < 12; ++l) {
+                const double wl = w[3 * (size_t)conn[e * 4 + l / 3] + l % 3];
+                sm += wl * dmu[l];
+                sl += wl * dla[l];
+            }
+            dJdmu[e] += sm;
+            if (dJdlambda) dJdlambda[e] += sl;
+        }
+    }
+    return OK;
+}
+
+// One neo-Hookean Tet4 response (for element-level tests): fe [12], ke [144], dfe/dmu, dfe/dlambda.
+int oracle_neo_hookean_tet4(const double* coords12, double lambda, double mu, const double* ue, double* fe,
+                            double* ke, double* dfe_dmu, double* dfe_dlambda) {
+    double c[4][3];
+    for (int a = 0; a < 4; ++a)
+        for (int k = 0; k < 3; ++k) c[a][k] = coords12[3 * a + k];
+    return neo_hookean_tet4(c, lambda, mu, ue, fe, ke, dfe_dmu, dfe_dlambda) ? OK : INVALID;
 }
 
 }  // extern "C"

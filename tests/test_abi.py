@@ -47,7 +47,9 @@ def test_version_and_device_count_need_no_gpu(lib):
 
 
 STRUCTS = (("MailleElasticProblem", _lib.ElasticProblem), ("MailleElasticResult", _lib.ElasticResult),
-           ("MailleBatchProblem", _lib.BatchProblem), ("MailleBatchResult", _lib.BatchResult))
+           ("MailleBatchProblem", _lib.BatchProblem), ("MailleBatchResult", _lib.BatchResult),
+           ("MailleLargeStrainProblem", _lib.LargeStrainProblem),
+           ("MailleLargeStrainResult", _lib.LargeStrainResult))
 
 
 def test_struct_layouts_match_the_header(tmp_path):
