@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost section")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched section")
+    ap.add_argument("--no-large-strain", action="store_true", help="skip the large-strain section")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--adjoint-cells", type=int, default=48)
     ap.add_argument("--only", choices=["mixed", "plain"], default=None,
@@ -303,6 +304,44 @@ def batched_section(torch, mb, mg, L, count, tol, steps, warmup, device, rank=0,
     return out
 
 
+def large_strain_section(mb, mg, steps, device):
+    """Large-strain neo-Hookean Tet4 block (64 x 16 x 16 cells, 56 355 DOF, 98 304 tets): one
+    forward = the whole quasi-static step (10 increments of Newton to 1e-8 with IC(0)-PCG inner
+    solves, checkpoints kept on the device); one backward = the gradient of the final tip
+    reaction force with respect to every mu_e (reverse pass: tangent at the checkpoint, one
+    adjoint PCG solve, element gradient kernel). Host wall clock around the synchronous calls."""
+    p, mu, tip = mg.large_strain_block()
+    out = {"workload": "neo_hookean_tet4_64x16x16_10inc", "dofs": 3 * p.n_nodes, "elements": p.n_elems}
+    with mb.LargeStrainSolver(p, increments=10, device=device) as s:
+        h = s.run()  # warm-up
+        w = np.zeros_like(h.reactions)
+        w[-1, tip] = 1.0
+        s.backward(w)
+        fw, bw = [], []
+        for _ in range(max(1, steps)):
+            t0 = time.perf_counter()
+            h = s.run()
+            fw.append((time.perf_counter() - t0) * 1e3)
+            t0 = time.perf_counter()
+            gm, _ = s.backward(w)
+            bw.append((time.perf_counter() - t0) * 1e3)
+    out.update({"forward_ms": statistics.median(fw), "backward_ms": statistics.median(bw),
+                "backward_over_forward": statistics.median(bw) / statistics.median(fw),
+                "newton_total": int(h.newton_total), "pcg_total": int(h.pcg_total),
+                "tip_reaction": float(h.reactions[-1, tip].sum())})
+    path = os.path.join(ROOT, "tests", "golden", "large_strain_oracle_summary.json")
+    if os.path.exists(path):
+        g = json.load(open(path))
+        el = np.array(g["elements"])
+        out["grad_rel_err_vs_oracle"] = float(np.linalg.norm(gm[el] - np.array(g["dJdmu"]))
+                                              / np.linalg.norm(g["dJdmu"]))
+        out["tip_reaction_rel_err_vs_oracle"] = abs(out["tip_reaction"] - g["tip_reaction"][-1]) / abs(
+            g["tip_reaction"][-1])
+        out["oracle_cpu_forward_s"] = g["wall_s"]
+        out["oracle_cpu_note"] = "oracle wall time from the golden summary (1 core, build container)"
+    return out
+
+
 def spmv_roofline(torch, h, L, precision, blocks, nb, reps=50):
     """Average duration of the PCG SpMV kernel over `reps` launches (CUDA events on the
     library's stream) and its algorithmic bytes: per block 9 values + one int32 column index,
@@ -512,6 +551,10 @@ def run_ours(args):
         batched = batched_section(torch, mb, mg, L, args.batch_count, args.tol, args.steps,
                                   args.warmup, local, rank, world)
 
+    large_strain = None
+    if not args.no_large_strain:
+        large_strain = large_strain_section(mb, mg, args.steps, local)
+
     adjoint = None
     if not args.no_adjoint:
         adjoint = adjoint_section(torch, mb, mg, L, args.adjoint_cells, args.tol, args.steps,
@@ -553,6 +596,7 @@ def run_ours(args):
                  "fp64": {"achieved": gbs64, "frac": gbs64 / hbm, "bytes_per_launch": bytes64,
                           "ms_per_launch": ms64}},
         "batched": batched,
+        "large_strain": large_strain,
         "adjoint": adjoint,
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
     }
