@@ -30,16 +30,33 @@ def stale() -> bool:
     return any(os.path.getmtime(f) > t for f in SRC + HDR)
 
 
+OBJ_DIR = os.path.join(HERE, "..", "_build", "obj")
+
+
+def _compile(src: str, verbose: bool) -> str:
+    obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+    cmd = [NVCC, *[f for f in FLAGS if f != "-shared"], "-c", "-o", obj, src]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {os.path.basename(src)}:\n" + r.stdout + r.stderr)
+    if verbose:
+        sys.stderr.write(r.stderr)
+    return obj
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every translation unit (in parallel, one nvcc per file) and links the library."""
     if force or stale():
-        cmd = [NVCC, *FLAGS, "-o", LIB, *SRC]
-        if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        from concurrent.futures import ThreadPoolExecutor
+        os.makedirs(OBJ_DIR, exist_ok=True)
+        with ThreadPoolExecutor(max_workers=min(len(SRC), os.cpu_count() or 1)) as pool:
+            objs = list(pool.map(lambda f: _compile(f, verbose), SRC))
+        r = subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB, *objs],
+                           capture_output=True, text=True)
         if r.returncode != 0:
-            raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
-        if verbose:
-            sys.stderr.write(r.stderr)
+            raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     return LIB
 
 

@@ -75,6 +75,27 @@ struct SellHost {
 
 enum SellKind { SELL_FULL = 0, SELL_LOWER = 1, SELL_UPPER = 2 };
 
+// Packed sliced layout of the strictly lower (L) or upper (U) factor blocks, the operands of the
+// dataflow sweeps. The rows of one level are packed in order into slices of one step of 128 slots
+// (32 lanes x 4 consecutive slots, value plane k of step g at vals[(g * 9 + k) * 128 + slot] as in
+// SellHost). A row takes max(1, length) consecutive slots and may span lanes; a slice closes when
+// the next row does not fit or it holds 32 rows, and its unused slots are padding (the dummy node,
+// zero values) that count as part of its last row. A row longer than 128 blocks gets a slice of its own over several
+// steps. Bit b of head[4 s + w] is set when slot 32 w + b of slice s starts a row; the rows of
+// slice s, in slot order, are rows[row0[s] .. row0[s + 1]). Slices are stored in sweep order:
+// levels ascending for L (forward sweep), descending for U (backward sweep); level_slices[q] is
+// the first slice of the q-th level swept.
+struct PsellHost {
+    std::vector<int64_t> off{0};        // [nslices + 1] first step of each slice
+    std::vector<int32_t> col, src;      // [steps * 128] node column / CSR block of each slot
+    std::vector<uint32_t> head;         // [nslices * 4] row-start bits
+    std::vector<int32_t> row0{0};       // [nslices + 1]
+    std::vector<int32_t> rows;          // [nb] matrix row of each packed row
+    std::vector<int32_t> level_slices;  // [levels + 1]
+    int64_t steps() const { return off.back(); }
+    int32_t nslices() const { return (int32_t)off.size() - 1; }
+};
+
 // Sliced layout of the batched solver (block-diagonal system of many instances, several
 // right-hand sides). A slice holds `rows` rows of ONE instance (and, for L and U, of one level);
 // each row's blocks are spread over `sub` lanes of 4 slots per step, so a step holds
@@ -101,6 +122,9 @@ void build_bsell(const Symbolic& s, SellKind kind, int rows, int sub, const std:
 // Builds the sliced layout of one part of the analysed pattern. lpr <= 0 picks lanes per row
 // from the mean row length.
 void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out);
+
+// Builds the packed layout of the strictly lower (SELL_LOWER) or upper (SELL_UPPER) blocks.
+void build_psell(const Symbolic& s, SellKind kind, PsellHost& out);
 
 // Builds the symbolic analysis. conn is [n_elems * npe] in the caller's node numbering.
 bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,

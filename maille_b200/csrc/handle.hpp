@@ -41,6 +41,38 @@ struct SellBuf {
     }
 };
 
+// A packed layout of a factor triangle: host description plus its device arrays.
+struct PsellBuf {
+    PsellHost h;
+    int64_t* off = nullptr;
+    int32_t* col = nullptr;
+    int32_t* src = nullptr;
+    uint32_t* head = nullptr;
+    int32_t* row0 = nullptr;
+    int32_t* rows = nullptr;
+    PsellDev dev() const {
+        return PsellDev{h.nslices(), off, col, reinterpret_cast<const uint4*>(head), row0, rows};
+    }
+    void upload(cudaStream_t st) {
+        off = dupload(h.off.data(), h.off.size(), st);
+        col = dupload(h.col.data(), h.col.size(), st);
+        src = dupload(h.src.data(), h.src.size(), st);
+        head = dupload(h.head.data(), h.head.size(), st);
+        row0 = dupload(h.row0.data(), h.row0.size(), st);
+        rows = dupload(h.rows.data(), h.rows.size(), st);
+    }
+    void release() {
+        for (void* p : {(void*)off, (void*)col, (void*)src, (void*)head, (void*)row0, (void*)rows})
+            if (p) cudaFree(p);
+        off = nullptr;
+        col = nullptr;
+        src = nullptr;
+        head = nullptr;
+        row0 = nullptr;
+        rows = nullptr;
+    }
+};
+
 struct MailleGpuHandle {
     int device = 0;
     cudaStream_t st = nullptr;
@@ -71,10 +103,12 @@ struct MailleGpuHandle {
     // device: numeric (CSR K and factor F; sliced copies for the iterations)
     double* ke = nullptr;
     double *K = nullptr, *F = nullptr;
-    SellBuf sk, sl, su;
+    SellBuf sk;      // K, sliced, for the SpMV
+    PsellBuf pl, pu;  // strictly lower / upper blocks of the factor, packed, for the sweeps
     double *Ks64 = nullptr, *Ls64 = nullptr, *Us64 = nullptr, *D64 = nullptr;
     float *Ks32 = nullptr, *Ls32 = nullptr, *Us32 = nullptr, *D32 = nullptr;
-    // padded solver vectors (4 entries per block row)
+    // padded solver vectors (4 entries per block row); z64 / z32 hold the sweep records
+    // (z0, z1, z2, tag) of the persistent kernel
     double *b64 = nullptr, *x64 = nullptr, *r64 = nullptr, *z64 = nullptr, *p64 = nullptr,
            *ap64 = nullptr;
     float *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *ap32 = nullptr;
@@ -83,22 +117,15 @@ struct MailleGpuHandle {
     PcgScalars* scal = nullptr;
     PcgScalars* h_scal = nullptr;  // pinned
     double* partials = nullptr;
-    double* lvl_total = nullptr;
     double* dsum = nullptr;        // [4] misc sums
     double* h_sum = nullptr;       // pinned [4]
     unsigned int* dticket = nullptr;
     int32_t* dfail = nullptr;
     int spmv_grid = 1;
-    cudaGraphExec_t graph = nullptr;  // PCG iterations of the handle's form (per-level launches)
-    int persist_grid = 0;             // > 0: the persistent cooperative kernel runs the PCG
+    int persist_grid = 0;             // co-resident grid of the persistent PCG kernel
     int persist_chunk = 64;           // iterations per persistent launch
-    int32_t *lvl_l = nullptr, *lvl_u = nullptr;
     unsigned long long* timing = nullptr;  // per-phase ns when MAILLE_PHASE_TIMING is set
-    int32_t* claim = nullptr;              // dataflow sweeps: claim counters [2] + timeout flag
-    unsigned int* flags = nullptr;         // row-ready flags [nb + 1] (the dummy's is always set)
-    int32_t* bwd_seq = nullptr;            // U slices by level, descending
-    int graph_iters = 8;
-    long long graph_kernels = 0;
+    int32_t* claim = nullptr;              // [4]; claim[2]: the sweeps' timeout flag
     std::atomic<int> cancel{0};
     double shift = 0.0;
     bool solved = false;

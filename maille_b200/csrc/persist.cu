@@ -9,11 +9,21 @@
 // whose FP32 residual fell by `delta` since the last one.
 //
 // Sweeps are dataflow instead of one barrier per level: warps take slices in level order on a
-// fixed round-robin schedule; before gathering a neighbour's value a lane waits for that row's
-// ready flag to reach the current sweep epoch (acquire), and after writing a row the lane
-// publishes its flag (release). A slice only depends on slices of earlier levels, which come
-// earlier in every warp's schedule, and all warps are co-resident (cooperative launch), so every
-// wait ends; each wait is also bounded and reports a timeout status instead of spinning forever.
+// fixed round-robin schedule; before gathering a neighbour's value a lane waits until that row
+// has been written in the current sweep (epoch). A slice only depends on slices of earlier
+// levels, which come earlier in every warp's schedule, and all warps are co-resident
+// (cooperative launch), so every wait ends; each wait is also bounded and reports a timeout
+// status instead of spinning forever. How a lane knows a row is ready depends on the precision:
+//  * FP32: the sweep vector holds one 16-byte record per node, (z0, z1, z2, tag), written and
+//    read as single 128-bit accesses; the tag is the epoch of the sweep that wrote the record.
+//    A gather that sees the current tag has the row's values in the same access (the
+//    single-transaction property of aligned 16-byte accesses that CUB's decoupled look-back
+//    also relies on), so one round trip per gather and no fence.
+//  * FP64: (z0, z1, z2, tag) in one 32-byte word, read and written as single 256-bit accesses
+//    (sm_100 vector width), aligned to one L2 sector, so the same single-access argument holds.
+// The factors use the packed layout (PsellDev): one-step slices of whole rows, a segmented scan
+// over the warp instead of a fixed number of lanes per row, so neither padding to a row-length
+// multiple nor a chain of steps per row sits on the sweep's critical path.
 //
 // Vectors written inside the launch are read with ld.global.cg (L2, coherent after a barrier or
 // an acquire); matrix data, which no phase writes, through the read-only path.
@@ -84,42 +94,34 @@ __device__ __forceinline__ void put3(T* x, int64_t i, T a, T b, T d) {
     set4(x, i, v);
 }
 
-__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
-    unsigned int v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+
+
+// FP32 sweep record of node c: (z0, z1, z2, tag) in one 128-bit access
+__device__ __forceinline__ float4 ld_rec(const float* z, int32_t c) {
+    float4 v;
+    asm volatile("ld.relaxed.gpu.global.v4.f32 {%0,%1,%2,%3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(z + 4 * (int64_t)c)
+                 : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_rec(float* z, int32_t c, float a, float b, float d, unsigned int tag) {
+    asm volatile("st.relaxed.gpu.global.v4.f32 [%0], {%1,%2,%3,%4};" ::"l"(z + 4 * (int64_t)c), "f"(a),
+                 "f"(b), "f"(d), "f"(__uint_as_float(tag))
+                 : "memory");
 }
 
-// Waits (acquire loads) until row c is ready for sweep `epoch`; false after the spin limit.
-__device__ __forceinline__ bool wait_ready(const unsigned int* flags, int32_t c, unsigned int epoch) {
-    if (ld_acquire(flags + c) >= epoch) return true;
-    for (unsigned int k = 0; k < kSpinLimit; ++k) {
-        __nanosleep(64);
-        if (ld_acquire(flags + c) >= epoch) return true;
-    }
-    return false;
-}
 
-// this lane's 4 slots of step g: acc += V_b x[col_b] (x read coherently through L2). With
-// `flags`, each column's ready flag is awaited first (dataflow sweeps).
+// this lane's 4 slots of step g: acc += V_b x[col_b] (x read coherently through L2)
 template <typename M, typename T>
-__device__ __forceinline__ bool step(const M* __restrict__ vals, const int32_t* __restrict__ col,
-                                     int64_t g, const T* x, int lane, T& a0, T& a1, T& a2,
-                                     const unsigned int* flags = nullptr, unsigned int epoch = 0) {
+__device__ __forceinline__ void step(const M* __restrict__ vals, const int32_t* __restrict__ col,
+                                     int64_t g, const T* x, int lane, T& a0, T& a1, T& a2) {
     const int4 c4 = __ldg(reinterpret_cast<const int4*>(col + g * kStepSlots + 4 * lane));
     const M* V = vals + g * 9 * kStepSlots + 4 * lane;
     M v[9][4];
 #pragma unroll
     for (int k = 0; k < 9; ++k) ldv4(V + k * kStepSlots, v[k]);
     const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
-    bool ok = true;
-    if (flags) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j) ok = wait_ready(flags, cc[j], epoch) && ok;
-    }
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         T x0, x1, x2;
@@ -128,7 +130,6 @@ __device__ __forceinline__ bool step(const M* __restrict__ vals, const int32_t* 
         a1 += (T)v[3][j] * x0 + (T)v[4][j] * x1 + (T)v[5][j] * x2;
         a2 += (T)v[6][j] * x0 + (T)v[7][j] * x1 + (T)v[8][j] * x2;
     }
-    return ok;
 }
 
 template <typename T, int LPR>
@@ -189,57 +190,375 @@ __device__ __forceinline__ double spmv_phase(const SellDev& A, const M* vals, co
     return loc;
 }
 
-// One dataflow sweep, one warp per slice. Warp w of the grid takes slices k = w, w + W, ... of
-// `seq` (slice ids in dependency order: levels ascending forward, descending backward), a fixed
-// round-robin schedule: the smallest unfinished slice always belongs to a warp that has finished
-// all its earlier slices, and everything it depends on comes earlier in `seq`, so the sweep
-// always progresses; the schedule is also fixed from run to run, which keeps the r . z partial
-// sums deterministic. Before gathering a neighbour a lane waits for its ready flag (acquire);
-// after writing a row it publishes the row's flag (release). Returns this thread's share of
-// r . z (backward); `ok` turns false when a wait hit the spin limit.
-template <typename T, int LPR, bool FWD>
-__device__ __forceinline__ double sweep(const SellDev& A, int32_t nslices, const int32_t* seq,
-                                        unsigned int* flags, unsigned int epoch, const T* vals,
-                                        const T* D, int32_t nb, const T* r, T* z, bool& ok) {
-    const int lane = threadIdx.x & 31, rr = lane / LPR, q = lane % LPR;
-    constexpr int S = 32 / LPR;
-    const int32_t nw = (int32_t)(gridDim.x * kPW);
+// ---- dataflow sweeps on the packed layout -------------------------------------------------
+
+// Sweep records: (z0, z1, z2, tag) per node, 16 bytes in FP32 and 32 bytes in FP64, each
+// written and read as one vector access and carrying the epoch of the sweep that wrote it, so a
+// reader that sees the current tag has the row's current values.
+struct Rec32 {
+    float4 q;
+};
+struct Rec64 {
+    double x, y, z, w;
+};
+__device__ __forceinline__ Rec32 ld_record(const float* z, int32_t c) { return Rec32{ld_rec(z, c)}; }
+__device__ __forceinline__ Rec64 ld_record(const double* z, int32_t c) {
+    Rec64 v;
+    asm volatile("ld.relaxed.gpu.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+                 : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+                 : "l"(z + 4 * (int64_t)c)
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ bool ready(const Rec32& r, unsigned int epoch) {
+    return __float_as_uint(r.q.w) >= epoch;
+}
+__device__ __forceinline__ bool ready(const Rec64& r, unsigned int epoch) {
+    return (unsigned long long)__double_as_longlong(r.w) >= epoch;
+}
+__device__ __forceinline__ void values(const Rec32& r, float& a, float& b, float& d) {
+    a = r.q.x; b = r.q.y; d = r.q.z;
+}
+__device__ __forceinline__ void values(const Rec64& r, double& a, double& b, double& d) {
+    a = r.x; b = r.y; d = r.z;
+}
+template <typename T>
+struct RecOf;
+template <>
+struct RecOf<float> { using type = Rec32; };
+template <>
+struct RecOf<double> { using type = Rec64; };
+
+// Re-reads record c until it carries `epoch` (at most kSpinLimit polls); returns the last read.
+template <typename T>
+__device__ __forceinline__ typename RecOf<T>::type spin_record(const T* z, int32_t c, unsigned int epoch,
+                                                               typename RecOf<T>::type r) {
+    for (unsigned int k = 0; k < kSpinLimit && !ready(r, epoch); ++k) {
+        __nanosleep(32);
+        r = ld_record(z, c);
+    }
+    return r;
+}
+
+// publishes row `row` of the sweep output for sweep `epoch`
+__device__ __forceinline__ void publish_row(float* z, int32_t row, float a, float b, float d, unsigned int epoch) {
+    st_rec(z, row, a, b, d, epoch);
+}
+__device__ __forceinline__ void publish_row(double* z, int32_t row, double a, double b, double d, unsigned int epoch) {
+    asm volatile("st.relaxed.gpu.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(z + 4 * (int64_t)row), "d"(a),
+                 "d"(b), "d"(d), "d"(__longlong_as_double((long long)epoch))
+                 : "memory");
+}
+// values of row i of a sweep record vector (plain loads: callers read after a grid barrier)
+__device__ __forceinline__ void rec_get(const float* z, int64_t i, double v[3]) {
+    const float4 q = __ldcg(reinterpret_cast<const float4*>(z + 4 * i));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z;
+}
+__device__ __forceinline__ void rec_get(const double* z, int64_t i, double v[3]) {
+    const double2 q = __ldcg(reinterpret_cast<const double2*>(z + 4 * i));
+    v[0] = q.x; v[1] = q.y; v[2] = __ldcg(z + 4 * i + 2);
+}
+
+// ---- staging of the factor values: TMA bulk copies into a per-warp shared buffer ------------
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// one 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16) that
+// completes on `bar`; the issuing lane also arrives on `bar`, announcing the bytes
+__device__ __forceinline__ void bulk_stage(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// Waits for phase `parity` of `bar` to complete; false after the spin limit. A bulk copy from
+// global memory depends on nothing else, so the wait ends; the bound only guards against a hang.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (unsigned int k = 0; k < kSpinLimit; ++k)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void lds4(const float* p, float v[4]) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void lds4(const double* p, double v[4]) {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
+// Per-warp staging state of a sweep: the warp's shared buffer (one step: 9 planes x 128 slots),
+// its mbarrier and the phase parity the next wait expects.
+template <typename T>
+struct Stage {
+    T* buf;
+    uint64_t* bar;
+    uint32_t phase;
+};
+// starts the bulk copy of step g's values (9 planes x 128 slots) into the warp's buffer
+template <typename T>
+__device__ __forceinline__ void stage_step(const T* vals, int64_t g, Stage<T>& st) {
+    constexpr uint32_t kBytes = 9 * kStepSlots * sizeof(T);
+    bulk_stage(st.buf, vals + g * 9 * kStepSlots, kBytes, st.bar);
+}
+
+// One step of a packed slice for this lane's 4 slots: P[j] = V_j z[col_j], every column first
+// awaited for sweep `epoch`; false when a wait hit the spin limit. The step's values are already on
+// their way into the warp's buffer (a bulk copy started when the buffer last became free) and the
+// lane's columns were fetched ahead, so the records are requested at once and their L2 round trip
+// is the step's only wait. Once every lane has read the buffer, lane 0 starts the copy of step
+// `next` (the next step of this slice or the first of the warp's next slice; < 0: none).
+template <typename T>
+__device__ __forceinline__ bool slot_products(const T* __restrict__ vals, int4 c4, const T* z,
+                                              unsigned int epoch, int lane, Stage<T>& st,
+                                              int64_t next, T P[4][3]) {
+    using R = typename RecOf<T>::type;
+    const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+    R q[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) q[j] = ld_record(z, cc[j]);
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (!ready(q[j], epoch)) q[j] = spin_record(z, cc[j], epoch, q[j]);
+        ok = ok && ready(q[j], epoch);
+    }
+    ok = mbar_wait(st.bar, st.phase) && ok;
+    st.phase ^= 1u;
+    const T* V = st.buf + 4 * lane;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) P[j][0] = P[j][1] = P[j][2] = 0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        T v[4];
+        lds4(V + k * kStepSlots, v);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            T x0, x1, x2;
+            values(q[j], x0, x1, x2);
+            const T x = k % 3 == 0 ? x0 : (k % 3 == 1 ? x1 : x2);
+            P[j][k / 3] += v[j] * x;
+        }
+    }
+    __syncwarp();  // every lane has read the buffer before lane 0 refills it
+    if (lane == 0 && next >= 0) stage_step(vals, next, st);
+    return ok;
+}
+
+// position of the n-th (0-based) set bit of m (m has more than n bits set)
+__device__ __forceinline__ int nth_set(uint32_t m, int n) {
+    int pos = 0, c = __popc(m & 0xFFFFu);
+    if (n >= c) { n -= c; m >>= 16; pos += 16; }
+    c = __popc(m & 0xFFu);
+    if (n >= c) { n -= c; m >>= 8; pos += 8; }
+    c = __popc(m & 0xFu);
+    if (n >= c) { n -= c; m >>= 4; pos += 4; }
+    c = __popc(m & 0x3u);
+    if (n >= c) { n -= c; m >>= 2; pos += 2; }
+    if (n >= (int)(m & 1u)) pos += 1;
+    return pos;
+}
+__device__ __forceinline__ int nth_set(uint4 h, int n) {
+    int c = __popc(h.x);
+    if (n < c) return nth_set(h.x, n);
+    n -= c;
+    c = __popc(h.y);
+    if (n < c) return 32 + nth_set(h.y, n);
+    n -= c;
+    c = __popc(h.z);
+    if (n < c) return 64 + nth_set(h.z, n);
+    return 96 + nth_set(h.w, n - c);
+}
+__device__ __forceinline__ uint32_t head_bits(uint4 h, int lane) {
+    const int w = lane >> 3;
+    const uint32_t word = w == 0 ? h.x : w == 1 ? h.y : w == 2 ? h.z : h.w;
+    return (word >> ((lane & 7) * 4)) & 0xFu;
+}
+
+// The right-hand side and diagonal inverse of one sweep row: t = (FWD ? r : y) at the row; D is
+// 9 planes of nb entries, lower triangular (entries 0, 3, 4, 6, 7, 8).
+template <typename T, bool FWD>
+struct RowIn {
+    T t0, t1, t2, d0, d3, d4, d6, d7, d8;
+    T q0, q1, q2;  // backward: r at the row, for r . z
+    __device__ __forceinline__ void load(int32_t row, const T* D, int32_t nb, const T* r, const T* z) {
+        if (FWD) {
+            node3_cg<T>(r, row, t0, t1, t2);
+        } else {
+            double v[3];
+            rec_get(z, row, v);
+            t0 = (T)v[0]; t1 = (T)v[1]; t2 = (T)v[2];
+            node3_cg<T>(r, row, q0, q1, q2);
+        }
+        const T* d = D + row;
+        d0 = __ldg(d);
+        d3 = __ldg(d + 3 * (int64_t)nb);
+        d4 = __ldg(d + 4 * (int64_t)nb);
+        d6 = __ldg(d + 6 * (int64_t)nb);
+        d7 = __ldg(d + 7 * (int64_t)nb);
+        d8 = __ldg(d + 8 * (int64_t)nb);
+    }
+    // forward: y = L_II^-1 (r - sum L y); backward: z = L_II^-T (y - sum L^T z) and r . z
+    __device__ __forceinline__ double finish(int32_t row, T a0, T a1, T a2, const T* r, T* z,
+                                             unsigned int epoch) const {
+        const T u0 = t0 - a0, u1 = t1 - a1, u2 = t2 - a2;
+        if (FWD) {
+            publish_row(z, row, d0 * u0, d3 * u0 + d4 * u1, d6 * u0 + d7 * u1 + d8 * u2, epoch);
+            return 0.0;
+        }
+        const T z0 = d0 * u0 + d3 * u1 + d6 * u2, z1 = d4 * u1 + d7 * u2, z2 = d8 * u2;
+        publish_row(z, row, z0, z1, z2, epoch);
+        return (double)q0 * (double)z0 + (double)q1 * (double)z1 + (double)q2 * (double)z2;
+    }
+};
+
+// Slice bookkeeping a warp fetches ahead: the slice's steps [g0, g1), its packed rows [r0, r1)
+// and its row-start bits. Out-of-range slices read as empty.
+struct SliceMeta {
+    int64_t g0, g1;
+    int32_t r0, r1;
+    uint4 head;
+};
+__device__ __forceinline__ SliceMeta slice_meta(const PsellDev& A, int32_t sl) {
+    SliceMeta m{0, 0, 0, 0, make_uint4(0u, 0u, 0u, 0u)};
+    if (sl < A.nslices) {
+        m.g0 = __ldg(A.off + sl);
+        m.g1 = __ldg(A.off + sl + 1);
+        m.r0 = __ldg(A.row0 + sl);
+        m.r1 = __ldg(A.row0 + sl + 1);
+        m.head = __ldg(A.head + sl);
+    }
+    return m;
+}
+__device__ __forceinline__ int4 lane_cols(const PsellDev& A, int64_t g, int lane) {
+    return __ldg(reinterpret_cast<const int4*>(A.col + g * kStepSlots + 4 * lane));
+}
+
+// One dataflow sweep over a packed layout whose slices are stored in sweep order, one warp per
+// slice. Warp w of the grid takes slices w, w + W, ...: a fixed round-robin schedule in which the
+// smallest unfinished slice always belongs to a warp that has finished all its earlier slices, and
+// everything it depends on comes earlier, so the sweep always progresses; the schedule is also
+// fixed from run to run, which keeps the r . z partial sums deterministic.
+// The warp's slice loop is software-pipelined so that a slice's critical path is the L2 round
+// trip of its records: the bookkeeping of the slice after next, the columns and owned rows of the
+// next slice, the next slice's right-hand sides and diagonal blocks, and (once the buffer frees)
+// the next step's values are all requested while the current slice runs.
+// In a one-step slice (at most 32 rows) lane k owns row k. Each lane forms the products of its 4
+// slots and sums them per row inside the lane; a segmented scan over the warp (fixed order)
+// carries the partial sums across lanes, and the owner of each row fetches the row's total from
+// the lane that holds its last slot. A multi-step slice holds one long row, summed over the warp.
+// Returns this thread's share of r . z (backward); `ok` turns false when a wait hit the spin limit.
+template <typename T, bool FWD>
+__device__ __forceinline__ double sweep(const PsellDev& A, unsigned int epoch, const T* vals,
+                                        const T* D, int32_t nb, const T* r, T* z, Stage<T>& st,
+                                        bool& ok) {
+    const int lane = threadIdx.x & 31;
+    const int32_t nw = (int32_t)(gridDim.x * kPW), n = A.nslices;
     double loc = 0.0;
-    for (int32_t k = (int32_t)(blockIdx.x * kPW + (threadIdx.x >> 5)); k < nslices; k += nw) {
-        const int32_t sl = seq ? __ldg(seq + k) : k;
-        const int32_t row = __ldg(A.rowid + (int64_t)sl * S + rr);
-        // the row's right-hand side and diagonal block, loaded while the steps run
-        T t0 = 0, t1 = 0, t2 = 0, d0 = 0, d3 = 0, d4 = 0, d6 = 0, d7 = 0, d8 = 0;
-        if (q == 0 && row >= 0) {
-            node3_cg<T>(FWD ? r : z, row, t0, t1, t2);
-            const T* d = D + row;
-            d0 = __ldg(d);
-            d3 = __ldg(d + 3 * (int64_t)nb);
-            d4 = __ldg(d + 4 * (int64_t)nb);
-            d6 = __ldg(d + 6 * (int64_t)nb);
-            d7 = __ldg(d + 7 * (int64_t)nb);
-            d8 = __ldg(d + 8 * (int64_t)nb);
+    int32_t k = (int32_t)(blockIdx.x * kPW + (threadIdx.x >> 5));
+    if (k >= n) return loc;
+    SliceMeta m0 = slice_meta(A, k), m1 = slice_meta(A, k + nw);
+    int4 c0 = lane_cols(A, m0.g0, lane);
+    int32_t row0 = lane < m0.r1 - m0.r0 ? __ldg(A.rows + m0.r0 + lane) : -1;
+    if (lane == 0) stage_step(vals, m0.g0, st);
+    RowIn<T, FWD> in0{};
+    if (row0 >= 0) in0.load(row0, D, nb, r, z);
+    for (; k < n; k += nw) {
+        const bool more = k + nw < n;
+        const SliceMeta m2 = slice_meta(A, k + 2 * nw);
+        int4 c1 = make_int4(nb, nb, nb, nb);
+        int32_t row1 = -1;
+        if (more) {
+            c1 = lane_cols(A, m1.g0, lane);
+            if (lane < m1.r1 - m1.r0) row1 = __ldg(A.rows + m1.r0 + lane);
         }
+        const int64_t next_slice = more ? m1.g0 : -1;
         T a0 = 0, a1 = 0, a2 = 0;
-        const int64_t g1 = __ldg(A.off + sl + 1);
-        for (int64_t g = __ldg(A.off + sl); g < g1; ++g)
-            ok = step<T, T>(vals, A.col, g, z, lane, a0, a1, a2, flags, epoch) && ok;
-        lanes_sum<T, LPR>(a0, a1, a2);
-        if (q == 0 && row >= 0) {
-            const T u0 = t0 - a0, u1 = t1 - a1, u2 = t2 - a2;
-            if (FWD) {
-                // y = L_II^-1 (r - sum L y)
-                put3(z, row, d0 * u0, d3 * u0 + d4 * u1, d6 * u0 + d7 * u1 + d8 * u2);
-            } else {
-                // z = L_II^-T (y - sum L^T z), and r . z
-                const T z0 = d0 * u0 + d3 * u1 + d6 * u2, z1 = d4 * u1 + d7 * u2, z2 = d8 * u2;
-                put3(z, row, z0, z1, z2);
-                T r0, r1, r2;
-                node3_cg<T>(r, row, r0, r1, r2);
-                loc += (double)r0 * (double)z0 + (double)r1 * (double)z1 + (double)r2 * (double)z2;
+        if (m0.g1 - m0.g0 == 1) {
+            const int32_t nrows = m0.r1 - m0.r0;
+            const uint32_t mine = head_bits(m0.head, lane);
+            const int last = lane + 1 < nrows ? nth_set(m0.head, lane + 1) - 1 : 127;
+            T P[4][3];
+            ok = slot_products(vals, c0, z, epoch, lane, st, next_slice, P) && ok;
+            // in-lane running sums, restarted at each row start; the lane's carry-out is the sum
+            // of its slots after its last row start (all 4 when none starts here)
+            T s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if ((mine >> j) & 1u) s0 = s1 = s2 = 0;
+                s0 += P[j][0]; s1 += P[j][1]; s2 += P[j][2];
+                P[j][0] = s0; P[j][1] = s1; P[j][2] = s2;
             }
-            st_release(flags + row, epoch);  // orders the row's stores before its flag
+            // segmented inclusive scan of the carry-outs over the warp
+            int f = mine != 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const T u0 = __shfl_up_sync(0xffffffffu, s0, o);
+                const T u1 = __shfl_up_sync(0xffffffffu, s1, o);
+                const T u2 = __shfl_up_sync(0xffffffffu, s2, o);
+                const int fu = __shfl_up_sync(0xffffffffu, f, o);
+                if (lane >= o) {
+                    if (!f) { s0 += u0; s1 += u1; s2 += u2; }
+                    f |= fu;
+                }
+            }
+            // the open row's sum over the lanes before this one completes the slots before the
+            // lane's first row start
+            T i0 = __shfl_up_sync(0xffffffffu, s0, 1), i1 = __shfl_up_sync(0xffffffffu, s1, 1),
+              i2 = __shfl_up_sync(0xffffffffu, s2, 1);
+            if (lane == 0) i0 = i1 = i2 = 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if ((mine & ((2u << j) - 1u)) == 0) {
+                    P[j][0] += i0; P[j][1] += i1; P[j][2] += i2;
+                }
+            // the owner of each row takes the sum at the row's last slot
+            const int src = last >> 2, js = last & 3;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const T v0 = __shfl_sync(0xffffffffu, P[j][0], src);
+                const T v1 = __shfl_sync(0xffffffffu, P[j][1], src);
+                const T v2 = __shfl_sync(0xffffffffu, P[j][2], src);
+                if (j == js) { a0 = v0; a1 = v1; a2 = v2; }
+            }
+        } else {
+            for (int64_t g = m0.g0; g < m0.g1; ++g) {
+                const int4 cg4 = g == m0.g0 ? c0 : lane_cols(A, g, lane);
+                T P[4][3];
+                ok = slot_products(vals, cg4, z, epoch, lane, st, g + 1 < m0.g1 ? g + 1 : next_slice, P) && ok;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) { a0 += P[j][0]; a1 += P[j][1]; a2 += P[j][2]; }
+            }
+            lanes_sum<T, 32>(a0, a1, a2);
         }
+        if (row0 >= 0) loc += in0.finish(row0, a0, a1, a2, r, z, epoch);
+        // the next slice's right-hand sides and diagonal blocks (its rows arrived meanwhile)
+        RowIn<T, FWD> in1{};
+        if (row1 >= 0) in1.load(row1, D, nb, r, z);
+        m0 = m1;
+        m1 = m2;
+        c0 = c1;
+        row0 = row1;
+        in0 = in1;
     }
     return loc;
 }
@@ -256,10 +575,17 @@ __device__ __forceinline__ unsigned long long gtime() {
     return t;
 }
 
-template <typename T, int LPRK, int LPRLU, bool MIXED>
-__global__ void __launch_bounds__(kPW * 32, sizeof(T) == 4 ? 4 : 2) k_pcg(PcgArgs<T> a, int init) {
+template <typename T, int LPRK, bool MIXED>
+__global__ void __launch_bounds__(kPW * 32, 2) k_pcg(PcgArgs<T> a, int init) {
     __shared__ double sh[kPW];
+    __shared__ uint64_t bars[kPW];
+    extern __shared__ __align__(128) unsigned char stage_mem[];  // kPW x one step of factor values
     cg::grid_group grid = cg::this_grid();
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) mbar_init(&bars[warp]);
+    mbar_init_fence();
+    __syncthreads();
+    Stage<T> stage{reinterpret_cast<T*>(stage_mem) + (size_t)warp * 9 * kStepSlots, &bars[warp], 0u};
     PcgScalars* s = a.s;
     Local v{s->alpha, s->beta, s->rz, s->rr, s->bb, s->tol, s->maxr, s->delta, s->rr_true,
             s->iter, s->max_iter, s->done, s->status, s->updates, s->epoch};
@@ -366,13 +692,11 @@ __global__ void __launch_bounds__(kPW * 32, sizeof(T) == 4 ? 4 : 2) k_pcg(PcgArg
         // z = (L L^T)^-1 r (Csr::precondition, iterative.rs:173-188): dataflow sweeps
         bool ok = true;
         v.epoch += 1;
-        sweep<T, LPRLU, true>(a.L, a.L.nslices, nullptr, a.flags, v.epoch, a.Lv, a.D, a.nb, a.r,
-                              a.z, ok);
+        sweep<T, true>(a.L, v.epoch, a.Lv, a.D, a.nb, a.r, a.z, stage, ok);
         grid.sync();
         mark(3);
         v.epoch += 1;
-        loc = sweep<T, LPRLU, false>(a.U, a.U.nslices, a.bwd_seq, a.flags, v.epoch, a.Uv, a.D,
-                                     a.nb, a.r, a.z, ok);
+        loc = sweep<T, false>(a.U, v.epoch, a.Uv, a.D, a.nb, a.r, a.z, stage, ok);
         if (!ok) atomicExch(timeout, 1);
         publish(loc, a.partials, 3, sh);
         grid.sync();
@@ -387,11 +711,11 @@ __global__ void __launch_bounds__(kPW * 32, sizeof(T) == 4 ? 4 : 2) k_pcg(PcgArg
         v.rz = rz;
         // p = z + beta p (iterative.rs:240-242)
         for (int64_t i = tid; i < a.nb; i += nthreads) {
-            double zv[4], pv[4];
-            get4(a.z, i, zv);
+            double zv[3], pv[4];
+            rec_get(a.z, i, zv);
             get4(a.p, i, pv);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) pv[c] = (double)(T)(zv[c] + v.beta * pv[c]);
+            for (int c = 0; c < 3; ++c) pv[c] = (double)(T)(zv[c] + v.beta * pv[c]);
             set4(a.p, i, pv);
         }
         grid.sync();
@@ -414,13 +738,17 @@ __global__ void __launch_bounds__(kPW * 32, sizeof(T) == 4 ? 4 : 2) k_pcg(PcgArg
     }
 }
 
+// dynamic shared memory of the persistent kernel: one staged step of factor values per warp
+template <typename T>
+constexpr size_t stage_bytes() {
+    return (size_t)kPW * 9 * kStepSlots * sizeof(T);
+}
+
 template <typename T, bool MIXED>
-void* pick(int lprk, int lprlu) {
-#define MAILLE_PICK(K, LU) \
-    if (lprk == K && lprlu == LU) return (void*)k_pcg<T, K, LU, MIXED>;
-    MAILLE_PICK(1, 1) MAILLE_PICK(1, 2) MAILLE_PICK(1, 4) MAILLE_PICK(2, 1) MAILLE_PICK(2, 2)
-    MAILLE_PICK(2, 4) MAILLE_PICK(4, 1) MAILLE_PICK(4, 2) MAILLE_PICK(4, 4)
-#undef MAILLE_PICK
+void* pick(int lprk) {
+    if (lprk == 1) return (void*)k_pcg<T, 1, MIXED>;
+    if (lprk == 2) return (void*)k_pcg<T, 2, MIXED>;
+    if (lprk == 4) return (void*)k_pcg<T, 4, MIXED>;
     return nullptr;
 }
 
@@ -429,29 +757,31 @@ void* pick(int lprk, int lprlu) {
 // Grid size of the persistent kernel: every block co-resident (0 when the layout's lanes-per-
 // row combination has no instance).
 template <typename T, bool MIXED>
-int pcg_persistent_grid(int lprk, int lprlu) {
-    void* f = pick<T, MIXED>(lprk, lprlu);
+int pcg_persistent_grid(int lprk) {
+    void* f = pick<T, MIXED>(lprk);
     if (!f) return 0;
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kPW * 32, 0);
+    const size_t smem = stage_bytes<T>();
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kPW * 32, smem);
     return sms * per_sm;
 }
 
 template <typename T, bool MIXED>
 cudaError_t launch_pcg_persistent(const PcgArgs<T>& a, int grid, bool init, cudaStream_t st) {
-    void* f = pick<T, MIXED>(a.K.lpr, a.L.lpr);
+    void* f = pick<T, MIXED>(a.K.lpr);
     if (!f) return cudaErrorInvalidValue;
     PcgArgs<T> copy = a;
     int in = init ? 1 : 0;
     void* args[] = {&copy, &in};
     g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    return cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kPW * 32), args, 0, st);
+    return cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kPW * 32), args, stage_bytes<T>(), st);
 }
 
-template int pcg_persistent_grid<double, false>(int, int);
-template int pcg_persistent_grid<float, true>(int, int);
+template int pcg_persistent_grid<double, false>(int);
+template int pcg_persistent_grid<float, true>(int);
 template cudaError_t launch_pcg_persistent<double, false>(const PcgArgs<double>&, int, bool, cudaStream_t);
 template cudaError_t launch_pcg_persistent<float, true>(const PcgArgs<float>&, int, bool, cudaStream_t);
 

@@ -432,6 +432,55 @@ void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out) {
     }
 }
 
+void build_psell(const Symbolic& s, SellKind kind, PsellHost& out) {
+    out = PsellHost{};
+    constexpr int64_t kSlots = 128;
+    auto start = [&](int32_t i) { return kind == SELL_UPPER ? s.diag[i] + 1 : s.row_ptr[i]; };
+    auto end = [&](int32_t i) { return kind == SELL_LOWER ? s.diag[i] : s.row_ptr[i + 1]; };
+    out.level_slices.push_back(0);
+    out.rows.reserve(s.nb);
+    std::vector<int32_t> open;  // rows of the slice being packed
+    int64_t used = 0;
+    auto close = [&]() {
+        if (open.empty()) return;
+        const int64_t g0 = out.off.back();
+        const int64_t len0 = end(open[0]) - start(open[0]);
+        const int64_t steps = open.size() == 1 && len0 > kSlots ? (len0 + kSlots - 1) / kSlots : 1;
+        out.off.push_back(g0 + steps);
+        out.col.resize((size_t)(g0 + steps) * kSlots, s.nb);  // padding: the dummy zero node
+        out.src.resize((size_t)(g0 + steps) * kSlots, -1);
+        uint32_t head[4] = {0, 0, 0, 0};
+        int64_t slot = 0;
+        for (int32_t i : open) {
+            head[slot >> 5] |= 1u << (slot & 31);
+            const int64_t n = end(i) - start(i);
+            for (int64_t b = 0; b < n; ++b) {
+                out.col[(size_t)(g0 * kSlots + slot + b)] = s.col[start(i) + b];
+                out.src[(size_t)(g0 * kSlots + slot + b)] = (int32_t)(start(i) + b);
+            }
+            slot += std::max<int64_t>(1, n);
+            out.rows.push_back(i);
+        }
+        for (uint32_t w : head) out.head.push_back(w);
+        out.row0.push_back((int32_t)out.rows.size());
+        open.clear();
+        used = 0;
+    };
+    // L is swept levels ascending, U levels descending: slices are stored in sweep order
+    for (int32_t q = 0; q < s.levels; ++q) {
+        const int32_t l = kind == SELL_UPPER ? s.levels - 1 - q : q;
+        for (int32_t i = s.level_ptr[l]; i < s.level_ptr[l + 1]; ++i) {
+            const int64_t need = std::max<int64_t>(1, end(i) - start(i));
+            if (used + need > kSlots || open.size() == 32) close();
+            open.push_back(i);
+            used += need;
+            if (used >= kSlots) close();
+        }
+        close();
+        out.level_slices.push_back(out.nslices());
+    }
+}
+
 void build_bsell(const Symbolic& s, SellKind kind, int rows, int sub, const std::vector<int32_t>& group,
                  BSellHost& out) {
     out = BSellHost{};

@@ -6,9 +6,9 @@
 //   assembly -> level-scheduled block IC(0) with the reference's diagonal-shift ladder.
 // solve  = FreeSystem::solve + Pcg::solve (model.rs:1502-1516, iterative.rs:210-248), then the
 //   reactions (product, model.rs:586-593) and Gauss-point stresses (model.rs:596-598).
-// The PCG iteration is a fixed kernel sequence (SpMV, forward levels, backward levels, p update)
-// captured once into a CUDA graph of several iterations; kernels skip their work once the
-// on-device `done` flag is set, and the host reads the device scalars after each graph launch.
+// The PCG runs in the persistent cooperative kernel of persist.cu: one launch for the initial
+// preconditioning, then launches of `persist_chunk` iterations until the device flags the end
+// (the host reads the device scalars after each launch: stopping, cancel flag).
 
 #include <atomic>
 #include <chrono>
@@ -49,14 +49,15 @@ MailleGpuHandle::~MailleGpuHandle() {
                      t[0] * 1e-6, t[1] * 1e-6, t[2] * 1e-6, t[3] * 1e-6, t[4] * 1e-6, t[5] * 1e-6,
                      t[6], persist_grid);
     }
-    if (graph) cudaGraphExecDestroy(graph);
     void* bufs[] = {coords, young, poisson, imposed, f, f0, conn, fixed, perm, inv, col, lrow, fixmask,
                     row_ptr, diag, tpos, lslot, lptr, contrib, inc_ptr, inc, belem, bnodes,
                     elem_slot, ke, K, F, Ks64, Ls64, Us64, D64, Ks32, Ls32, Us32, D32, b64, x64,
                     r64, z64, p64, ap64, x32, r32, z32, p32, ap32, u_full, y_full, ye, gauss, vm,
-                    react, lambda_full, grad, scal, partials, lvl_l, lvl_u, timing, claim, flags, bwd_seq, lvl_total, dsum, dticket, dfail};
+                    react, lambda_full, grad, scal, partials, timing, claim, dsum, dticket, dfail};
     for (void* p : bufs) dfree(p);
-    for (SellBuf* b : {&sk, &sl, &su}) b->release();
+    sk.release();
+    pl.release();
+    pu.release();
     if (h_scal) cudaFreeHost(h_scal);
     if (h_sum) cudaFreeHost(h_sum);
     for (auto& e : ev)
@@ -80,52 +81,6 @@ int grid_for_slices(int64_t slices) {
 
 bool is_mixed(const MailleGpuHandle* h) { return h->precision == MAILLE_MIXED; }
 
-// The preconditioner z = (L L^T)^-1 r: forward levels then backward levels (Csr::precondition,
-// iterative.rs:173-188), in the precision of the form.
-void enqueue_precondition(MailleGpuHandle* h) {
-    const int L = h->sym.levels;
-    const int32_t nb = h->sym.nb;
-    const SellDev Ld = h->sl.dev(), Ud = h->su.dev();
-    const auto& ls = h->sl.h.level_slices;
-    const auto& us = h->su.h.level_slices;
-    double* lt = h->lvl_total;
-    if (is_mixed(h)) {
-        for (int l = 0; l < L; ++l)
-            launch_fwd<float>(Ld, ls[l], ls[l + 1], h->Ls32, h->D32, nb, h->r32, h->z32, h->scal, h->st);
-        for (int l = L - 1; l >= 0; --l)
-            launch_bwd<float>(Ud, us[l], us[l + 1], l, L, h->Us32, h->D32, nb, h->r32, h->z32,
-                              h->scal, h->partials, lt, h->st);
-        launch_pupdate<float>(nb, h->z32, h->p32, h->scal, h->st);
-    } else {
-        for (int l = 0; l < L; ++l)
-            launch_fwd<double>(Ld, ls[l], ls[l + 1], h->Ls64, h->D64, nb, h->r64, h->z64, h->scal, h->st);
-        for (int l = L - 1; l >= 0; --l)
-            launch_bwd<double>(Ud, us[l], us[l + 1], l, L, h->Us64, h->D64, nb, h->r64, h->z64,
-                               h->scal, h->partials, lt, h->st);
-        launch_pupdate<double>(nb, h->z64, h->p64, h->scal, h->st);
-    }
-}
-
-// One PCG iteration (Pcg::solve loop body, iterative.rs:223-242).
-// Plain form: ap = K p, x/r update + stopping test, z = M^-1 r, beta, p.
-// Mixed form: the same in FP32 on the FP32 matrix and factor, plus a reliable update (x64 +=
-// x32, r64 = b - K64 x64 against the FP64 matrix, r32 = r64) on the iterations that raise it.
-void enqueue_iteration(MailleGpuHandle* h) {
-    const int32_t nb = h->sym.nb;
-    const SellDev Kd = h->sk.dev();
-    if (is_mixed(h)) {
-        launch_spmv<float>(Kd, h->Ks32, h->p32, h->ap32, h->scal, h->partials, h->spmv_grid, false, h->st);
-        launch_axpy<float>(nb, h->x32, h->r32, h->p32, h->ap32, h->scal, h->partials, true, h->st);
-        launch_upd_x(nb, h->x64, h->x32, h->scal, h->st);
-        launch_upd_r(Kd, h->Ks64, h->b64, h->x64, h->r64, h->scal, h->partials, h->spmv_grid, h->st);
-        launch_upd_cast(nb, h->r64, h->r32, h->scal, h->st);
-    } else {
-        launch_spmv<double>(Kd, h->Ks64, h->p64, h->ap64, h->scal, h->partials, h->spmv_grid, false, h->st);
-        launch_axpy<double>(nb, h->x64, h->r64, h->p64, h->ap64, h->scal, h->partials, false, h->st);
-    }
-    enqueue_precondition(h);
-}
-
 template <typename T>
 PcgArgs<T> pcg_args(MailleGpuHandle* h, const T* Kv, const T* Lv, const T* Uv, const T* D, T* x,
                     T* r, T* z, T* p, T* ap) {
@@ -134,10 +89,8 @@ PcgArgs<T> pcg_args(MailleGpuHandle* h, const T* Kv, const T* Lv, const T* Uv, c
     a.levels = h->sym.levels;
     a.chunk = h->persist_chunk;
     a.K = h->sk.dev();
-    a.L = h->sl.dev();
-    a.U = h->su.dev();
-    a.lvl_l = h->lvl_l;
-    a.lvl_u = h->lvl_u;
+    a.L = h->pl.dev();
+    a.U = h->pu.dev();
     a.Kv = Kv;
     a.Lv = Lv;
     a.Uv = Uv;
@@ -155,8 +108,6 @@ PcgArgs<T> pcg_args(MailleGpuHandle* h, const T* Kv, const T* Lv, const T* Uv, c
     a.partials = h->partials;
     a.timing = h->timing;
     a.claim = h->claim;
-    a.flags = h->flags;
-    a.bwd_seq = h->bwd_seq;
     return a;
 }
 
@@ -216,46 +167,8 @@ int32_t run_pcg(MailleGpuHandle* h, int32_t* iterations, int32_t* updates, doubl
     } else {
         for (double* q : {h->p64, h->ap64}) CK(cudaMemsetAsync(q, 0, n4 * sizeof(double), st));
     }
-    if (h->persist_grid > 0) return run_pcg_persistent(h, iterations, updates, rel_res);
-    // z = M^-1 b, rz = b.z, p = z (iterative.rs:217-220)
-    enqueue_precondition(h);
-    CK(cudaGetLastError());
-    if (!h->graph) {
-        cudaGraph_t g;
-        const long long before = g_kernel_launches.load();
-        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < h->graph_iters; ++k) enqueue_iteration(h);
-        CK(cudaStreamEndCapture(st, &g));
-        h->graph_kernels = g_kernel_launches.load() - before;
-        g_kernel_launches.store(before);  // captured, not launched
-        CK(cudaGraphInstantiate(&h->graph, g, 0));
-        cudaGraphDestroy(g);
-    }
-    int32_t status = MAILLE_OK;
-    for (;;) {
-        CK(cudaGraphLaunch(h->graph, st));
-        g_kernel_launches.fetch_add(h->graph_kernels);
-        CK(cudaMemcpyAsync(h->h_scal, h->scal, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        const PcgScalars& s = *h->h_scal;
-        if (s.done) {
-            status = s.status == 1 ? MAILLE_SINGULAR : (s.status == 2 ? MAILLE_NOT_CONVERGED : MAILLE_OK);
-            break;
-        }
-        if (h->cancel.load()) {
-            status = MAILLE_CANCELLED;
-            break;
-        }
-        if (s.iter >= h->max_iter + 1) {  // the device test stops at the cap; this is a guard
-            status = MAILLE_NOT_CONVERGED;
-            break;
-        }
-    }
-    const PcgScalars& s = *h->h_scal;
-    *iterations = s.iter;
-    *updates = mixed ? s.updates : 1;
-    *rel_res = s.bb > 0 ? std::sqrt((mixed ? s.rr_true : s.rr) / s.bb) : 0.0;
-    return status;
+    if (h->persist_grid <= 0) throw CudaFailure{"the persistent PCG kernel cannot be made co-resident on this device"};
+    return run_pcg_persistent(h, iterations, updates, rel_res);
 }
 
 void set_error(const std::string& m) { g_last_error = m; }
@@ -360,12 +273,12 @@ int32_t assemble_factor(MailleGpuHandle* h, Error& err) {
     if (factorize(h, err) != MAILLE_OK) return err.status;
     if (is_mixed(h)) {
         launch_sell_fill<float>(h->sk.h.steps(), h->sk.src, h->K, h->Ks32, st);
-        launch_sell_fill<float>(h->sl.h.steps(), h->sl.src, h->F, h->Ls32, st);
-        launch_sell_fill<float>(h->su.h.steps(), h->su.src, h->F, h->Us32, st);
+        launch_sell_fill<float>(h->pl.h.steps(), h->pl.src, h->F, h->Ls32, st);
+        launch_sell_fill<float>(h->pu.h.steps(), h->pu.src, h->F, h->Us32, st);
         launch_diag_fill<float>(s.nb, h->diag, h->F, h->D32, st);
     } else {
-        launch_sell_fill<double>(h->sl.h.steps(), h->sl.src, h->F, h->Ls64, st);
-        launch_sell_fill<double>(h->su.h.steps(), h->su.src, h->F, h->Us64, st);
+        launch_sell_fill<double>(h->pl.h.steps(), h->pl.src, h->F, h->Ls64, st);
+        launch_sell_fill<double>(h->pu.h.steps(), h->pu.src, h->F, h->Us64, st);
         launch_diag_fill<double>(s.nb, h->diag, h->F, h->D64, st);
     }
     CK(cudaGetLastError());
@@ -392,7 +305,6 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
     h->tol = p->rel_tol > 0 ? p->rel_tol : kDefaultTol;
     h->max_iter = p->max_iter > 0 ? p->max_iter : kDefaultMaxIter;
     if (const char* e = std::getenv("MAILLE_RELIABLE_DELTA")) h->delta = std::atof(e);
-    h->graph_iters = std::max(1, env_int("MAILLE_GRAPH_ITERS", h->graph_iters));
     const int64_t n3 = 3 * p->n_nodes;
     h->h_fixed.assign(n3, 0);
     if (p->fixed)
@@ -413,11 +325,11 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         return fail(err);
     if (h->sym.levels >= kMaxLevels) return fail({MAILLE_INVALID_INPUT, "too many IC(0) levels"});
     {
-        // the three sliced layouts are independent: build them side by side
-        const int lk = env_int("MAILLE_LPR_K", 0), llu = env_int("MAILLE_LPR_LU", 0);
+        // the three layouts are independent: build them side by side
+        const int lk = env_int("MAILLE_LPR_K", 0);
         std::thread tk([&] { build_sell(h->sym, SELL_FULL, lk, h->sk.h); });
-        std::thread tl([&] { build_sell(h->sym, SELL_LOWER, llu, h->sl.h); });
-        build_sell(h->sym, SELL_UPPER, llu, h->su.h);
+        std::thread tl([&] { build_psell(h->sym, SELL_LOWER, h->pl.h); });
+        build_psell(h->sym, SELL_UPPER, h->pu.h);
         tk.join();
         tl.join();
     }
@@ -471,7 +383,9 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         std::vector<int32_t> slot(p->n_elems, -1);
         for (size_t k = 0; k < s.belem.size(); ++k) slot[s.belem[k]] = (int32_t)k;
         h->elem_slot = dupload(slot.data(), slot.size(), st);
-        for (SellBuf* b : {&h->sk, &h->sl, &h->su}) b->upload(st);
+        h->sk.upload(st);
+        h->pl.upload(st);
+        h->pu.upload(st);
         // numeric buffers
         const int np = node_pairs(h->npe);
         const int64_t n4 = 4 * ((int64_t)s.nb + 1);  // + the dummy node that padding points at
@@ -479,23 +393,33 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         h->K = dalloc<double>((size_t)s.blocks * 9);
         h->F = dalloc<double>((size_t)s.blocks * 9);
         h->Ks64 = dalloc<double>((size_t)h->sk.h.steps() * 9 * kStepSlots);
-        for (double** q : {&h->b64, &h->x64, &h->r64, &h->z64, &h->p64, &h->ap64}) {
+        for (double** q : {&h->b64, &h->x64, &h->r64, &h->p64, &h->ap64}) {
             *q = dalloc<double>(n4);
             CK(cudaMemsetAsync(*q, 0, n4 * sizeof(double), st));
         }
         if (is_mixed(h.get())) {
             h->Ks32 = dalloc<float>((size_t)h->sk.h.steps() * 9 * kStepSlots);
-            h->Ls32 = dalloc<float>((size_t)h->sl.h.steps() * 9 * kStepSlots);
-            h->Us32 = dalloc<float>((size_t)h->su.h.steps() * 9 * kStepSlots);
+            h->Ls32 = dalloc<float>((size_t)h->pl.h.steps() * 9 * kStepSlots);
+            h->Us32 = dalloc<float>((size_t)h->pu.h.steps() * 9 * kStepSlots);
             h->D32 = dalloc<float>((size_t)s.nb * 9);
             for (float** q : {&h->x32, &h->r32, &h->z32, &h->p32, &h->ap32}) {
                 *q = dalloc<float>(n4);
                 CK(cudaMemsetAsync(*q, 0, n4 * sizeof(float), st));
             }
+            // the dummy node's sweep record is always ready (tag = the largest epoch)
+            static const unsigned int kAlwaysReady = 0xFFFFFFFFu;
+            CK(cudaMemcpyAsync(h->z32 + 4 * (int64_t)s.nb + 3, &kAlwaysReady, sizeof(unsigned int),
+                               cudaMemcpyHostToDevice, st));
         } else {
-            h->Ls64 = dalloc<double>((size_t)h->sl.h.steps() * 9 * kStepSlots);
-            h->Us64 = dalloc<double>((size_t)h->su.h.steps() * 9 * kStepSlots);
+            h->Ls64 = dalloc<double>((size_t)h->pl.h.steps() * 9 * kStepSlots);
+            h->Us64 = dalloc<double>((size_t)h->pu.h.steps() * 9 * kStepSlots);
             h->D64 = dalloc<double>((size_t)s.nb * 9);
+            // sweep records (z0, z1, z2, tag); the dummy node's tag is the largest epoch
+            h->z64 = dalloc<double>(n4);
+            CK(cudaMemsetAsync(h->z64, 0, n4 * sizeof(double), st));
+            static const unsigned long long kAlwaysReady64 = ~0ull;
+            CK(cudaMemcpyAsync(h->z64 + 4 * (int64_t)s.nb + 3, &kAlwaysReady64, sizeof(kAlwaysReady64),
+                               cudaMemcpyHostToDevice, st));
         }
         h->u_full = dalloc<double>(n3);
         h->y_full = dalloc<double>(n3);
@@ -506,39 +430,21 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         CK(cudaMallocHost(&h->h_scal, sizeof(PcgScalars)));
         CK(cudaMallocHost(&h->h_sum, 4 * sizeof(double)));
         h->partials = dalloc<double>(4 * 148 * 8);  // >= 4 slots x the persistent grid
-        h->lvl_total = dalloc<double>(kMaxLevels);
         h->dsum = dalloc<double>(4);
         h->dticket = dalloc<unsigned int>(1);
         CK(cudaMemsetAsync(h->dticket, 0, sizeof(unsigned int), st));
         h->dfail = dalloc<int32_t>(1);
         h->spmv_grid = grid_for_slices(h->sk.h.nslices());
-        h->lvl_l = dupload(h->sl.h.level_slices.data(), h->sl.h.level_slices.size(), st);
-        {
-            std::vector<int32_t> seq;
-            const auto& us = h->su.h.level_slices;
-            for (int l = s.levels - 1; l >= 0; --l)
-                for (int32_t k = us[l]; k < us[l + 1]; ++k) seq.push_back(k);
-            h->bwd_seq = dupload(seq.data(), seq.size(), st);
-            std::vector<unsigned int> fl((size_t)s.nb + 1, 0u);
-            fl[s.nb] = 0xFFFFFFFFu;
-            h->flags = dupload(fl.data(), fl.size(), st);
-            h->claim = dalloc<int32_t>(4);
-            CK(cudaMemsetAsync(h->claim, 0, 4 * sizeof(int32_t), st));
-        }
-        h->lvl_u = dupload(h->su.h.level_slices.data(), h->su.h.level_slices.size(), st);
-        if (env_int("MAILLE_PERSISTENT", 1) && h->sl.h.lpr == h->su.h.lpr) {
-            h->persist_grid = is_mixed(h.get()) ? pcg_persistent_grid<float, true>(h->sk.h.lpr, h->sl.h.lpr)
-                                                : pcg_persistent_grid<double, false>(h->sk.h.lpr, h->sl.h.lpr);
-            h->persist_grid = std::min(h->persist_grid, 148 * 8);  // partials hold 4 x 1184 blocks
-        }
+        h->claim = dalloc<int32_t>(4);
+        CK(cudaMemsetAsync(h->claim, 0, 4 * sizeof(int32_t), st));
+        h->persist_grid = is_mixed(h.get()) ? pcg_persistent_grid<float, true>(h->sk.h.lpr)
+                                            : pcg_persistent_grid<double, false>(h->sk.h.lpr);
+        h->persist_grid = std::min(h->persist_grid, 148 * 8);  // partials hold 4 x 1184 blocks
         if (env_int("MAILLE_PHASE_TIMING", 0)) {
             h->timing = dalloc<unsigned long long>(8);
             CK(cudaMemsetAsync(h->timing, 0, 8 * sizeof(unsigned long long), st));
         }
         h->persist_chunk = std::max(1, env_int("MAILLE_PERSIST_CHUNK", h->persist_chunk));
-        // graph size: keep a few thousand kernel nodes at most
-        const int per_iter = 2 * s.levels + 6;
-        h->graph_iters = std::max(1, std::min(h->graph_iters, 4000 / per_iter));
         CK(cudaEventRecord(h->ev[1], st));
         if (numeric_phase(h.get(), err) != MAILLE_OK) return fail(err);
         CK(cudaStreamSynchronize(st));

@@ -1,4 +1,4 @@
-// sparse.cu -- SELL 3x3-block SpMV, level-scheduled IC(0) sweeps and the PCG vector kernels.
+// sparse.cu -- SELL 3x3-block SpMV (standalone), PCG set-up kernels and the layout fills.
 // Layout and conventions: sparse.cuh. Reductions: reduce.cuh (deterministic).
 
 #include <atomic>
@@ -104,37 +104,6 @@ __device__ __forceinline__ void slice_accum(const T* __restrict__ vals,
     for (int64_t g = g0; g < g1; ++g) step_accum<T>(vals, col, g, x, lane, a0, a1, a2);
 }
 
-// Slice sum split across the kSweepWarps warps of a block: warp w takes steps g0 + w,
-// g0 + w + kSweepWarps, ...; the partial sums meet in shared memory and warp 0 returns the total
-// (the other warps return 0). Summation order is fixed, so results are deterministic.
-constexpr int kSweepWarps = 8;
-template <typename T>
-__device__ __forceinline__ void slice_accum_cta(const T* __restrict__ vals,
-                                                const int32_t* __restrict__ col, int64_t g0,
-                                                int64_t g1, const T* __restrict__ x, T (*red)[32][3],
-                                                T& a0, T& a1, T& a2) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    a0 = 0;
-    a1 = 0;
-    a2 = 0;
-    for (int64_t g = g0 + w; g < g1; g += kSweepWarps) step_accum<T>(vals, col, g, x, lane, a0, a1, a2);
-    if (w > 0) {
-        red[w - 1][lane][0] = a0;
-        red[w - 1][lane][1] = a1;
-        red[w - 1][lane][2] = a2;
-    }
-    __syncthreads();
-    if (w == 0) {
-#pragma unroll
-        for (int k = 0; k < kSweepWarps - 1; ++k) {
-            a0 += red[k][lane][0];
-            a1 += red[k][lane][1];
-            a2 += red[k][lane][2];
-        }
-    }
-    __syncthreads();
-}
-
 template <typename T, int LPR>
 __device__ __forceinline__ void row_reduce(T& a0, T& a1, T& a2) {
 #pragma unroll
@@ -185,220 +154,6 @@ __global__ void __launch_bounds__(kThr) k_spmv(SellDev A, const T* __restrict__ 
             }
             s->ticket[0] = 0;
         }
-    }
-}
-
-// x += alpha p, r -= alpha ap (iterative.rs:229-232) with ||r||^2. Plain form: the last block
-// applies the reference's stopping test ||r|| <= tol ||b|| (iterative.rs:233) and the cap.
-// Mixed form: it raises `update` (a reliable update of x and r in FP64) when the iterated
-// residual fell by `delta` since the last update, claims convergence, or the cap is reached.
-template <typename T>
-__global__ void __launch_bounds__(kThr) k_axpy(int32_t nb, T* __restrict__ x, T* __restrict__ r,
-                                                const T* __restrict__ p, const T* __restrict__ ap,
-                                                PcgScalars* s, double* partials, int mixed) {
-    __shared__ double sh[kWarp];
-    if (s->done) return;
-    const double alpha = s->alpha;
-    double loc = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        F4 xv = ld4(x, i), rv = ld4(r, i);
-        const F4 pv = ld4(p, i), av = ld4(ap, i);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            xv.v[c] = (double)(T)(xv.v[c] + alpha * pv.v[c]);
-            rv.v[c] = (double)(T)(rv.v[c] - alpha * av.v[c]);
-            loc += rv.v[c] * rv.v[c];
-        }
-        st4(x, i, xv);
-        st4(r, i, rv);
-    }
-    if (publish_partial(loc, partials, &s->ticket[1], sh)) {
-        const double rr = gather_sum(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            s->rr = rr;
-            s->ticket[1] = 0;
-            const bool small = sqrt(rr) <= s->tol * sqrt(s->bb);
-            if (!mixed) {
-                if (small) {
-                    s->done = 1;
-                } else if (s->iter >= s->max_iter) {
-                    s->done = 1;
-                    s->status = 2;
-                }
-            } else {
-                s->update = (small || sqrt(rr) < s->delta * s->maxr || s->iter >= s->max_iter) ? 1 : 0;
-            }
-        }
-    }
-}
-
-// reliable update, part 1: x64 += x32, x32 = 0
-__global__ void k_upd_x(int32_t nb, double* __restrict__ x64, float* __restrict__ x32, PcgScalars* s) {
-    if (s->done || !s->update) return;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        F4 a = ld4(x64, i);
-        const F4 d = ld4(x32, i);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) a.v[c] += d.v[c];
-        st4(x64, i, a);
-        st4(x32, i, F4{{0.0, 0.0, 0.0, 0.0}});
-    }
-}
-
-// reliable update, part 2: the true residual r64 = b - K64 x64 against the FP64 matrix, its norm
-// and the convergence test on it.
-template <int LPR>
-__global__ void __launch_bounds__(kThr) k_upd_r(SellDev A, const double* __restrict__ vals,
-                                                 const double* __restrict__ b,
-                                                 const double* __restrict__ x64,
-                                                 double* __restrict__ r64, PcgScalars* s,
-                                                 double* partials) {
-    __shared__ double sh[kWarp];
-    if (s->done || !s->update) return;
-    const int lane = threadIdx.x & 31;
-    double loc = 0.0;
-    for (int32_t sl = (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); sl < A.nslices;
-         sl += (int32_t)((gridDim.x * blockDim.x) >> 5)) {
-        double a0 = 0, a1 = 0, a2 = 0;
-        slice_accum<double>(vals, A.col, A.off[sl], A.off[sl + 1], x64, lane, a0, a1, a2);
-        row_reduce<double, LPR>(a0, a1, a2);
-        const int32_t row = A.rowid[(int64_t)sl * (32 / LPR) + lane / LPR];
-        if (lane % LPR == 0 && row >= 0) {
-            const double q0 = b[4 * (int64_t)row] - a0, q1 = b[4 * (int64_t)row + 1] - a1,
-                         q2 = b[4 * (int64_t)row + 2] - a2;
-            store_node(r64, row, q0, q1, q2);
-            loc += q0 * q0 + q1 * q1 + q2 * q2;
-        }
-    }
-    if (publish_partial(loc, partials, &s->ticket[3], sh)) {
-        const double rr = gather_sum(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            s->rr_true = rr;
-            s->maxr = sqrt(rr);
-            s->updates += 1;
-            s->ticket[3] = 0;
-            if (sqrt(rr) <= s->tol * sqrt(s->bb)) {
-                s->done = 1;
-            } else if (s->iter >= s->max_iter) {
-                s->done = 1;
-                s->status = 2;
-            }
-        }
-    }
-}
-
-// reliable update, part 3: the FP32 recurrence restarts from the true residual
-__global__ void k_upd_cast(int32_t nb, const double* __restrict__ r64, float* __restrict__ r32,
-                           PcgScalars* s) {
-    if (s->done || !s->update) return;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb;
-         i += (int64_t)gridDim.x * blockDim.x)
-        st4(r32, i, ld4(r64, i));
-}
-
-// One level of the forward sweep y_I = L_II^-1 (r_I - sum_{J<I} L_IJ y_J) (Csr::precondition,
-// iterative.rs:175-179, block form; D_I = L_II^-1 stored as 9 planes of nb entries). One block of
-// kSweepWarps warps per slice: the warps split the slice's steps, so a level with few slices still
-// keeps every SM busy.
-template <typename T, int LPR>
-__global__ void __launch_bounds__(kSweepWarps * 32) k_fwd(SellDev Lm, int32_t s0, int32_t s1,
-                                                          const T* __restrict__ vals,
-                                                          const T* __restrict__ D, int32_t nb,
-                                                          const T* __restrict__ r, T* y,
-                                                          const PcgScalars* s) {
-    __shared__ T red[kSweepWarps - 1][32][3];
-    if (s->done) return;
-    const int lane = threadIdx.x & 31, rr = lane / LPR, q = lane % LPR;
-    constexpr int S = 32 / LPR;
-    for (int32_t sl = s0 + (int32_t)blockIdx.x; sl < s1; sl += (int32_t)gridDim.x) {
-        T a0, a1, a2;
-        slice_accum_cta<T>(vals, Lm.col, Lm.off[sl], Lm.off[sl + 1], y, red, a0, a1, a2);
-        if (threadIdx.x < 32) {
-            row_reduce<T, LPR>(a0, a1, a2);
-            const int32_t row = Lm.rowid[(int64_t)sl * S + rr];
-            if (q == 0 && row >= 0) {
-                T r0, r1, r2;
-                node3(r, row, r0, r1, r2);
-                const T u0 = r0 - a0, u1 = r1 - a1, u2 = r2 - a2;
-                const T* d = D + row;
-                const T y0 = d[0] * u0;
-                const T y1 = d[3 * (int64_t)nb] * u0 + d[4 * (int64_t)nb] * u1;
-                const T y2 = d[6 * (int64_t)nb] * u0 + d[7 * (int64_t)nb] * u1 + d[8 * (int64_t)nb] * u2;
-                store_node(y, row, y0, y1, y2);
-            }
-        }
-    }
-}
-
-// One level of the backward sweep z_I = L_II^-T (y_I - sum_{J>I} L_JI^T z_J), in place over y
-// (Csr::precondition, iterative.rs:180-186, as a gather on the stored upper blocks L_JI^T), with
-// r . z partials; the last launch (level 0) sets beta = rz_new / rz, rz = rz_new
-// (iterative.rs:237-239). One block per slice, as in the forward sweep.
-template <typename T, int LPR>
-__global__ void __launch_bounds__(kSweepWarps * 32) k_bwd(SellDev Um, int32_t s0, int32_t s1,
-                                                          int level, int nlevels,
-                                                          const T* __restrict__ vals,
-                                                          const T* __restrict__ D, int32_t nb,
-                                                          const T* __restrict__ r, T* z,
-                                                          PcgScalars* s, double* partials,
-                                                          double* lvl_total) {
-    __shared__ T red[kSweepWarps - 1][32][3];
-    __shared__ double sh[kSweepWarps];
-    if (s->done) return;
-    const int lane = threadIdx.x & 31, rr = lane / LPR, q = lane % LPR;
-    constexpr int S = 32 / LPR;
-    double loc = 0.0;
-    for (int32_t sl = s0 + (int32_t)blockIdx.x; sl < s1; sl += (int32_t)gridDim.x) {
-        T a0, a1, a2;
-        slice_accum_cta<T>(vals, Um.col, Um.off[sl], Um.off[sl + 1], z, red, a0, a1, a2);
-        if (threadIdx.x < 32) {
-            row_reduce<T, LPR>(a0, a1, a2);
-            const int32_t row = Um.rowid[(int64_t)sl * S + rr];
-            if (q == 0 && row >= 0) {
-                T y0, y1, y2;
-                node3_rw(z, row, y0, y1, y2);
-                const T u0 = y0 - a0, u1 = y1 - a1, u2 = y2 - a2;
-                const T* d = D + row;
-                const T z0 = d[0] * u0 + d[3 * (int64_t)nb] * u1 + d[6 * (int64_t)nb] * u2;
-                const T z1 = d[4 * (int64_t)nb] * u1 + d[7 * (int64_t)nb] * u2;
-                const T z2 = d[8 * (int64_t)nb] * u2;
-                store_node(z, row, z0, z1, z2);
-                T r0, r1, r2;
-                node3(r, row, r0, r1, r2);
-                loc += (double)r0 * (double)z0 + (double)r1 * (double)z1 + (double)r2 * (double)z2;
-            }
-        }
-    }
-    if (publish_partial(loc, partials, &s->ticket[2], sh)) {
-        const double tot = gather_sum(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            lvl_total[level] = tot;
-            s->ticket[2] = 0;
-        }
-        if (level == 0) {
-            const double rz = gather_sum(lvl_total, nlevels, sh);
-            if (threadIdx.x == 0) {
-                s->beta = (s->iter == 0) ? 0.0 : rz / s->rz;
-                s->rz = rz;
-            }
-        }
-    }
-}
-
-// p = z + beta p (iterative.rs:240-242)
-template <typename T>
-__global__ void k_pupdate(int32_t nb, const T* __restrict__ z, T* __restrict__ p, PcgScalars* s) {
-    if (s->done) return;
-    const double beta = s->beta;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const F4 zv = ld4(z, i);
-        F4 pv = ld4(p, i);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) pv.v[c] = zv.v[c] + beta * pv.v[c];
-        st4(p, i, pv);
     }
 }
 
@@ -513,59 +268,6 @@ void launch_spmv(const SellDev& A, const T* vals, const T* p, T* ap, PcgScalars*
     MAILLE_LPR_SWITCH(A.lpr, k_spmv, grid, kThr, 0, st>>>(A, vals, p, ap, s, partials, standalone ? 1 : 0));
 }
 
-template <typename T>
-void launch_axpy(int32_t nb, T* x, T* r, const T* p, const T* ap, PcgScalars* s, double* partials,
-                 bool mixed, cudaStream_t st) {
-    counted();
-    k_axpy<T><<<grid_for(nb, kThr, 148 * 16), kThr, 0, st>>>(nb, x, r, p, ap, s, partials, mixed ? 1 : 0);
-}
-
-void launch_upd_x(int32_t nb, double* x64, float* x32, PcgScalars* s, cudaStream_t st) {
-    counted();
-    k_upd_x<<<grid_for(nb, kThr, 148 * 16), kThr, 0, st>>>(nb, x64, x32, s);
-}
-
-void launch_upd_r(const SellDev& A, const double* vals, const double* b, const double* x64,
-                  double* r64, PcgScalars* s, double* partials, int grid, cudaStream_t st) {
-    counted();
-    using T = double;
-    (void)sizeof(T);
-    switch (A.lpr) {
-        case 1: k_upd_r<1><<<grid, kThr, 0, st>>>(A, vals, b, x64, r64, s, partials); break;
-        case 2: k_upd_r<2><<<grid, kThr, 0, st>>>(A, vals, b, x64, r64, s, partials); break;
-        case 4: k_upd_r<4><<<grid, kThr, 0, st>>>(A, vals, b, x64, r64, s, partials); break;
-        default: k_upd_r<8><<<grid, kThr, 0, st>>>(A, vals, b, x64, r64, s, partials); break;
-    }
-}
-
-void launch_upd_cast(int32_t nb, const double* r64, float* r32, PcgScalars* s, cudaStream_t st) {
-    counted();
-    k_upd_cast<<<grid_for(nb, kThr, 148 * 16), kThr, 0, st>>>(nb, r64, r32, s);
-}
-
-template <typename T>
-void launch_fwd(const SellDev& L, int32_t s0, int32_t s1, const T* vals, const T* D, int32_t nb,
-                const T* r, T* y, PcgScalars* s, cudaStream_t st) {
-    counted();
-    const int grid = grid_for(s1 - s0, 1, 148 * 16);
-    MAILLE_LPR_SWITCH(L.lpr, k_fwd, grid, kSweepWarps * 32, 0, st>>>(L, s0, s1, vals, D, nb, r, y, s));
-}
-
-template <typename T>
-void launch_bwd(const SellDev& U, int32_t s0, int32_t s1, int level, int nlevels, const T* vals,
-                const T* D, int32_t nb, const T* r, T* z, PcgScalars* s, double* partials,
-                double* lvl_total, cudaStream_t st) {
-    counted();
-    const int grid = grid_for(s1 - s0, 1, 148 * 16);
-    MAILLE_LPR_SWITCH(U.lpr, k_bwd, grid, kSweepWarps * 32, 0, st>>>(U, s0, s1, level, nlevels, vals, D, nb, r, z, s, partials, lvl_total));
-}
-
-template <typename T>
-void launch_pupdate(int32_t nb, const T* z, T* p, PcgScalars* s, cudaStream_t st) {
-    counted();
-    k_pupdate<T><<<grid_for(nb, kThr, 148 * 16), kThr, 0, st>>>(nb, z, p, s);
-}
-
 void launch_pcg_init(PcgScalars* s, double tol, int32_t max_iter, double delta, cudaStream_t st) {
     counted();
     k_pcg_init<<<1, 1, 0, st>>>(s, tol, max_iter, delta);
@@ -611,14 +313,6 @@ void launch_cast(int64_t n, const double* a, float* b, cudaStream_t st) {
 #define MAILLE_INST(T)                                                                          \
     template void launch_spmv<T>(const SellDev&, const T*, const T*, T*, PcgScalars*, double*,  \
                                  int, bool, cudaStream_t);                                      \
-    template void launch_axpy<T>(int32_t, T*, T*, const T*, const T*, PcgScalars*, double*,     \
-                                 bool, cudaStream_t);                                           \
-    template void launch_fwd<T>(const SellDev&, int32_t, int32_t, const T*, const T*, int32_t, \
-                                const T*, T*, PcgScalars*, cudaStream_t);                       \
-    template void launch_bwd<T>(const SellDev&, int32_t, int32_t, int, int, const T*, const T*, \
-                                int32_t, const T*, T*, PcgScalars*, double*, double*,          \
-                                cudaStream_t);                                                  \
-    template void launch_pupdate<T>(int32_t, const T*, T*, PcgScalars*, cudaStream_t);          \
     template void launch_norm2<T>(int64_t, const T*, double*, unsigned int*, double*,           \
                                   cudaStream_t);                                                \
     template void launch_sell_fill<T>(int64_t, const int32_t*, const double*, T*, cudaStream_t); \

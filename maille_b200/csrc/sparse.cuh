@@ -1,4 +1,4 @@
-// sparse.cuh -- sliced 3x3-block layout (SELL) and the PCG kernels that run on it.
+// sparse.cuh -- sliced 3x3-block layouts (SELL for K, packed for the factor) and the PCG kernels.
 //
 // Layout. Rows of one level are cut into warp slices of 32/lpr rows (lpr = lanes per row); in a
 // slice every step holds 128 slots, 4 consecutive slots per lane, so a lane reads the 9 values
@@ -28,6 +28,17 @@ struct SellDev {
     const int32_t* col;     // [steps * 128] node column of each slot
 };
 
+// Packed layout of a strictly lower or upper factor (PsellHost in common.hpp): one-step slices of
+// whole rows (a row may span lanes), row starts marked in a 128-bit mask per slice.
+struct PsellDev {
+    int32_t nslices;
+    const int64_t* off;    // [nslices + 1] first step of each slice
+    const int32_t* col;    // [steps * 128] node column of each slot
+    const uint4* head;     // [nslices] row-start bits of the 128 slots
+    const int32_t* row0;   // [nslices + 1] first packed row of each slice
+    const int32_t* rows;   // [nb] matrix row of each packed row
+};
+
 // Device-resident scalars of one PCG run.
 struct PcgScalars {
     double alpha, beta, rz, rr, bb, tol, pap;
@@ -41,22 +52,6 @@ struct PcgScalars {
 template <typename T>
 void launch_spmv(const SellDev& A, const T* vals, const T* p, T* ap, PcgScalars* s,
                  double* partials, int grid, bool standalone, cudaStream_t st);
-template <typename T>
-void launch_axpy(int32_t nb, T* x, T* r, const T* p, const T* ap, PcgScalars* s,
-                 double* partials, bool mixed, cudaStream_t st);
-void launch_upd_x(int32_t nb, double* x64, float* x32, PcgScalars* s, cudaStream_t st);
-void launch_upd_r(const SellDev& A, const double* vals, const double* b, const double* x64,
-                  double* r64, PcgScalars* s, double* partials, int grid, cudaStream_t st);
-void launch_upd_cast(int32_t nb, const double* r64, float* r32, PcgScalars* s, cudaStream_t st);
-template <typename T>
-void launch_fwd(const SellDev& L, int32_t s0, int32_t s1, const T* vals, const T* D, int32_t nb,
-                const T* r, T* y, PcgScalars* s, cudaStream_t st);
-template <typename T>
-void launch_bwd(const SellDev& U, int32_t s0, int32_t s1, int level, int nlevels, const T* vals,
-                const T* D, int32_t nb, const T* r, T* z, PcgScalars* s, double* partials,
-                double* lvl_total, cudaStream_t st);
-template <typename T>
-void launch_pupdate(int32_t nb, const T* z, T* p, PcgScalars* s, cudaStream_t st);
 void launch_pcg_init(PcgScalars* s, double tol, int32_t max_iter, double delta, cudaStream_t st);
 template <typename T>
 void launch_norm2(int64_t n, const T* v, double* partials, unsigned int* ticket, double* out,
@@ -77,25 +72,21 @@ void launch_cast(int64_t n, const double* a, float* b, cudaStream_t st);
 template <typename T>
 struct PcgArgs {
     int32_t nb, levels, chunk;
-    SellDev K, L, U;
-    const int32_t* lvl_l;  // [levels + 1] slice ranges of the L layout per level
-    const int32_t* lvl_u;
+    SellDev K;
+    PsellDev L, U;
     const T *Kv, *Lv, *Uv, *D;
+    // padded vectors (4 entries per node); z holds the sweep records (z0, z1, z2, tag)
     T *x, *r, *z, *p, *ap;
     const double* K64;  // mixed form: FP64 matrix, right-hand side, solution, true residual
     const double* b64;
     double *x64, *r64;
     PcgScalars* s;
-    // dataflow sweeps: slice claim counters, row-ready flags ([nb + 1], monotonic epochs) and the
-    // order in which the backward sweep claims the U slices (levels descending)
-    int32_t* claim;
-    unsigned int* flags;
-    const int32_t* bwd_seq;
+    int32_t* claim;  // claim[2]: the sweeps' timeout flag
     double* partials;       // [4 * grid]
     unsigned long long* timing;  // optional [8] ns per phase (block 0): spmv, axpy, update, fwd, bwd, p
 };
 template <typename T, bool MIXED>
-int pcg_persistent_grid(int lprk, int lprlu);
+int pcg_persistent_grid(int lprk);
 template <typename T, bool MIXED>
 cudaError_t launch_pcg_persistent(const PcgArgs<T>& a, int grid, bool init, cudaStream_t st);
 
