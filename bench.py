@@ -373,6 +373,13 @@ def pcg_bytes_per_iteration(blocks, nb, vb):
     return matrix + vectors
 
 
+# DRAM traffic of the persistent PCG kernel per iteration over its algorithmic bytes, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum of one 8-iteration launch, Tet10 30^3,
+# profiles/k_pcg_tet10_30_full.md: 0.587 GB against 0.560 GB); traffic grows with the blocks, so
+# the ratio scales the capture to the benchmark size.
+PCG_TRAFFIC_RATIO = 0.587 / 0.560
+
+
 def cpu_baseline(p, tol, iterations_needed, max_iter=5):
     """The CPU oracle (single-thread restatement of the reference path) on the full workload:
     element integration + assembly + RCM + IC(0) + `max_iter` PCG iterations timed, the PCG part
@@ -589,7 +596,9 @@ def run_ours(args):
                      "achieved": pcg_gbs, "peak": hbm, "unit": "GB/s", "frac": pcg_gbs / hbm,
                      "peak_kind": peak_kind, "bytes_per_iteration": it_bytes,
                      "ms_per_iteration": info_m["ms_solve"] / info_m["iterations"],
-                     "traffic": None},
+                     "traffic": PCG_TRAFFIC_RATIO * it_bytes,
+                     "traffic_note": "bytes per iteration, ncu DRAM bytes of a Tet10 30^3 launch "
+                                     "scaled by blocks (profiles/k_pcg_tet10_30_full.md)"},
         "spmv": {"kernel": "k_spmv<float> (SELL 3x3-block SpMV, FP32, standalone)",
                  "achieved": gbs32, "frac": gbs32 / hbm, "bytes_per_launch": bytes32,
                  "ms_per_launch": ms32,

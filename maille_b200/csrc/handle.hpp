@@ -83,7 +83,7 @@ struct MailleGpuHandle {
     int precision = MAILLE_FP64;
     double tol = kDefaultTol;
     int32_t max_iter = kDefaultMaxIter;
-    double delta = 0.1;  // reliable update when the FP32 residual fell by this factor
+    double delta = 0.3;  // reliable update when the FP32 residual fell by this factor
     std::vector<uint8_t> h_fixed;
     std::vector<double> h_f, h_f0, h_imposed;
     bool any_imposed = false;
