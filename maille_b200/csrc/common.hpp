@@ -46,6 +46,7 @@ struct Symbolic {
     int64_t blocks = 0;
     // deterministic assembly: lower slots (col <= row), each summing a sorted list of element
     // node-pair blocks. contrib entry = (e * npairs + pair) | (transpose << 31)
+    int64_t nl = 0;                    // lower slots
     std::vector<int64_t> lslot;        // [NL] position of the lower slot in the full pattern
     std::vector<int64_t> lptr;         // [NL + 1]
     std::vector<uint32_t> contrib;     // [pairs kept]
@@ -63,11 +64,12 @@ struct Symbolic {
 // level rows are taken by decreasing length. src maps each slot to its block in the CSR
 // pattern (-1 for padding), so the numeric values are filled by one gather per assembly.
 // Padding slots point at column nb, a dummy node whose vector entries stay 0.
+// Plan of the sliced layout of K (the slot columns and CSR sources are filled on the device from
+// the plan and the pattern: fill_sell in analysis.cu).
 struct SellHost {
     int32_t lpr = 1;
     std::vector<int32_t> rowid;         // [nslices * 32 / lpr], -1 when empty
     std::vector<int64_t> off{0};        // [nslices + 1] first step of each slice
-    std::vector<int32_t> col, src;      // [steps * 128]
     std::vector<int32_t> level_slices;  // [levels + 1]
     int64_t steps() const { return off.back(); }
     int32_t nslices() const { return (int32_t)off.size() - 1; }
@@ -85,12 +87,13 @@ enum SellKind { SELL_FULL = 0, SELL_LOWER = 1, SELL_UPPER = 2 };
 // slice s, in slot order, are rows[row0[s] .. row0[s + 1]). Slices are stored in sweep order:
 // levels ascending for L (forward sweep), descending for U (backward sweep); level_slices[q] is
 // the first slice of the q-th level swept.
+// (Plan only: the slot columns and CSR sources are filled on the device, fill_psell.)
 struct PsellHost {
     std::vector<int64_t> off{0};        // [nslices + 1] first step of each slice
-    std::vector<int32_t> col, src;      // [steps * 128] node column / CSR block of each slot
     std::vector<uint32_t> head;         // [nslices * 4] row-start bits
     std::vector<int32_t> row0{0};       // [nslices + 1]
     std::vector<int32_t> rows;          // [nb] matrix row of each packed row
+    std::vector<int64_t> rstart;        // [nb] first slot of each packed row
     std::vector<int32_t> level_slices;  // [levels + 1]
     int64_t steps() const { return off.back(); }
     int32_t nslices() const { return (int32_t)off.size() - 1; }
@@ -119,16 +122,20 @@ struct BSellHost {
 void build_bsell(const Symbolic& s, SellKind kind, int rows, int sub, const std::vector<int32_t>& group,
                  BSellHost& out);
 
-// Builds the sliced layout of one part of the analysed pattern. lpr <= 0 picks lanes per row
-// from the mean row length.
+// Plans the sliced layout of one part of the analysed pattern (reads s.row_ptr, s.diag and the
+// levels only). lpr <= 0 picks lanes per row from the mean row length.
 void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out);
 
-// Builds the packed layout of the strictly lower (SELL_LOWER) or upper (SELL_UPPER) blocks.
+// Plans the packed layout of the strictly lower (SELL_LOWER) or upper (SELL_UPPER) blocks (reads
+// s.row_ptr, s.diag and the levels only).
 void build_psell(const Symbolic& s, SellKind kind, PsellHost& out);
 
-// Builds the symbolic analysis. conn is [n_elems * npe] in the caller's node numbering.
+// Builds the symbolic analysis. conn is [n_elems * npe] in the caller's node numbering. With
+// pattern = false it stops after the ordering, the levels and the boundary lists (perm, inv,
+// fixmask, level_ptr, incidence, belem, bnodes): the block pattern and the scatter map are then
+// built on the device (analysis.cu).
 bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
-             const uint8_t* fixed, int ordering, Symbolic& s, Error& err);
+             const uint8_t* fixed, int ordering, Symbolic& s, Error& err, bool pattern = true);
 
 // Face pressure loads f_a -= p * integral(N_a n dS) added into f (assembly.rs:650-674 with the
 // tet branch of face_rule, assembly.rs:556-585). Host-side: part of the host program's assemble.

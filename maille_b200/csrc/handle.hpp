@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 
+#include "analysis.cuh"
 #include "common.hpp"
 #include "cuda_host.hpp"
 #include "kernels.cuh"
@@ -17,7 +18,8 @@
 // the handle types live at global scope (the C ABI names them); their members are library types
 using namespace maille;
 
-// A sliced layout: host description (level slices) plus its device index arrays.
+// A sliced layout: host plan (level slices) plus its device index arrays; the slot columns and
+// CSR sources are filled on the device from the plan and the device pattern.
 struct SellBuf {
     SellHost h;
     int32_t* rowid = nullptr;
@@ -25,11 +27,13 @@ struct SellBuf {
     int32_t* col = nullptr;
     int32_t* src = nullptr;
     SellDev dev() const { return SellDev{h.lpr, h.nslices(), rowid, off, col}; }
-    void upload(cudaStream_t st) {
+    void upload(const PatternDev& pt, int32_t nb, cudaStream_t st) {
         rowid = dupload(h.rowid.data(), h.rowid.size(), st);
         off = dupload(h.off.data(), h.off.size(), st);
-        col = dupload(h.col.data(), h.col.size(), st);
-        src = dupload(h.src.data(), h.src.size(), st);
+        col = dalloc<int32_t>((size_t)h.steps() * 128);
+        src = dalloc<int32_t>((size_t)h.steps() * 128);
+        fill_sell(SELL_FULL, h.lpr, h.nslices(), h.steps(), rowid, off, pt.row_ptr, pt.col, pt.diag,
+                  nb, col, src, st);
     }
     void release() {
         for (void* p : {(void*)rowid, (void*)off, (void*)col, (void*)src})
@@ -44,6 +48,7 @@ struct SellBuf {
 // A packed layout of a factor triangle: host description plus its device arrays.
 struct PsellBuf {
     PsellHost h;
+    SellKind kind = SELL_LOWER;
     int64_t* off = nullptr;
     int32_t* col = nullptr;
     int32_t* src = nullptr;
@@ -53,13 +58,18 @@ struct PsellBuf {
     PsellDev dev() const {
         return PsellDev{h.nslices(), off, col, reinterpret_cast<const uint4*>(head), row0, rows};
     }
-    void upload(cudaStream_t st) {
+    void upload(const PatternDev& pt, int32_t nb, cudaStream_t st) {
         off = dupload(h.off.data(), h.off.size(), st);
-        col = dupload(h.col.data(), h.col.size(), st);
-        src = dupload(h.src.data(), h.src.size(), st);
         head = dupload(h.head.data(), h.head.size(), st);
         row0 = dupload(h.row0.data(), h.row0.size(), st);
         rows = dupload(h.rows.data(), h.rows.size(), st);
+        int64_t* rstart = dupload(h.rstart.data(), h.rstart.size(), st);
+        col = dalloc<int32_t>((size_t)h.steps() * 128);
+        src = dalloc<int32_t>((size_t)h.steps() * 128);
+        fill_psell(kind, (int64_t)h.rows.size(), h.steps(), rows, rstart, pt.row_ptr, pt.col, pt.diag,
+                   nb, col, src, st);
+        CK(cudaStreamSynchronize(st));
+        cudaFree(rstart);
     }
     void release() {
         for (void* p : {(void*)off, (void*)col, (void*)src, (void*)head, (void*)row0, (void*)rows})

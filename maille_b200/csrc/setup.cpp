@@ -141,10 +141,30 @@ std::vector<int32_t> greedy_colour(const NodeGraph& g, const std::vector<int32_t
     return colour;
 }
 
+// elements touching a fixed DOF, and the nodes with a fixed DOF they contain
+void boundary(Symbolic& s, int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
+              const uint8_t* fixed) {
+    if (!fixed) return;
+    std::vector<uint8_t> bn(n_nodes, 0);
+    for (int64_t e = 0; e < n_elems; ++e) {
+        bool any = false;
+        for (int a = 0; a < npe && !any; ++a) {
+            const int64_t v = conn[e * npe + a];
+            any = fixed[3 * v] || fixed[3 * v + 1] || fixed[3 * v + 2];
+        }
+        if (any) {
+            s.belem.push_back((int32_t)e);
+            for (int a = 0; a < npe; ++a) bn[conn[e * npe + a]] = 1;
+        }
+    }
+    for (int64_t v = 0; v < n_nodes; ++v)
+        if (bn[v]) s.bnodes.push_back((int32_t)v);
+}
+
 }  // namespace
 
 bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
-             const uint8_t* fixed, int ordering, Symbolic& s, Error& err) {
+             const uint8_t* fixed, int ordering, Symbolic& s, Error& err, bool pattern) {
     const double t0 = now_ms();
     if (npe != 4 && npe != 10) {
         err = {MAILLE_INVALID_INPUT, "nodes_per_elem must be 4 or 10"};
@@ -207,9 +227,9 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
     NodeGraph g;
     g.off.assign(nk + 1, 0);
     {
-        std::vector<int32_t> mark(nk, -1);
-        g.adj.reserve((size_t)nk * (npe == 4 ? 15 : 28));
-        for (int32_t k = 0; k < nk; ++k) {
+        // neighbours of each kept node in element-encounter order, deduplicated with a per-thread
+        // mark array: a counting pass, then a filling pass
+        auto visit = [&](int32_t k, std::vector<int32_t>& mark, auto&& fn) {
             const int32_t v = kept[k];
             mark[k] = k;
             for (int64_t q = s.inc_ptr[v]; q < s.inc_ptr[v + 1]; ++q) {
@@ -218,19 +238,36 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
                     const int32_t w = kept_of[conn[e * npe + a]];
                     if (w >= 0 && mark[w] != k) {
                         mark[w] = k;
-                        g.adj.push_back(w);
+                        fn(w);
                     }
                 }
             }
-            g.off[k + 1] = (int64_t)g.adj.size();
-        }
+        };
+        parallel_for(nk, [&](int64_t k0, int64_t k1) {
+            std::vector<int32_t> mark(nk, -1);
+            for (int64_t k = k0; k < k1; ++k) {
+                int64_t c = 0;
+                visit((int32_t)k, mark, [&](int32_t) { ++c; });
+                g.off[k + 1] = c;
+            }
+        });
+        for (int32_t k = 0; k < nk; ++k) g.off[k + 1] += g.off[k];
+        g.adj.resize(g.off[nk]);
+        parallel_for(nk, [&](int64_t k0, int64_t k1) {
+            std::vector<int32_t> mark(nk, -1);
+            for (int64_t k = k0; k < k1; ++k) {
+                int64_t q = g.off[k];
+                visit((int32_t)k, mark, [&](int32_t w) { g.adj[q++] = w; });
+            }
+        });
     }
 
     stage("graph");
     // ordering over kept nodes: order[new] = kept index
     std::vector<int32_t> order = rcm(g);
+    std::vector<int32_t> colour;
     if (ordering != MAILLE_ORDER_RCM) {
-        std::vector<int32_t> colour = greedy_colour(g, order);
+        colour = greedy_colour(g, order);
         std::vector<int32_t> rank(nk);
         for (int32_t r = 0; r < nk; ++r) rank[order[r]] = r;
         std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
@@ -238,9 +275,20 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
         });
     }
     stage("ordering");
-    // levels of the lower-triangular dependency graph in that order, then group rows by level
-    // (a topological renumbering leaves the IC(0) factor unchanged)
-    {
+    if (!colour.empty()) {
+        // Multicolour order: a row's lower neighbours are exactly its neighbours of smaller
+        // colours, and greedy colouring gives a node colour c only when its earlier-visited
+        // neighbours hold every colour below c, so the level of each row is its colour and the
+        // rows are already grouped by level.
+        int32_t nc = 0;
+        for (int32_t k = 0; k < nk; ++k) nc = std::max(nc, colour[k] + 1);
+        s.levels = nc;
+        s.level_ptr.assign(s.levels + 1, 0);
+        for (int32_t k = 0; k < nk; ++k) s.level_ptr[colour[k] + 1]++;
+        for (int32_t l = 0; l < s.levels; ++l) s.level_ptr[l + 1] += s.level_ptr[l];
+    } else {
+        // levels of the lower-triangular dependency graph in that order, then group rows by
+        // level (a topological renumbering leaves the IC(0) factor unchanged)
         std::vector<int32_t> rank(nk), level(nk, 0);
         for (int32_t r = 0; r < nk; ++r) rank[order[r]] = r;
         int32_t maxl = 0;
@@ -274,6 +322,13 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
     }
 
     stage("levels");
+    if (!pattern) {
+        g = NodeGraph{};
+        boundary(s, n_nodes, npe, n_elems, conn, fixed);
+        stage("boundary");
+        s.ms = now_ms() - t0;
+        return true;
+    }
     // full block pattern in new numbering (neighbours + the diagonal), columns ascending
     s.row_ptr.assign(nk + 1, 0);
     for (int32_t r = 0; r < nk; ++r) {
@@ -358,25 +413,10 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
             visit_row((int32_t)r, slotmap, [&](int32_t ls, uint32_t c) { s.contrib[cur[ls]++] = c; });
         }
     });
+    s.nl = nl;
 
     stage("scatter map");
-    // elements touching a fixed DOF, and the nodes with a fixed DOF they contain
-    if (fixed) {
-        std::vector<uint8_t> bn(N, 0);
-        for (int64_t e = 0; e < n_elems; ++e) {
-            bool any = false;
-            for (int a = 0; a < npe && !any; ++a) {
-                const int64_t v = conn[e * npe + a];
-                any = fixed[3 * v] || fixed[3 * v + 1] || fixed[3 * v + 2];
-            }
-            if (any) {
-                s.belem.push_back((int32_t)e);
-                for (int a = 0; a < npe; ++a) bn[conn[e * npe + a]] = 1;
-            }
-        }
-        for (int32_t v = 0; v < N; ++v)
-            if (bn[v]) s.bnodes.push_back(v);
-    }
+    boundary(s, n_nodes, npe, n_elems, conn, fixed);
     stage("boundary");
     s.ms = now_ms() - t0;
     return true;
@@ -411,22 +451,8 @@ void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out) {
             int64_t maxlen = 0;
             for (size_t k = c0; k < c1; ++k) maxlen = std::max<int64_t>(maxlen, end(rows[k]) - start(rows[k]));
             const int64_t steps = (maxlen + per_step - 1) / per_step;
-            const int64_t g0 = out.off.back();
-            out.off.push_back(g0 + steps);
-            out.col.resize((size_t)(g0 + steps) * 128, s.nb);  // padding: the dummy zero node
-            out.src.resize((size_t)(g0 + steps) * 128, -1);
+            out.off.push_back(out.off.back() + steps);
             for (int r = 0; r < S; ++r) out.rowid.push_back(c0 + r < c1 ? rows[c0 + r] : -1);
-            for (size_t k = c0; k < c1; ++k) {
-                const int32_t i = rows[k];
-                const int r = (int)(k - c0);
-                for (int64_t p = start(i), b = 0; p < end(i); ++p, ++b) {
-                    const int64_t t = b / per_step, rem = b % per_step;
-                    const int64_t lane = r * lpr + rem / 4, j = rem % 4;
-                    const size_t slot = (size_t)(g0 + t) * 128 + 4 * lane + j;
-                    out.col[slot] = s.col[p];
-                    out.src[slot] = (int32_t)p;
-                }
-            }
         }
         out.level_slices.push_back(out.nslices());
     }
@@ -447,19 +473,13 @@ void build_psell(const Symbolic& s, SellKind kind, PsellHost& out) {
         const int64_t len0 = end(open[0]) - start(open[0]);
         const int64_t steps = open.size() == 1 && len0 > kSlots ? (len0 + kSlots - 1) / kSlots : 1;
         out.off.push_back(g0 + steps);
-        out.col.resize((size_t)(g0 + steps) * kSlots, s.nb);  // padding: the dummy zero node
-        out.src.resize((size_t)(g0 + steps) * kSlots, -1);
         uint32_t head[4] = {0, 0, 0, 0};
         int64_t slot = 0;
         for (int32_t i : open) {
             head[slot >> 5] |= 1u << (slot & 31);
-            const int64_t n = end(i) - start(i);
-            for (int64_t b = 0; b < n; ++b) {
-                out.col[(size_t)(g0 * kSlots + slot + b)] = s.col[start(i) + b];
-                out.src[(size_t)(g0 * kSlots + slot + b)] = (int32_t)(start(i) + b);
-            }
-            slot += std::max<int64_t>(1, n);
             out.rows.push_back(i);
+            out.rstart.push_back(g0 * kSlots + slot);
+            slot += std::max<int64_t>(1, end(i) - start(i));
         }
         for (uint32_t w : head) out.head.push_back(w);
         out.row0.push_back((int32_t)out.rows.size());

@@ -265,7 +265,7 @@ int32_t numeric_phase(MailleGpuHandle* h, Error& err) {
 int32_t assemble_factor(MailleGpuHandle* h, Error& err) {
     const Symbolic& s = h->sym;
     cudaStream_t st = h->st;
-    launch_assemble(h->pattern(), (int64_t)s.lslot.size(), h->lslot, h->lrow, h->lptr, h->contrib,
+    launch_assemble(h->pattern(), s.nl, h->lslot, h->lrow, h->lptr, h->contrib,
                     h->ke, h->K, st);
     launch_sell_fill<double>(h->sk.h.steps(), h->sk.src, h->K, h->Ks64, st);
     CK(cudaGetLastError());
@@ -319,20 +319,13 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
     h->h_f.assign(n3, 0.0);
     if (p->f) std::memcpy(h->h_f.data(), p->f, n3 * sizeof(double));
 
+    // host: ordering, levels and boundary lists; the pattern and scatter map are built on the
+    // device below (analysis.cu)
     const double t_setup0 = now_ms();
     if (!analyse(p->n_nodes, p->nodes_per_elem, p->n_elems, p->conn, h->h_fixed.data(), p->ordering,
-                 h->sym, err))
+                 h->sym, err, /*pattern=*/false))
         return fail(err);
     if (h->sym.levels >= kMaxLevels) return fail({MAILLE_INVALID_INPUT, "too many IC(0) levels"});
-    {
-        // the three layouts are independent: build them side by side
-        const int lk = env_int("MAILLE_LPR_K", 0);
-        std::thread tk([&] { build_sell(h->sym, SELL_FULL, lk, h->sk.h); });
-        std::thread tl([&] { build_psell(h->sym, SELL_LOWER, h->pl.h); });
-        build_psell(h->sym, SELL_UPPER, h->pu.h);
-        tk.join();
-        tl.join();
-    }
     const double t_setup1 = now_ms();
     try {
         int ndev = 0;
@@ -362,20 +355,32 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         h->perm = dupload(s.perm.data(), s.perm.size(), st);
         h->inv = dupload(s.inv.data(), s.inv.size(), st);
         h->fixmask = dupload(s.fixmask.data(), s.fixmask.size(), st);
-        h->row_ptr = dupload(s.row_ptr.data(), s.row_ptr.size(), st);
-        h->col = dupload(s.col.data(), s.col.size(), st);
-        h->diag = dupload(s.diag.data(), s.diag.size(), st);
-        h->tpos = dupload(s.tpos.data(), s.tpos.size(), st);
-        std::vector<int32_t> lrow(s.lslot.size());
         {
-            size_t q = 0;
-            for (int32_t r = 0; r < s.nb; ++r)
-                for (int64_t pp = s.row_ptr[r]; pp <= s.diag[r]; ++pp) lrow[q++] = r;
+            PatternDev pt;
+            gpu_pattern(h->npe, h->n_elems, h->conn, h->inv, s.nb, st, pt, h->sym.row_ptr, h->sym.diag);
+            h->row_ptr = pt.row_ptr;
+            h->col = pt.col;
+            h->diag = pt.diag;
+            h->tpos = pt.tpos;
+            h->lslot = pt.lslot;
+            h->lrow = pt.lrow;
+            h->lptr = pt.lptr;
+            h->contrib = pt.contrib;
+            h->sym.blocks = pt.blocks;
+            h->sym.nl = pt.nl;
+            // layout plans from the row lengths (host, side by side), slot fills on the device
+            const int lk = env_int("MAILLE_LPR_K", 0);
+            std::thread tk([&] { build_sell(h->sym, SELL_FULL, lk, h->sk.h); });
+            std::thread tl([&] { build_psell(h->sym, SELL_LOWER, h->pl.h); });
+            build_psell(h->sym, SELL_UPPER, h->pu.h);
+            tk.join();
+            tl.join();
+            h->pl.kind = SELL_LOWER;
+            h->pu.kind = SELL_UPPER;
+            h->sk.upload(pt, s.nb, st);
+            h->pl.upload(pt, s.nb, st);
+            h->pu.upload(pt, s.nb, st);
         }
-        h->lslot = dupload(s.lslot.data(), s.lslot.size(), st);
-        h->lrow = dupload(lrow.data(), lrow.size(), st);
-        h->lptr = dupload(s.lptr.data(), s.lptr.size(), st);
-        h->contrib = dupload(s.contrib.data(), s.contrib.size(), st);
         h->inc_ptr = dupload(s.inc_ptr.data(), s.inc_ptr.size(), st);
         h->inc = dupload(s.inc.data(), s.inc.size(), st);
         h->belem = dupload(s.belem.data(), s.belem.size(), st);
@@ -383,9 +388,6 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         std::vector<int32_t> slot(p->n_elems, -1);
         for (size_t k = 0; k < s.belem.size(); ++k) slot[s.belem[k]] = (int32_t)k;
         h->elem_slot = dupload(slot.data(), slot.size(), st);
-        h->sk.upload(st);
-        h->pl.upload(st);
-        h->pu.upload(st);
         // numeric buffers
         const int np = node_pairs(h->npe);
         const int64_t n4 = 4 * ((int64_t)s.nb + 1);  // + the dummy node that padding points at
