@@ -327,6 +327,16 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         return fail(err);
     if (h->sym.levels >= kMaxLevels) return fail({MAILLE_INVALID_INPUT, "too many IC(0) levels"});
     const double t_setup1 = now_ms();
+    // MAILLE_SETUP_TIMING: wall time of the device-side set-up steps (stream synchronised)
+    const bool stage_timing = std::getenv("MAILLE_SETUP_TIMING") != nullptr;
+    double t_mark = now_ms();
+    auto tmark = [&](const char* name) {
+        if (!stage_timing) return;
+        if (h->st) cudaStreamSynchronize(h->st);
+        const double t = now_ms();
+        std::fprintf(stderr, "maille create %-14s %8.1f ms\n", name, t - t_mark);
+        t_mark = t;
+    };
     try {
         int ndev = 0;
         CK(cudaGetDeviceCount(&ndev));
@@ -338,6 +348,7 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         cudaStream_t st = h->st;
         const Symbolic& s = h->sym;
         CK(cudaEventRecord(h->ev[0], st));
+        tmark("context");
         // inputs
         std::vector<int32_t> conn32(p->n_elems * p->nodes_per_elem);
         for (size_t k = 0; k < conn32.size(); ++k) conn32[k] = (int32_t)p->conn[k];
@@ -355,6 +366,7 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         h->perm = dupload(s.perm.data(), s.perm.size(), st);
         h->inv = dupload(s.inv.data(), s.inv.size(), st);
         h->fixmask = dupload(s.fixmask.data(), s.fixmask.size(), st);
+        tmark("inputs");
         {
             PatternDev pt;
             gpu_pattern(h->npe, h->n_elems, h->conn, h->inv, s.nb, st, pt, h->sym.row_ptr, h->sym.diag);
@@ -368,6 +380,7 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
             h->contrib = pt.contrib;
             h->sym.blocks = pt.blocks;
             h->sym.nl = pt.nl;
+            tmark("pattern");
             // layout plans from the row lengths (host, side by side), slot fills on the device
             const int lk = env_int("MAILLE_LPR_K", 0);
             std::thread tk([&] { build_sell(h->sym, SELL_FULL, lk, h->sk.h); });
@@ -377,6 +390,7 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
             tl.join();
             h->pl.kind = SELL_LOWER;
             h->pu.kind = SELL_UPPER;
+            tmark("layout plans");
             h->sk.upload(pt, s.nb, st);
             h->pl.upload(pt, s.nb, st);
             h->pu.upload(pt, s.nb, st);
@@ -447,8 +461,10 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
             CK(cudaMemsetAsync(h->timing, 0, 8 * sizeof(unsigned long long), st));
         }
         h->persist_chunk = std::max(1, env_int("MAILLE_PERSIST_CHUNK", h->persist_chunk));
+        tmark("layouts+buffers");
         CK(cudaEventRecord(h->ev[1], st));
         if (numeric_phase(h.get(), err) != MAILLE_OK) return fail(err);
+        tmark("numeric");
         CK(cudaStreamSynchronize(st));
         if (res) {
             res->ms_setup = t_setup1 - t_setup0;
@@ -665,10 +681,17 @@ void maille_gpu_destroy(MailleGpuHandle* h) { delete h; }
 int32_t maille_gpu_elastic_solve(const MailleElasticProblem* problem, MailleElasticResult* result) {
     g_last_error.clear();
     MailleGpuHandle* h = nullptr;
+    const bool timing = std::getenv("MAILLE_SETUP_TIMING") != nullptr;
+    const double t0 = now_ms();
     int32_t s = create_impl(problem, &h, result);
     if (s != MAILLE_OK) return s;
+    const double t1 = now_ms();
     s = solve_impl(h, nullptr, result);
+    const double t2 = now_ms();
     delete h;
+    if (timing)
+        std::fprintf(stderr, "maille one-shot: create %.1f ms, solve %.1f ms, destroy %.1f ms\n", t1 - t0,
+                     t2 - t1, now_ms() - t2);
     return s;
 }
 
