@@ -147,6 +147,15 @@ int32_t maille_gpu_refactor(MailleGpuHandle* h, const double* young, const doubl
  * [3 n_nodes] in the caller's numbering; x is read at free DOFs, y is 0 at fixed DOFs. */
 int32_t maille_gpu_multiply(MailleGpuHandle* h, const double* x, double* y);
 
+/* Nodal stresses of the last solve (nodal_stresses / smooth, results.rs:137-230, and the
+ * `stress` / `von_mises` point arrays of maille-io/src/vtk/fields.rs:54-74): the Gauss-point
+ * stresses extrapolated to each element's nodes (Tet4: the point value; Tet10: the
+ * TET10_EXTRAPOLATION weights, results.rs:114-132) and averaged over the elements sharing a node,
+ * in element order; a node no element touches gets 0. stress: [6 n_nodes] (sxx, syy, szz, txy,
+ * tyz, txz per node), von_mises: [n_nodes] (Stress::von_mises of the smoothed stress). Needs a
+ * solve on the handle (MAILLE_INVALID_INPUT otherwise). */
+int32_t maille_gpu_nodal_stresses(MailleGpuHandle* h, double* stress, double* von_mises);
+
 /* Enqueues `count` launches of the PCG's 3x3-block SpMV kernel on the handle's device vectors
  * and stream (precision MAILLE_FP64 or MAILLE_MIXED for the FP32 matrix), without waiting: for
  * timing the kernel with events on maille_gpu_stream(). No counterpart in the reference. */

@@ -124,6 +124,7 @@ struct MailleGpuHandle {
     float *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *ap32 = nullptr;
     double *u_full = nullptr, *y_full = nullptr, *ye = nullptr, *gauss = nullptr, *vm = nullptr,
            *react = nullptr, *lambda_full = nullptr, *grad = nullptr;
+    double *node_stress = nullptr, *node_vm = nullptr;  // smoothed nodal stresses [6 n], von Mises [n]
     PcgScalars* scal = nullptr;
     PcgScalars* h_scal = nullptr;  // pinned
     double* partials = nullptr;

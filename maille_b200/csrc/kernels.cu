@@ -476,6 +476,62 @@ __global__ void k_stresses(ElemIn in, const double* __restrict__ u, double* __re
     }
 }
 
+// Nodal smoothing of the Gauss-point stresses (nodal_stresses / smooth, results.rs:137-230): each
+// element's Gauss values are extrapolated to its nodes (Tet4: the single point's value,
+// TET4_EXTRAPOLATION results.rs:98; Tet10: TET10_EXTRAPOLATION results.rs:118-132, the weights of
+// the 4 points for the 4 vertices and 6 mid-edge nodes) and averaged over the elements sharing
+// the node; a node no element touches gets 0. One thread per node gathers its incident elements in
+// element order (the incidence list is sorted by element), with separately rounded products and
+// sums in the reference's order, so the result equals the sequential accumulation exactly. Also
+// writes Stress::von_mises (results.rs:24-32) of the smoothed stress, in the reference's order.
+// gauss: [ne * ng * 9] (x, y, z, sxx, syy, szz, txy, tyz, txz); stress: [n * 6] (sxx, syy, szz,
+// txy, tyz, txz); vm: [n].
+// TET10_EXTRAPOLATION (results.rs:114-132): with the barycentric coordinates a = (5 + 3 sqrt 5) / 20,
+// b = (5 - sqrt 5) / 20 of TETRA_4's points, a vertex takes (3 sqrt 5 + 1) / 4 of its own point and
+// -(sqrt 5 - 1) / 4 of the others, a mid-edge node (sqrt 5 + 1) / 4 of the points of its two
+// vertices (Tet10 edge order 0-1, 1-2, 2-0, 0-3, 1-3, 2-3) and -(sqrt 5 - 1) / 4 of the others.
+__device__ __forceinline__ double tet10_extrapolation(int a, int g) {
+    constexpr double V = 1.9270509831248424, M = 0.8090169943749475, O = -0.30901699437494745;
+    if (a < 4) return g == a ? V : O;
+    constexpr int ei[6] = {0, 1, 2, 0, 1, 2}, ej[6] = {1, 2, 0, 3, 3, 3};
+    return (g == ei[a - 4] || g == ej[a - 4]) ? M : O;
+}
+
+__global__ void k_nodal_stresses(int npe, int64_t n_nodes, const int64_t* __restrict__ inc_ptr,
+                                 const int32_t* __restrict__ inc, const double* __restrict__ gauss,
+                                 double* __restrict__ stress, double* __restrict__ vm) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n_nodes) return;
+    const int ng = npe == 4 ? 1 : 4;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    const int64_t q0 = inc_ptr[v], q1 = inc_ptr[v + 1];
+    for (int64_t q = q0; q < q1; ++q) {
+        const int32_t k = inc[q];
+        const int64_t e = k / npe;
+        const int a = (int)(k - e * npe);
+        for (int g = 0; g < ng; ++g) {
+            const double w = npe == 4 ? 1.0 : tet10_extrapolation(a, g);
+            const double* p = gauss + (e * ng + g) * 9 + 3;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) s[c] = __dadd_rn(s[c], __dmul_rn(w, p[c]));
+        }
+    }
+    const double cnt = (double)(q1 - q0 > 0 ? q1 - q0 : 1);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        s[c] = __ddiv_rn(s[c], cnt);
+        stress[6 * v + c] = s[c];
+    }
+    const double a = s[0], b = s[1], c = s[2];
+    const double shear = __dadd_rn(__dadd_rn(__dmul_rn(s[3], s[3]), __dmul_rn(s[4], s[4])), __dmul_rn(s[5], s[5]));
+    double t = __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c));
+    t = __dsub_rn(t, __dmul_rn(a, b));
+    t = __dsub_rn(t, __dmul_rn(b, c));
+    t = __dsub_rn(t, __dmul_rn(c, a));
+    t = __dadd_rn(t, __dmul_rn(3.0, shear));
+    vm[v] = __dsqrt_rn(t > 0.0 ? t : 0.0);
+}
+
 // dJ/dE_e = -lambda_e^T (dK_e/dE_e) u_e = -lambda_e^T K_e u_e / E_e (K_e is linear in E_e).
 __global__ void k_adjoint_grad(int npe, int64_t ne, const int32_t* __restrict__ conn,
                                const double* __restrict__ ke, const double* __restrict__ young,
@@ -613,6 +669,13 @@ void launch_stresses(int npe, const ElemIn& in, const double* u, double* gauss, 
         k_stresses<4><<<blocks_for(in.ne * ng, 128, INT32_MAX), 128, 0, st>>>(in, u, gauss, vm);
     else
         k_stresses<10><<<blocks_for(in.ne * ng, 128, INT32_MAX), 128, 0, st>>>(in, u, gauss, vm);
+}
+
+void launch_nodal_stresses(int npe, int64_t n_nodes, const int64_t* inc_ptr, const int32_t* inc,
+                           const double* gauss, double* stress, double* vm, cudaStream_t st) {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    k_nodal_stresses<<<(unsigned)((n_nodes + 127) / 128), 128, 0, st>>>(npe, n_nodes, inc_ptr, inc, gauss,
+                                                                        stress, vm);
 }
 
 void launch_adjoint_grad(int npe, int64_t ne, const int32_t* conn, const double* ke_up,

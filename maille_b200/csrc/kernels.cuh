@@ -66,6 +66,9 @@ void launch_reactions(int64_t n_nodes, const int32_t* nodes, int64_t nnodes,
                       cudaStream_t st);
 void launch_stresses(int npe, const ElemIn& in, const double* u, double* gauss, double* vm,
                      cudaStream_t st);
+// smoothed nodal stresses [n * 6] and their von Mises values [n] from the Gauss stresses
+void launch_nodal_stresses(int npe, int64_t n_nodes, const int64_t* inc_ptr, const int32_t* inc,
+                           const double* gauss, double* stress, double* vm, cudaStream_t st);
 void launch_adjoint_grad(int npe, int64_t ne, const int32_t* conn, const double* ke_up,
                          const double* young, const double* lambda, const double* u,
                          double* grad, cudaStream_t st);

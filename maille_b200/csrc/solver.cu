@@ -53,7 +53,7 @@ MailleGpuHandle::~MailleGpuHandle() {
                     row_ptr, diag, tpos, lslot, lptr, contrib, inc_ptr, inc, belem, bnodes,
                     elem_slot, ke, K, F, Ks64, Ls64, Us64, D64, Ks32, Ls32, Us32, D32, b64, x64,
                     r64, z64, p64, ap64, x32, r32, z32, p32, ap32, u_full, y_full, ye, gauss, vm,
-                    react, lambda_full, grad, scal, partials, timing, claim, dsum, dticket, dfail};
+                    react, lambda_full, grad, node_stress, node_vm, scal, partials, timing, claim, dsum, dticket, dfail};
     for (void* p : bufs) dfree(p);
     sk.release();
     pl.release();
@@ -756,6 +756,31 @@ int32_t maille_gpu_multiply(MailleGpuHandle* h, const double* x, double* y) {
         CK(cudaMemcpyAsync(y, h->y_full, n3 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
         CK(cudaStreamSynchronize(h->st));
         h->solved = false;
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+    return MAILLE_OK;
+}
+
+int32_t maille_gpu_nodal_stresses(MailleGpuHandle* h, double* stress, double* von_mises) {
+    g_last_error.clear();
+    if (!h || !stress || !von_mises) return fail({MAILLE_INVALID_INPUT, "null argument"});
+    if (!h->solved || !h->gauss)
+        return fail({MAILLE_INVALID_INPUT, "nodal stresses need the Gauss stresses of a solve"});
+    try {
+        CK(cudaSetDevice(h->device));
+        if (!h->node_stress) {
+            h->node_stress = dalloc<double>((size_t)h->n_nodes * 6);
+            h->node_vm = dalloc<double>((size_t)h->n_nodes);
+        }
+        launch_nodal_stresses(h->npe, h->n_nodes, h->inc_ptr, h->inc, h->gauss, h->node_stress,
+                              h->node_vm, h->st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(stress, h->node_stress, (size_t)h->n_nodes * 6 * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->st));
+        CK(cudaMemcpyAsync(von_mises, h->node_vm, (size_t)h->n_nodes * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
     } catch (const CudaFailure& e) {
         return fail({MAILLE_CUDA_ERROR, e.what});
     }

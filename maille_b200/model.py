@@ -334,6 +334,16 @@ class SolverHandle:
         _raise_for(s, r)
         return Field(out["u"], out["reactions"], out["gauss"], out["vm"], _info(r))
 
+    def nodal_stresses(self):
+        """Smoothed nodal stresses of the last solve (nodal_stresses, results.rs:137-230):
+        returns (stress (n, 6) as sxx, syy, szz, txy, tyz, txz; von_mises (n,))."""
+        n = self.model.mesh.coords.shape[0]
+        st = np.zeros(6 * n)
+        vm = np.zeros(n)
+        s = self._L.maille_gpu_nodal_stresses(self._h, ptr(st, _lib._d), ptr(vm, _lib._d))
+        _raise_for(s)
+        return st.reshape(n, 6), vm
+
     def backward(self, dJdu):
         """dJ/dE per element for J with gradient dJ/du (adjoint of the last solve);
         returns (dJdE, lambda)."""

@@ -247,6 +247,42 @@ def voigt(g):
     return np.stack([g[..., 3], g[..., 4], g[..., 5], g[..., 7], g[..., 8], g[..., 6]], -1)
 
 
+def test_tet10_extrapolation_reproduces_a_linear_function_at_the_ten_nodes(oracle_lib):
+    # results.rs:258-278 through the oracle's smoothing: one reference Tet10 whose Gauss values are a
+    # linear f at the TETRA_4 points (point g near vertex g: barycentric a on it, b on the others)
+    # must give f at the ten nodes
+    from types import SimpleNamespace
+    f = lambda x, y, z: 2.0 + 3.0 * x - 5.0 * y + 7.0 * z  # noqa: E731
+    a, b = (5.0 + 3.0 * 5 ** 0.5) / 20.0, (5.0 - 5 ** 0.5) / 20.0
+    nodes = np.array([(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (.5, 0, 0), (.5, .5, 0), (0, .5, 0),
+                      (0, 0, .5), (.5, 0, .5), (0, .5, .5)], float)
+    gauss = np.zeros((1, 4, 9))
+    for g in range(4):
+        lam = np.full(4, b)
+        lam[g] = a
+        x, y, z = lam[1], lam[2], lam[3]
+        gauss[0, g, 3:] = f(x, y, z)
+    prob = SimpleNamespace(coords=nodes, conn=np.arange(10, dtype=np.int64).reshape(1, 10))
+    out = oracle_lib.nodal_stresses(prob, gauss)
+    for k in range(10):
+        assert np.abs(out[k] - f(*nodes[k])).max() < 1e-12, k
+
+
+def test_nodal_smoothing_averages_over_the_elements_of_a_node(oracle_lib):
+    # smooth, results.rs:198-230: component-wise mean over the elements sharing a node; an
+    # isolated node gets 0 (two Tet4 sharing the face 1-2-3, node 5 touched by no element)
+    from types import SimpleNamespace
+    prob = SimpleNamespace(coords=np.zeros((6, 3)), conn=np.array([[0, 1, 2, 3], [1, 2, 3, 4]], np.int64))
+    gauss = np.zeros((2, 1, 9))
+    gauss[0, 0, 3:] = [1, 2, 3, 4, 5, 6]
+    gauss[1, 0, 3:] = [3, 4, 5, 6, 7, 8]
+    out = oracle_lib.nodal_stresses(prob, gauss)
+    assert np.array_equal(out[0], [1, 2, 3, 4, 5, 6]) and np.array_equal(out[4], [3, 4, 5, 6, 7, 8])
+    for k in (1, 2, 3):
+        assert np.array_equal(out[k], [2, 3, 4, 5, 6, 7])
+    assert np.array_equal(out[5], np.zeros(6))
+
+
 @pytest.mark.parametrize("solver", [1, 2])
 @pytest.mark.parametrize("quadratic", [False, True])
 def test_uniform_strain_patch_is_exact(oracle_lib, quadratic, solver):
