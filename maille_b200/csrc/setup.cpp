@@ -50,26 +50,41 @@ struct NodeGraph {
     int64_t degree(int32_t v) const { return off[v + 1] - off[v]; }
 };
 
-// BFS levels from `start` that do not enter `excluded` vertices (bfs_levels, solve.rs:248-270).
-std::vector<std::vector<int32_t>> bfs_levels(const NodeGraph& g, int32_t start,
-                                             const std::vector<uint8_t>& excluded) {
-    std::vector<uint8_t> seen = excluded;
-    seen[start] = 1;
-    std::vector<std::vector<int32_t>> levels{{start}};
-    for (;;) {
-        std::vector<int32_t> next;
-        for (int32_t v : levels.back())
-            for (int64_t p = g.off[v]; p < g.off[v + 1]; ++p) {
-                const int32_t w = g.adj[p];
-                if (!seen[w]) {
-                    seen[w] = 1;
-                    next.push_back(w);
+// Breadth-first search from `start` that does not enter `excluded` vertices (bfs_levels,
+// solve.rs:248-270), on flat buffers reused across calls: returns the number of levels and keeps
+// the last level, in discovery order, in `last`.
+struct Bfs {
+    std::vector<int32_t> queue, mark, last;
+    int32_t stamp = 0;
+    explicit Bfs(int32_t n) : queue(n), mark(n, 0) {}
+    int32_t run(const NodeGraph& g, int32_t start, const std::vector<uint8_t>& excluded) {
+        ++stamp;
+        int64_t head = 0, tail = 0;
+        queue[tail++] = start;
+        mark[start] = stamp;
+        int32_t levels = 0;
+        int64_t level_begin = 0;
+        for (;;) {
+            const int64_t level_end = tail;
+            ++levels;
+            for (head = level_begin; head < level_end; ++head) {
+                const int32_t v = queue[head];
+                for (int64_t p = g.off[v]; p < g.off[v + 1]; ++p) {
+                    const int32_t w = g.adj[p];
+                    if (!excluded[w] && mark[w] != stamp) {
+                        mark[w] = stamp;
+                        queue[tail++] = w;
+                    }
                 }
             }
-        if (next.empty()) return levels;
-        levels.push_back(std::move(next));
+            if (tail == level_end) {
+                last.assign(queue.begin() + level_begin, queue.begin() + level_end);
+                return levels;
+            }
+            level_begin = level_end;
+        }
     }
-}
+};
 
 // Reverse Cuthill-McKee with a George-Liu pseudo-peripheral start and neighbours visited by
 // increasing degree (stable), one connected component at a time; the algorithm of
@@ -79,6 +94,8 @@ std::vector<int32_t> rcm(const NodeGraph& g) {
     std::vector<uint8_t> visited(n, 0);
     std::vector<int32_t> order;
     order.reserve(n);
+    Bfs bfs(n);
+    std::vector<int32_t> next;
     int32_t scan = 0;
     for (;;) {
         while (scan < n && visited[scan]) ++scan;
@@ -87,29 +104,40 @@ std::vector<int32_t> rcm(const NodeGraph& g) {
             if (!visited[v] && (seed < 0 || g.degree(v) < g.degree(seed))) seed = v;
         if (seed < 0) break;
         int32_t start = seed;
-        auto levels = bfs_levels(g, start, visited);
+        int32_t depth = bfs.run(g, start, visited);
         for (;;) {
             int32_t far = -1;
-            for (int32_t v : levels.back())
+            for (int32_t v : bfs.last)
                 if (far < 0 || g.degree(v) < g.degree(far)) far = v;
             if (far < 0) break;
-            auto far_levels = bfs_levels(g, far, visited);
-            if (far_levels.size() <= levels.size()) break;
+            const std::vector<int32_t> keep_last = bfs.last;
+            const int32_t far_depth = bfs.run(g, far, visited);
+            if (far_depth <= depth) {
+                bfs.last = keep_last;
+                break;
+            }
             start = far;
-            levels = std::move(far_levels);
+            depth = far_depth;
         }
         size_t head = order.size();
         visited[start] = 1;
         order.push_back(start);
-        std::vector<int32_t> next;
         while (head < order.size()) {
             const int32_t v = order[head++];
             next.clear();
             for (int64_t p = g.off[v]; p < g.off[v + 1]; ++p)
                 if (!visited[g.adj[p]]) next.push_back(g.adj[p]);
-            std::stable_sort(next.begin(), next.end(), [&](int32_t a, int32_t b) {
-                return g.degree(a) < g.degree(b);
-            });
+            // stable insertion sort by degree (neighbour lists are short)
+            for (size_t i = 1; i < next.size(); ++i) {
+                const int32_t x = next[i];
+                const int64_t dx = g.degree(x);
+                size_t j = i;
+                while (j > 0 && g.degree(next[j - 1]) > dx) {
+                    next[j] = next[j - 1];
+                    --j;
+                }
+                next[j] = x;
+            }
             for (int32_t w : next)
                 if (!visited[w]) {
                     visited[w] = 1;
@@ -268,11 +296,15 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
     std::vector<int32_t> colour;
     if (ordering != MAILLE_ORDER_RCM) {
         colour = greedy_colour(g, order);
-        std::vector<int32_t> rank(nk);
-        for (int32_t r = 0; r < nk; ++r) rank[order[r]] = r;
-        std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
-            return colour[a] != colour[b] ? colour[a] < colour[b] : rank[a] < rank[b];
-        });
+        // rows by colour, RCM order inside a colour (a stable counting sort)
+        int32_t nc = 0;
+        for (int32_t k = 0; k < nk; ++k) nc = std::max(nc, colour[k] + 1);
+        std::vector<int64_t> pos((size_t)nc + 1, 0);
+        for (int32_t k = 0; k < nk; ++k) pos[colour[k] + 1]++;
+        for (int32_t c = 0; c < nc; ++c) pos[c + 1] += pos[c];
+        std::vector<int32_t> by_colour(nk);
+        for (int32_t v : order) by_colour[pos[colour[v]]++] = v;
+        order.swap(by_colour);
     }
     stage("ordering");
     if (!colour.empty()) {

@@ -10,6 +10,7 @@
 // preconditioning, then launches of `persist_chunk` iterations until the device flags the end
 // (the host reads the device scalars after each launch: stopping, cancel flag).
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -319,14 +320,32 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
     h->h_f.assign(n3, 0.0);
     if (p->f) std::memcpy(h->h_f.data(), p->f, n3 * sizeof(double));
 
-    // host: ordering, levels and boundary lists; the pattern and scatter map are built on the
-    // device below (analysis.cu)
+    // the element kernels index with the connectivity: check it before any device work
+    if (p->nodes_per_elem != 4 && p->nodes_per_elem != 10)
+        return fail({MAILLE_INVALID_INPUT, "nodes_per_elem must be 4 or 10"});
+    for (int64_t k = 0; k < p->n_elems * p->nodes_per_elem; ++k)
+        if (p->conn[k] < 0 || p->conn[k] >= p->n_nodes)
+            return fail({MAILLE_INVALID_INPUT, "element " + std::to_string(k / p->nodes_per_elem) +
+                                                   " refers to unknown node " + std::to_string(p->conn[k])});
+    if (std::all_of(h->h_fixed.begin(), h->h_fixed.end(), [](uint8_t f) { return f != 0; }))
+        return fail({MAILLE_INVALID_INPUT, "every DOF is fixed"});
+    // host: ordering, levels and boundary lists, on a thread of its own while the device takes
+    // the inputs and integrates the element matrices (neither depends on the ordering); the
+    // pattern and scatter map are built on the device afterwards (analysis.cu)
     const double t_setup0 = now_ms();
-    if (!analyse(p->n_nodes, p->nodes_per_elem, p->n_elems, p->conn, h->h_fixed.data(), p->ordering,
-                 h->sym, err, /*pattern=*/false))
-        return fail(err);
-    if (h->sym.levels >= kMaxLevels) return fail({MAILLE_INVALID_INPUT, "too many IC(0) levels"});
-    const double t_setup1 = now_ms();
+    double t_setup1 = t_setup0;
+    bool analysed = false;
+    std::thread analysis([&] {
+        analysed = analyse(p->n_nodes, p->nodes_per_elem, p->n_elems, p->conn, h->h_fixed.data(),
+                           p->ordering, h->sym, err, /*pattern=*/false);
+        t_setup1 = now_ms();
+    });
+    struct Joiner {
+        std::thread& t;
+        ~Joiner() {
+            if (t.joinable()) t.join();
+        }
+    } joiner{analysis};
     // MAILLE_SETUP_TIMING: wall time of the device-side set-up steps (stream synchronised)
     const bool stage_timing = std::getenv("MAILLE_SETUP_TIMING") != nullptr;
     double t_mark = now_ms();
@@ -349,6 +368,7 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         const Symbolic& s = h->sym;
         CK(cudaEventRecord(h->ev[0], st));
         tmark("context");
+        const int np = node_pairs(h->npe);
         // inputs
         std::vector<int32_t> conn32(p->n_elems * p->nodes_per_elem);
         for (size_t k = 0; k < conn32.size(); ++k) conn32[k] = (int32_t)p->conn[k];
@@ -362,6 +382,14 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         h->f_cur = h->f0;
         h->h_f0 = h->h_f;
         h->fixed = dupload(h->h_fixed.data(), n3, st);
+        h->ke = dalloc<double>((size_t)p->n_elems * np * 9);
+        {
+            ElemIn in{h->n_elems, h->coords, h->conn, h->young, h->poisson};
+            launch_elem_stiffness(h->npe, in, h->ke, st);
+        }
+        analysis.join();
+        if (!analysed) return fail(err);
+        if (h->sym.levels >= kMaxLevels) return fail({MAILLE_INVALID_INPUT, "too many IC(0) levels"});
         // symbolic
         h->perm = dupload(s.perm.data(), s.perm.size(), st);
         h->inv = dupload(s.inv.data(), s.inv.size(), st);
@@ -403,9 +431,7 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         for (size_t k = 0; k < s.belem.size(); ++k) slot[s.belem[k]] = (int32_t)k;
         h->elem_slot = dupload(slot.data(), slot.size(), st);
         // numeric buffers
-        const int np = node_pairs(h->npe);
         const int64_t n4 = 4 * ((int64_t)s.nb + 1);  // + the dummy node that padding points at
-        h->ke = dalloc<double>((size_t)p->n_elems * np * 9);
         h->K = dalloc<double>((size_t)s.blocks * 9);
         h->F = dalloc<double>((size_t)s.blocks * 9);
         h->Ks64 = dalloc<double>((size_t)h->sk.h.steps() * 9 * kStepSlots);
@@ -463,7 +489,7 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         h->persist_chunk = std::max(1, env_int("MAILLE_PERSIST_CHUNK", h->persist_chunk));
         tmark("layouts+buffers");
         CK(cudaEventRecord(h->ev[1], st));
-        if (numeric_phase(h.get(), err) != MAILLE_OK) return fail(err);
+        if (assemble_factor(h.get(), err) != MAILLE_OK) return fail(err);
         tmark("numeric");
         CK(cudaStreamSynchronize(st));
         if (res) {
