@@ -156,6 +156,12 @@ int32_t maille_gpu_multiply(MailleGpuHandle* h, const double* x, double* y);
  * solve on the handle (MAILLE_INVALID_INPUT otherwise). */
 int32_t maille_gpu_nodal_stresses(MailleGpuHandle* h, double* stress, double* von_mises);
 
+/* Device memory: the library allocates from one memory pool per device that keeps freed memory
+ * reserved, so creating and destroying handles repeatedly does not map and unmap GBs each time.
+ * This returns the pool's unused memory of `device` to the device (call it when no handle is
+ * alive and the memory is wanted elsewhere). No counterpart in the reference. */
+int32_t maille_gpu_trim_memory(int32_t device);
+
 /* Enqueues `count` launches of the PCG's 3x3-block SpMV kernel on the handle's device vectors
  * and stream (precision MAILLE_FP64 or MAILLE_MIXED for the FP32 matrix), without waiting: for
  * timing the kernel with events on maille_gpu_stream(). No counterpart in the reference. */

@@ -308,7 +308,7 @@ int32_t numeric(MailleGpuBatch* b, Error& err) {
     CK(cudaEventRecord(b->ev[6], b->st));
     int32_t* dfail = dalloc<int32_t>(1);
     const int32_t status = factorize(b, err, dfail);
-    cudaFree(dfail);
+    dfree(dfail);
     CK(cudaEventRecord(b->ev[7], b->st));
     return status;
 }
@@ -687,7 +687,7 @@ int32_t create_batch(const MailleBatchProblem* p, MailleGpuBatch** out) {
         const size_t nv = b->vec_len();
         const size_t tsz = b->mixed() ? sizeof(float) : sizeof(double);
         for (void** q : {&b->x, &b->r, &b->z, &b->p, &b->ap}) {
-            CK(cudaMalloc(q, nv * tsz));
+            *q = device_alloc(nv * tsz);
             CK(cudaMemsetAsync(*q, 0, nv * tsz, st));
         }
         b->b = dalloc<double>(nv);

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <chrono>
+#include <cstdint>
 #include <string>
 
 #include <cuda_runtime.h>
@@ -26,12 +27,17 @@ inline double now_ms() {
         .count();
 }
 
+// Device memory from the library's per-device pool (memory.cu): an allocation is ready for any
+// stream when it returns; a free waits for the device to be idle, like cudaFree.
+void* device_alloc(size_t bytes);
+void device_free(void* p);
+// Returns the pool's unused memory of `device` to the device (0, or -1 on a CUDA error).
+int32_t trim_device_memory(int device);
+
 template <typename T>
 T* dalloc(size_t n) {
-    void* p = nullptr;
     if (n == 0) n = 1;
-    CK(cudaMalloc(&p, n * sizeof(T)));
-    return static_cast<T*>(p);
+    return static_cast<T*>(device_alloc(n * sizeof(T)));
 }
 
 template <typename T>
@@ -41,9 +47,7 @@ T* dupload(const T* src, size_t n, cudaStream_t st) {
     return d;
 }
 
-inline void dfree(void* p) {
-    if (p) cudaFree(p);
-}
+inline void dfree(void* p) { device_free(p); }
 
 constexpr double kDefaultTol = 1e-12;      // iterative.rs:9
 constexpr int32_t kDefaultMaxIter = 10000;  // iterative.rs:11

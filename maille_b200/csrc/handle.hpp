@@ -36,8 +36,7 @@ struct SellBuf {
                   nb, col, src, st);
     }
     void release() {
-        for (void* p : {(void*)rowid, (void*)off, (void*)col, (void*)src})
-            if (p) cudaFree(p);
+        for (void* p : {(void*)rowid, (void*)off, (void*)col, (void*)src}) dfree(p);
         rowid = nullptr;
         off = nullptr;
         col = nullptr;
@@ -69,11 +68,10 @@ struct PsellBuf {
         fill_psell(kind, (int64_t)h.rows.size(), h.steps(), rows, rstart, pt.row_ptr, pt.col, pt.diag,
                    nb, col, src, st);
         CK(cudaStreamSynchronize(st));
-        cudaFree(rstart);
+        dfree(rstart);
     }
     void release() {
-        for (void* p : {(void*)off, (void*)col, (void*)src, (void*)head, (void*)row0, (void*)rows})
-            if (p) cudaFree(p);
+        for (void* p : {(void*)off, (void*)col, (void*)src, (void*)head, (void*)row0, (void*)rows}) dfree(p);
         off = nullptr;
         col = nullptr;
         src = nullptr;

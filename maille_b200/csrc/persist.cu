@@ -112,11 +112,10 @@ __device__ __forceinline__ void st_rec(float* z, int32_t c, float a, float b, fl
 }
 
 
-// this lane's 4 slots of step g: acc += V_b x[col_b] (x read coherently through L2)
+// this lane's 4 slots of step g with columns c4: acc += V_b x[col_b] (x read coherently through L2)
 template <typename M, typename T>
-__device__ __forceinline__ void step(const M* __restrict__ vals, const int32_t* __restrict__ col,
-                                     int64_t g, const T* x, int lane, T& a0, T& a1, T& a2) {
-    const int4 c4 = __ldg(reinterpret_cast<const int4*>(col + g * kStepSlots + 4 * lane));
+__device__ __forceinline__ void step(const M* __restrict__ vals, int4 c4, int64_t g, const T* x, int lane,
+                                     T& a0, T& a1, T& a2) {
     const M* V = vals + g * 9 * kStepSlots + 4 * lane;
     M v[9][4];
 #pragma unroll
@@ -168,8 +167,14 @@ __device__ __forceinline__ double spmv_phase(const SellDev& A, const M* vals, co
     for (int32_t sl = (int32_t)(blockIdx.x * kPW + (threadIdx.x >> 5)); sl < A.nslices; sl += nw) {
         const int32_t row = A.rowid[(int64_t)sl * S + r];
         T a0 = 0, a1 = 0, a2 = 0;
-        const int64_t g1 = A.off[sl + 1];
-        for (int64_t g = A.off[sl]; g < g1; ++g) step<M, T>(vals, A.col, g, x, lane, a0, a1, a2);
+        const int64_t g0 = A.off[sl], g1 = A.off[sl + 1];
+        // each step's columns are fetched one step ahead, so its gathers wait on L2 only
+        int4 cnext = __ldg(reinterpret_cast<const int4*>(A.col + g0 * kStepSlots + 4 * lane));
+        for (int64_t g = g0; g < g1; ++g) {
+            const int4 c4 = cnext;
+            if (g + 1 < g1) cnext = __ldg(reinterpret_cast<const int4*>(A.col + (g + 1) * kStepSlots + 4 * lane));
+            step<M, T>(vals, c4, g, x, lane, a0, a1, a2);
+        }
         lanes_sum<T, LPR>(a0, a1, a2);
         if (q == 0 && row >= 0) {
             if (b) {

@@ -41,6 +41,7 @@ thread_local std::string g_last_error;
 
 MailleGpuHandle::~MailleGpuHandle() {
     cudaSetDevice(device);
+    if (st) cudaStreamSynchronize(st);
     if (timing) {
         unsigned long long t[8] = {0};
         cudaMemcpy(t, timing, sizeof(t), cudaMemcpyDeviceToHost);
@@ -810,6 +811,12 @@ int32_t maille_gpu_nodal_stresses(MailleGpuHandle* h, double* stress, double* vo
     } catch (const CudaFailure& e) {
         return fail({MAILLE_CUDA_ERROR, e.what});
     }
+    return MAILLE_OK;
+}
+
+int32_t maille_gpu_trim_memory(int32_t device) {
+    g_last_error.clear();
+    if (trim_device_memory(device) != 0) return fail({MAILLE_CUDA_ERROR, "cannot trim the memory pool of device " + std::to_string(device)});
     return MAILLE_OK;
 }
 

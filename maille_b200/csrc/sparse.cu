@@ -74,12 +74,10 @@ __device__ __forceinline__ void store_node(T* x, int64_t i, T a, T b, T d) {
     x[4 * i] = a; x[4 * i + 1] = b; x[4 * i + 2] = d; x[4 * i + 3] = T(0);
 }
 
-// acc += this lane's 4 slots of step g: V_b x[col_b] (3x3 blocks)
+// acc += this lane's 4 slots of step g with columns c4: V_b x[col_b] (3x3 blocks)
 template <typename T>
-__device__ __forceinline__ void step_accum(const T* __restrict__ vals,
-                                           const int32_t* __restrict__ col, int64_t g,
+__device__ __forceinline__ void step_accum(const T* __restrict__ vals, int4 c4, int64_t g,
                                            const T* __restrict__ x, int lane, T& a0, T& a1, T& a2) {
-    const int4 c4 = __ldg(reinterpret_cast<const int4*>(col + g * kStepSlots + 4 * lane));
     const T* V = vals + g * 9 * kStepSlots + 4 * lane;
     T v[9][4];
 #pragma unroll
@@ -100,8 +98,13 @@ template <typename T>
 __device__ __forceinline__ void slice_accum(const T* __restrict__ vals,
                                             const int32_t* __restrict__ col, int64_t g0, int64_t g1,
                                             const T* __restrict__ x, int lane, T& a0, T& a1, T& a2) {
-#pragma unroll 2
-    for (int64_t g = g0; g < g1; ++g) step_accum<T>(vals, col, g, x, lane, a0, a1, a2);
+    // each step's columns are fetched one step ahead, so its gathers wait on L2 only
+    int4 cnext = __ldg(reinterpret_cast<const int4*>(col + g0 * kStepSlots + 4 * lane));
+    for (int64_t g = g0; g < g1; ++g) {
+        const int4 c4 = cnext;
+        if (g + 1 < g1) cnext = __ldg(reinterpret_cast<const int4*>(col + (g + 1) * kStepSlots + 4 * lane));
+        step_accum<T>(vals, c4, g, x, lane, a0, a1, a2);
+    }
 }
 
 template <typename T, int LPR>
