@@ -234,17 +234,6 @@ struct RecOf<float> { using type = Rec32; };
 template <>
 struct RecOf<double> { using type = Rec64; };
 
-// Re-reads record c until it carries `epoch` (at most kSpinLimit polls); returns the last read.
-template <typename T>
-__device__ __forceinline__ typename RecOf<T>::type spin_record(const T* z, int32_t c, unsigned int epoch,
-                                                               typename RecOf<T>::type r) {
-    for (unsigned int k = 0; k < kSpinLimit && !ready(r, epoch); ++k) {
-        __nanosleep(32);
-        r = ld_record(z, c);
-    }
-    return r;
-}
-
 // publishes row `row` of the sweep output for sweep `epoch`
 __device__ __forceinline__ void publish_row(float* z, int32_t row, float a, float b, float d, unsigned int epoch) {
     st_rec(z, row, a, b, d, epoch);
@@ -341,12 +330,21 @@ __device__ __forceinline__ bool slot_products(const T* __restrict__ vals, int4 c
     R q[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) q[j] = ld_record(z, cc[j]);
-    bool ok = true;
+    // re-read every record that is not current yet, all together in each round (one L2 round trip
+    // per round however many are pending), at most kSpinLimit rounds
+    bool pending = false;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        if (!ready(q[j], epoch)) q[j] = spin_record(z, cc[j], epoch, q[j]);
-        ok = ok && ready(q[j], epoch);
+    for (int j = 0; j < 4; ++j) pending = pending || !ready(q[j], epoch);
+    for (unsigned int k = 0; pending && k < kSpinLimit; ++k) {
+        __nanosleep(32);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (!ready(q[j], epoch)) q[j] = ld_record(z, cc[j]);
+        pending = false;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) pending = pending || !ready(q[j], epoch);
     }
+    bool ok = !pending;
     ok = mbar_wait(st.bar, st.phase) && ok;
     st.phase ^= 1u;
     const T* V = st.buf + 4 * lane;
@@ -568,6 +566,81 @@ __device__ __forceinline__ double sweep(const PsellDev& A, unsigned int epoch, c
     return loc;
 }
 
+// The FP32 SpMV of the mixed form with its values staged through shared memory: the warp's steps
+// (slice after slice, in its round-robin order) stream through two buffers by TMA bulk copies,
+// the copy of step k + 2 starting as soon as step k's buffer has been read, so two steps (9 KB)
+// per warp are in flight without holding registers. Columns are fetched one step ahead and the
+// gathers of a step are requested before its values are awaited. Same arithmetic and summation
+// order as spmv_phase; returns this thread's share of x . y.
+template <int LPR>
+__device__ __forceinline__ double spmv_staged(const SellDev& A, const float* __restrict__ vals,
+                                              const float* x, float* y, float* buf, uint64_t* bars,
+                                              uint32_t& phases) {
+    const int lane = threadIdx.x & 31, r = lane / LPR, q = lane % LPR;
+    constexpr int S = 32 / LPR;
+    constexpr uint32_t kBytes = 9 * kStepSlots * sizeof(float);
+    const int32_t nw = (int32_t)(gridDim.x * kPW), n = A.nslices;
+    int32_t sl = (int32_t)(blockIdx.x * kPW + (threadIdx.x >> 5));
+    double loc = 0.0;
+    if (sl >= n) return loc;
+    // staging cursor of lane 0: the next step to copy, walking the warp's slices
+    int32_t cs = sl;
+    int64_t cg = __ldg(A.off + sl), cg1 = __ldg(A.off + sl + 1);
+    auto stage_next = [&](int b) {
+        if (cs >= n) return;
+        bulk_stage(buf + b * 9 * kStepSlots, vals + cg * 9 * kStepSlots, kBytes, &bars[b]);
+        if (++cg == cg1) {
+            cs += nw;
+            if (cs < n) {
+                cg = __ldg(A.off + cs);
+                cg1 = __ldg(A.off + cs + 1);
+            }
+        }
+    };
+    if (lane == 0) {
+        stage_next(0);
+        stage_next(1);
+    }
+    int b = 0;
+    for (; sl < n; sl += nw) {
+        const int32_t row = A.rowid[(int64_t)sl * S + r];
+        float a0 = 0, a1 = 0, a2 = 0;
+        const int64_t g0 = A.off[sl], g1 = A.off[sl + 1];
+        int4 cnext = __ldg(reinterpret_cast<const int4*>(A.col + g0 * kStepSlots + 4 * lane));
+        for (int64_t g = g0; g < g1; ++g) {
+            const int4 c4 = cnext;
+            if (g + 1 < g1) cnext = __ldg(reinterpret_cast<const int4*>(A.col + (g + 1) * kStepSlots + 4 * lane));
+            const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+            float xv[4][3];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) node3_cg<float>(x, cc[j], xv[j][0], xv[j][1], xv[j][2]);
+            mbar_wait(&bars[b], (phases >> b) & 1u);
+            phases ^= 1u << b;
+            const float* V = buf + b * 9 * kStepSlots + 4 * lane;
+            float v[9][4];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) lds4(V + k * kStepSlots, v[k]);
+            __syncwarp();  // every lane has read the buffer before lane 0 refills it
+            if (lane == 0) stage_next(b);
+            b ^= 1;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                a0 += v[0][j] * xv[j][0] + v[1][j] * xv[j][1] + v[2][j] * xv[j][2];
+                a1 += v[3][j] * xv[j][0] + v[4][j] * xv[j][1] + v[5][j] * xv[j][2];
+                a2 += v[6][j] * xv[j][0] + v[7][j] * xv[j][1] + v[8][j] * xv[j][2];
+            }
+        }
+        lanes_sum<float, LPR>(a0, a1, a2);
+        if (q == 0 && row >= 0) {
+            float x0, x1, x2;
+            node3_cg<float>(x, row, x0, x1, x2);
+            loc += (double)x0 * (double)a0 + (double)x1 * (double)a1 + (double)x2 * (double)a2;
+            put3(y, row, a0, a1, a2);
+        }
+    }
+    return loc;
+}
+
 struct Local {
     double alpha, beta, rz, rr, bb, tol, maxr, delta, rr_true;
     int32_t iter, max_iter, done, status, updates;
@@ -584,13 +657,20 @@ template <typename T, int LPRK, bool MIXED>
 __global__ void __launch_bounds__(kPW * 32, 2) k_pcg(PcgArgs<T> a, int init) {
     __shared__ double sh[kPW];
     __shared__ uint64_t bars[kPW];
+    __shared__ uint64_t spmv_bars[2 * kPW];  // the two staging buffers of the mixed form's SpMV
     extern __shared__ __align__(128) unsigned char stage_mem[];  // kPW x one step of factor values
     cg::grid_group grid = cg::this_grid();
     const int warp = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) mbar_init(&bars[warp]);
+    if ((threadIdx.x & 31) == 0) {
+        mbar_init(&bars[warp]);
+        mbar_init(&spmv_bars[2 * warp]);
+        mbar_init(&spmv_bars[2 * warp + 1]);
+    }
+    uint32_t spmv_phases = 0;
     mbar_init_fence();
     __syncthreads();
-    Stage<T> stage{reinterpret_cast<T*>(stage_mem) + (size_t)warp * 9 * kStepSlots, &bars[warp], 0u};
+    // each warp's buffer: 9 KB (one FP64 step, or two FP32 steps for the staged SpMV)
+    Stage<T> stage{reinterpret_cast<T*>(stage_mem + (size_t)warp * 9 * kStepSlots * 8), &bars[warp], 0u};
     PcgScalars* s = a.s;
     Local v{s->alpha, s->beta, s->rz, s->rr, s->bb, s->tol, s->maxr, s->delta, s->rr_true,
             s->iter, s->max_iter, s->done, s->status, s->updates, s->epoch};
@@ -611,7 +691,10 @@ __global__ void __launch_bounds__(kPW * 32, 2) k_pcg(PcgArgs<T> a, int init) {
         double loc;
         if (!init) {
             // ap = K p, alpha = rz / p.ap (iterative.rs:223-228)
-            loc = spmv_phase<T, T, LPRK>(a.K, a.Kv, a.p, a.ap);
+            if constexpr (MIXED)
+                loc = spmv_staged<LPRK>(a.K, a.Kv, a.p, a.ap, stage.buf, &spmv_bars[2 * warp], spmv_phases);
+            else
+                loc = spmv_phase<T, T, LPRK>(a.K, a.Kv, a.p, a.ap);
             publish(loc, a.partials, 0, sh);
             grid.sync();
             mark(0);
@@ -746,7 +829,8 @@ __global__ void __launch_bounds__(kPW * 32, 2) k_pcg(PcgArgs<T> a, int init) {
 // dynamic shared memory of the persistent kernel: one staged step of factor values per warp
 template <typename T>
 constexpr size_t stage_bytes() {
-    return (size_t)kPW * 9 * kStepSlots * sizeof(T);
+    // one step of FP64 values (9 KB) per warp; two FP32 steps in the mixed form's staged SpMV
+    return (size_t)kPW * 9 * kStepSlots * 8;
 }
 
 template <typename T, bool MIXED>
