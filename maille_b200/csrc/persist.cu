@@ -45,7 +45,7 @@ extern std::atomic<long long> g_kernel_launches;
 namespace {
 
 constexpr int kPW = 8;                        // warps per block
-constexpr unsigned int kSpinLimit = 1u << 22;  // polls of one flag before a timeout (~0.3 s)
+constexpr unsigned int kSpinLimit = 1u << 22;  // rounds of a wait before a timeout (seconds)
 
 template <typename T>
 __device__ __forceinline__ void node3_cg(const T* x, int64_t c, T& a, T& b, T& d);
@@ -336,7 +336,6 @@ __device__ __forceinline__ bool slot_products(const T* __restrict__ vals, int4 c
 #pragma unroll
     for (int j = 0; j < 4; ++j) pending = pending || !ready(q[j], epoch);
     for (unsigned int k = 0; pending && k < kSpinLimit; ++k) {
-        __nanosleep(32);
 #pragma unroll
         for (int j = 0; j < 4; ++j)
             if (!ready(q[j], epoch)) q[j] = ld_record(z, cc[j]);
