@@ -156,6 +156,14 @@ int32_t maille_gpu_multiply(MailleGpuHandle* h, const double* x, double* y);
  * solve on the handle (MAILLE_INVALID_INPUT otherwise). */
 int32_t maille_gpu_nodal_stresses(MailleGpuHandle* h, double* stress, double* von_mises);
 
+/* Self-test of the bounded waits of the IC(0) sweeps (failure detection without a GPU fault): one
+ * warp awaits four sweep records, one of them stale when `stale` is non-zero (its tag is the epoch
+ * before the awaited one and nothing writes it), with the sweeps' re-read loop limited to 4096
+ * rounds. *timed_out is 1 when the wait ran out and 0 when all records were current; the call
+ * itself returns MAILLE_OK unless CUDA failed. A sweep whose wait runs out the same way ends the
+ * solve with MAILLE_CUDA_ERROR. No counterpart in the reference. */
+int32_t maille_gpu_wait_selftest(int32_t device, int32_t stale, int32_t* timed_out);
+
 /* Device memory: the library allocates from one memory pool per device that keeps freed memory
  * reserved, so creating and destroying handles repeatedly does not map and unmap GBs each time.
  * This returns the pool's unused memory of `device` to the device (call it when no handle is

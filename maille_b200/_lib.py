@@ -110,6 +110,7 @@ SIGNATURES = {
     "maille_gpu_multiply": ([ctypes.c_void_p, _d, _d], ctypes.c_int32),
     "maille_gpu_nodal_stresses": ([ctypes.c_void_p, _d, _d], ctypes.c_int32),
     "maille_gpu_trim_memory": ([ctypes.c_int32], ctypes.c_int32),
+    "maille_gpu_wait_selftest": ([ctypes.c_int32, ctypes.c_int32, _i32], ctypes.c_int32),
     "maille_gpu_spmv_device": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
     "maille_gpu_kernel_launches": ([], ctypes.c_int64),
     "maille_gpu_bsr3_spmv_dot_noalloc": ([ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p,

@@ -30,9 +30,11 @@
 
 #include <atomic>
 #include <cmath>
+#include <cstring>
 
 #include <cooperative_groups.h>
 
+#include "cuda_host.hpp"
 #include "reduce.cuh"
 #include "sparse.cuh"
 
@@ -234,6 +236,38 @@ struct RecOf<float> { using type = Rec32; };
 template <>
 struct RecOf<double> { using type = Rec64; };
 
+// Waits until the 4 records q (read from z at columns cc) carry `epoch`: every record that is not
+// current yet is re-read, all of them together in each round (one L2 round trip per round however
+// many are pending), for at most `limit` rounds; false when the limit ran out.
+template <typename T>
+__device__ __forceinline__ bool await_records(const T* z, const int32_t cc[4], unsigned int epoch,
+                                              typename RecOf<T>::type q[4], unsigned int limit) {
+    bool pending = false;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) pending = pending || !ready(q[j], epoch);
+    for (unsigned int k = 0; pending && k < limit; ++k) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (!ready(q[j], epoch)) q[j] = ld_record(z, cc[j]);
+        pending = false;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) pending = pending || !ready(q[j], epoch);
+    }
+    return !pending;
+}
+
+// Self-test of the bounded wait: one warp awaits records 0..3 of z for `epoch` with at most `limit`
+// rounds and lane 0 writes 1 to *timed_out when the wait ran out, 0 when every record was
+// current. Nothing else writes z meanwhile, so a record whose tag is below `epoch` stays stale.
+__global__ void k_wait_selftest(const float* z, unsigned int epoch, unsigned int limit, int32_t* timed_out) {
+    const int32_t cc[4] = {0, 1, 2, 3};
+    Rec32 q[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) q[j] = ld_record(z, cc[j]);
+    const bool ok = await_records<float>(z, cc, epoch, q, limit);
+    if ((threadIdx.x & 31) == 0) *timed_out = ok ? 0 : 1;
+}
+
 // publishes row `row` of the sweep output for sweep `epoch`
 __device__ __forceinline__ void publish_row(float* z, int32_t row, float a, float b, float d, unsigned int epoch) {
     st_rec(z, row, a, b, d, epoch);
@@ -330,20 +364,7 @@ __device__ __forceinline__ bool slot_products(const T* __restrict__ vals, int4 c
     R q[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) q[j] = ld_record(z, cc[j]);
-    // re-read every record that is not current yet, all together in each round (one L2 round trip
-    // per round however many are pending), at most kSpinLimit rounds
-    bool pending = false;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) pending = pending || !ready(q[j], epoch);
-    for (unsigned int k = 0; pending && k < kSpinLimit; ++k) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (!ready(q[j], epoch)) q[j] = ld_record(z, cc[j]);
-        pending = false;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) pending = pending || !ready(q[j], epoch);
-    }
-    bool ok = !pending;
+    bool ok = await_records<T>(z, cc, epoch, q, kSpinLimit);
     ok = mbar_wait(st.bar, st.phase) && ok;
     st.phase ^= 1u;
     const T* V = st.buf + 4 * lane;
@@ -841,6 +862,22 @@ void* pick(int lprk) {
 }
 
 }  // namespace
+
+// Runs k_wait_selftest on 4 FP32 records whose tags are `tags` for `epoch` with at most `limit`
+// rounds; *timed_out tells whether the wait ran out. Throws CudaFailure on a CUDA error.
+void wait_selftest(const unsigned int tags[4], unsigned int epoch, unsigned int limit, int32_t* timed_out) {
+    float host[16] = {};
+    for (int j = 0; j < 4; ++j) std::memcpy(&host[4 * j + 3], &tags[j], sizeof(unsigned int));
+    float* z = dalloc<float>(16);
+    int32_t* flag = dalloc<int32_t>(1);
+    CK(cudaMemcpy(z, host, sizeof(host), cudaMemcpyHostToDevice));
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    k_wait_selftest<<<1, 32>>>(z, epoch, limit, flag);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(timed_out, flag, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    dfree(z);
+    dfree(flag);
+}
 
 // Grid size of the persistent kernel: every block co-resident (0 when the layout's lanes-per-
 // row combination has no instance).

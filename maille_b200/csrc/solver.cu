@@ -814,6 +814,20 @@ int32_t maille_gpu_nodal_stresses(MailleGpuHandle* h, double* stress, double* vo
     return MAILLE_OK;
 }
 
+int32_t maille_gpu_wait_selftest(int32_t device, int32_t stale, int32_t* timed_out) {
+    g_last_error.clear();
+    if (!timed_out) return fail({MAILLE_INVALID_INPUT, "null argument"});
+    try {
+        CK(cudaSetDevice(device));
+        const unsigned int epoch = 7;
+        const unsigned int tags[4] = {epoch, epoch, stale ? epoch - 1 : epoch, epoch + 1};
+        wait_selftest(tags, epoch, 4096, timed_out);
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+    return MAILLE_OK;
+}
+
 int32_t maille_gpu_trim_memory(int32_t device) {
     g_last_error.clear();
     if (trim_device_memory(device) != 0) return fail({MAILLE_CUDA_ERROR, "cannot trim the memory pool of device " + std::to_string(device)});

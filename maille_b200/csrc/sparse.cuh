@@ -87,6 +87,9 @@ struct PcgArgs {
 };
 template <typename T, bool MIXED>
 int pcg_persistent_grid(int lprk);
+// Self-test of the sweeps' bounded wait (persist.cu): awaits 4 FP32 records with tags `tags` for
+// `epoch` within `limit` rounds; *timed_out = 1 when the wait ran out. Throws CudaFailure.
+void wait_selftest(const unsigned int tags[4], unsigned int epoch, unsigned int limit, int32_t* timed_out);
 template <typename T, bool MIXED>
 cudaError_t launch_pcg_persistent(const PcgArgs<T>& a, int grid, bool init, cudaStream_t st);
 
