@@ -26,8 +26,10 @@ struct SellBuf {
     int64_t* off = nullptr;
     int32_t* col = nullptr;
     int32_t* src = nullptr;
-    SellDev dev() const { return SellDev{h.lpr, h.nslices(), rowid, off, col}; }
+    int32_t pad = 0;  // the dummy node nb that padding slots point at
+    SellDev dev() const { return SellDev{h.lpr, h.nslices(), rowid, off, col, pad}; }
     void upload(const PatternDev& pt, int32_t nb, cudaStream_t st) {
+        pad = nb;
         rowid = dupload(h.rowid.data(), h.rowid.size(), st);
         off = dupload(h.off.data(), h.off.size(), st);
         col = dalloc<int32_t>((size_t)h.steps() * 128);
@@ -55,9 +57,11 @@ struct PsellBuf {
     int32_t* row0 = nullptr;
     int32_t* rows = nullptr;
     PsellDev dev() const {
-        return PsellDev{h.nslices(), off, col, reinterpret_cast<const uint4*>(head), row0, rows};
+        return PsellDev{h.nslices(), off, col, reinterpret_cast<const uint4*>(head), row0, rows, pad};
     }
+    int32_t pad = 0;  // the dummy node nb that padding slots point at
     void upload(const PatternDev& pt, int32_t nb, cudaStream_t st) {
+        pad = nb;
         off = dupload(h.off.data(), h.off.size(), st);
         head = dupload(h.head.data(), h.head.size(), st);
         row0 = dupload(h.row0.data(), h.row0.size(), st);

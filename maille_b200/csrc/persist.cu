@@ -117,7 +117,7 @@ __device__ __forceinline__ void st_rec(float* z, int32_t c, float a, float b, fl
 // this lane's 4 slots of step g with columns c4: acc += V_b x[col_b] (x read coherently through L2)
 template <typename M, typename T>
 __device__ __forceinline__ void step(const M* __restrict__ vals, int4 c4, int64_t g, const T* x, int lane,
-                                     T& a0, T& a1, T& a2) {
+                                     int32_t pad, T& a0, T& a1, T& a2) {
     const M* V = vals + g * 9 * kStepSlots + 4 * lane;
     M v[9][4];
 #pragma unroll
@@ -125,8 +125,8 @@ __device__ __forceinline__ void step(const M* __restrict__ vals, int4 c4, int64_
     const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        T x0, x1, x2;
-        node3_cg<T>(x, cc[j], x0, x1, x2);
+        T x0 = 0, x1 = 0, x2 = 0;
+        if (cc[j] != pad) node3_cg<T>(x, cc[j], x0, x1, x2);  // padding slots: zero values, no load
         a0 += (T)v[0][j] * x0 + (T)v[1][j] * x1 + (T)v[2][j] * x2;
         a1 += (T)v[3][j] * x0 + (T)v[4][j] * x1 + (T)v[5][j] * x2;
         a2 += (T)v[6][j] * x0 + (T)v[7][j] * x1 + (T)v[8][j] * x2;
@@ -175,7 +175,7 @@ __device__ __forceinline__ double spmv_phase(const SellDev& A, const M* vals, co
         for (int64_t g = g0; g < g1; ++g) {
             const int4 c4 = cnext;
             if (g + 1 < g1) cnext = __ldg(reinterpret_cast<const int4*>(A.col + (g + 1) * kStepSlots + 4 * lane));
-            step<M, T>(vals, c4, g, x, lane, a0, a1, a2);
+            step<M, T>(vals, c4, g, x, lane, A.pad, a0, a1, a2);
         }
         lanes_sum<T, LPR>(a0, a1, a2);
         if (q == 0 && row >= 0) {
@@ -235,6 +235,17 @@ template <>
 struct RecOf<float> { using type = Rec32; };
 template <>
 struct RecOf<double> { using type = Rec64; };
+// the record of a padding slot: zero values, always current (padding needs no load)
+template <typename T>
+__device__ __forceinline__ typename RecOf<T>::type pad_record();
+template <>
+__device__ __forceinline__ Rec32 pad_record<float>() {
+    return Rec32{make_float4(0.f, 0.f, 0.f, __uint_as_float(0xFFFFFFFFu))};
+}
+template <>
+__device__ __forceinline__ Rec64 pad_record<double>() {
+    return Rec64{0.0, 0.0, 0.0, __longlong_as_double(-1ll)};
+}
 
 // Waits until the 4 records q (read from z at columns cc) carry `epoch`: every record that is not
 // current yet is re-read, all of them together in each round (one L2 round trip per round however
@@ -358,12 +369,12 @@ __device__ __forceinline__ void stage_step(const T* vals, int64_t g, Stage<T>& s
 template <typename T>
 __device__ __forceinline__ bool slot_products(const T* __restrict__ vals, int4 c4, const T* z,
                                               unsigned int epoch, int lane, Stage<T>& st,
-                                              int64_t next, T P[4][3]) {
+                                              int64_t next, int32_t pad, T P[4][3]) {
     using R = typename RecOf<T>::type;
     const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
     R q[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) q[j] = ld_record(z, cc[j]);
+    for (int j = 0; j < 4; ++j) q[j] = cc[j] == pad ? pad_record<T>() : ld_record(z, cc[j]);
     bool ok = await_records<T>(z, cc, epoch, q, kSpinLimit);
     ok = mbar_wait(st.bar, st.phase) && ok;
     st.phase ^= 1u;
@@ -521,7 +532,7 @@ __device__ __forceinline__ double sweep(const PsellDev& A, unsigned int epoch, c
             const uint32_t mine = head_bits(m0.head, lane);
             const int last = lane + 1 < nrows ? nth_set(m0.head, lane + 1) - 1 : 127;
             T P[4][3];
-            ok = slot_products(vals, c0, z, epoch, lane, st, next_slice, P) && ok;
+            ok = slot_products(vals, c0, z, epoch, lane, st, next_slice, A.pad, P) && ok;
             // in-lane running sums, restarted at each row start; the lane's carry-out is the sum
             // of its slots after its last row start (all 4 when none starts here)
             T s0 = 0, s1 = 0, s2 = 0;
@@ -567,7 +578,7 @@ __device__ __forceinline__ double sweep(const PsellDev& A, unsigned int epoch, c
             for (int64_t g = m0.g0; g < m0.g1; ++g) {
                 const int4 cg4 = g == m0.g0 ? c0 : lane_cols(A, g, lane);
                 T P[4][3];
-                ok = slot_products(vals, cg4, z, epoch, lane, st, g + 1 < m0.g1 ? g + 1 : next_slice, P) && ok;
+                ok = slot_products(vals, cg4, z, epoch, lane, st, g + 1 < m0.g1 ? g + 1 : next_slice, A.pad, P) && ok;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) { a0 += P[j][0]; a1 += P[j][1]; a2 += P[j][2]; }
             }
@@ -633,7 +644,10 @@ __device__ __forceinline__ double spmv_staged(const SellDev& A, const float* __r
             const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
             float xv[4][3];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) node3_cg<float>(x, cc[j], xv[j][0], xv[j][1], xv[j][2]);
+            for (int j = 0; j < 4; ++j) {
+                xv[j][0] = xv[j][1] = xv[j][2] = 0.f;
+                if (cc[j] != A.pad) node3_cg<float>(x, cc[j], xv[j][0], xv[j][1], xv[j][2]);
+            }
             mbar_wait(&bars[b], (phases >> b) & 1u);
             phases ^= 1u << b;
             const float* V = buf + b * 9 * kStepSlots + 4 * lane;

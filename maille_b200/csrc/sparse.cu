@@ -77,7 +77,8 @@ __device__ __forceinline__ void store_node(T* x, int64_t i, T a, T b, T d) {
 // acc += this lane's 4 slots of step g with columns c4: V_b x[col_b] (3x3 blocks)
 template <typename T>
 __device__ __forceinline__ void step_accum(const T* __restrict__ vals, int4 c4, int64_t g,
-                                           const T* __restrict__ x, int lane, T& a0, T& a1, T& a2) {
+                                           const T* __restrict__ x, int lane, int32_t pad, T& a0, T& a1,
+                                           T& a2) {
     const T* V = vals + g * 9 * kStepSlots + 4 * lane;
     T v[9][4];
 #pragma unroll
@@ -85,8 +86,8 @@ __device__ __forceinline__ void step_accum(const T* __restrict__ vals, int4 c4, 
     const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        T x0, x1, x2;
-        node3(x, cc[j], x0, x1, x2);
+        T x0 = 0, x1 = 0, x2 = 0;
+        if (cc[j] != pad) node3(x, cc[j], x0, x1, x2);  // padding slots: zero values, no load
         a0 += v[0][j] * x0 + v[1][j] * x1 + v[2][j] * x2;
         a1 += v[3][j] * x0 + v[4][j] * x1 + v[5][j] * x2;
         a2 += v[6][j] * x0 + v[7][j] * x1 + v[8][j] * x2;
@@ -97,13 +98,14 @@ __device__ __forceinline__ void step_accum(const T* __restrict__ vals, int4 c4, 
 template <typename T>
 __device__ __forceinline__ void slice_accum(const T* __restrict__ vals,
                                             const int32_t* __restrict__ col, int64_t g0, int64_t g1,
-                                            const T* __restrict__ x, int lane, T& a0, T& a1, T& a2) {
+                                            const T* __restrict__ x, int lane, int32_t pad, T& a0,
+                                            T& a1, T& a2) {
     // each step's columns are fetched one step ahead, so its gathers wait on L2 only
     int4 cnext = __ldg(reinterpret_cast<const int4*>(col + g0 * kStepSlots + 4 * lane));
     for (int64_t g = g0; g < g1; ++g) {
         const int4 c4 = cnext;
         if (g + 1 < g1) cnext = __ldg(reinterpret_cast<const int4*>(col + (g + 1) * kStepSlots + 4 * lane));
-        step_accum<T>(vals, c4, g, x, lane, a0, a1, a2);
+        step_accum<T>(vals, c4, g, x, lane, pad, a0, a1, a2);
     }
 }
 
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(kThr) k_spmv(SellDev A, const T* __restrict__ 
     for (int32_t sl = (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); sl < A.nslices;
          sl += (int32_t)((gridDim.x * blockDim.x) >> 5)) {
         T a0 = 0, a1 = 0, a2 = 0;
-        slice_accum<T>(vals, A.col, A.off[sl], A.off[sl + 1], p, lane, a0, a1, a2);
+        slice_accum<T>(vals, A.col, A.off[sl], A.off[sl + 1], p, lane, A.pad, a0, a1, a2);
         row_reduce<T, LPR>(a0, a1, a2);
         const int32_t row = A.rowid[(int64_t)sl * S + r];
         if (q == 0 && row >= 0) {
@@ -208,7 +210,7 @@ __global__ void __launch_bounds__(kThr) k_residual64(SellDev A, const double* __
     for (int32_t sl = (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); sl < A.nslices;
          sl += (int32_t)((gridDim.x * blockDim.x) >> 5)) {
         double a0 = 0, a1 = 0, a2 = 0;
-        slice_accum<double>(vals, A.col, A.off[sl], A.off[sl + 1], u, lane, a0, a1, a2);
+        slice_accum<double>(vals, A.col, A.off[sl], A.off[sl + 1], u, lane, A.pad, a0, a1, a2);
         row_reduce<double, LPR>(a0, a1, a2);
         const int32_t row = A.rowid[(int64_t)sl * (32 / LPR) + lane / LPR];
         if (lane % LPR == 0 && row >= 0) {

@@ -26,6 +26,7 @@ struct SellDev {
     const int32_t* rowid;   // [nslices * 32 / lpr] matrix row of each slice row, -1 when empty
     const int64_t* off;     // [nslices + 1] first step of each slice
     const int32_t* col;     // [steps * 128] node column of each slot
+    int32_t pad;            // column of the padding slots (the dummy node nb, zero values)
 };
 
 // Packed layout of a strictly lower or upper factor (PsellHost in common.hpp): one-step slices of
@@ -37,6 +38,7 @@ struct PsellDev {
     const uint4* head;     // [nslices] row-start bits of the 128 slots
     const int32_t* row0;   // [nslices + 1] first packed row of each slice
     const int32_t* rows;   // [nb] matrix row of each packed row
+    int32_t pad;           // column of the padding slots (the dummy node nb, zero values)
 };
 
 // Device-resident scalars of one PCG run.
