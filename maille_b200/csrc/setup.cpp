@@ -48,20 +48,38 @@ struct NodeGraph {
     std::vector<int64_t> off;   // [n + 1]
     std::vector<int32_t> adj;   // neighbours, self excluded, element-encounter order
     int64_t degree(int32_t v) const { return off[v + 1] - off[v]; }
+    // asks the cache for vertex v's neighbour list ahead of its use: the searches below visit
+    // vertices far from memory order, so each list would otherwise cost a DRAM miss
+    void prefetch(int32_t v) const {
+        const int32_t* a = adj.data() + off[v];
+        __builtin_prefetch(a);
+        __builtin_prefetch(a + 16);
+    }
+    void prefetch_offset(int32_t v) const { __builtin_prefetch(off.data() + v); }
+};
+constexpr int64_t kAhead = 16;  // vertices ahead of the one being visited (lists; offsets 2x)
+
+// Vertex sets as bit sets: 64 KB for half a million vertices, so the random tests of a
+// breadth-first search stay in the core's cache.
+struct Bits {
+    std::vector<uint64_t> w;
+    explicit Bits(int64_t n = 0) : w((size_t)((n + 63) / 64), 0ull) {}
+    bool test(int64_t i) const { return (w[(size_t)(i >> 6)] >> (i & 63)) & 1ull; }
+    void set(int64_t i) { w[(size_t)(i >> 6)] |= 1ull << (i & 63); }
 };
 
 // Breadth-first search from `start` that does not enter `excluded` vertices (bfs_levels,
 // solve.rs:248-270), on flat buffers reused across calls: returns the number of levels and keeps
 // the last level, in discovery order, in `last`.
 struct Bfs {
-    std::vector<int32_t> queue, mark, last;
-    int32_t stamp = 0;
-    explicit Bfs(int32_t n) : queue(n), mark(n, 0) {}
-    int32_t run(const NodeGraph& g, int32_t start, const std::vector<uint8_t>& excluded) {
-        ++stamp;
+    std::vector<int32_t> queue, last;
+    Bits seen;
+    explicit Bfs(int32_t n) : queue(n), seen(n) {}
+    int32_t run(const NodeGraph& g, int32_t start, const Bits& excluded) {
+        seen = excluded;
         int64_t head = 0, tail = 0;
         queue[tail++] = start;
-        mark[start] = stamp;
+        seen.set(start);
         int32_t levels = 0;
         int64_t level_begin = 0;
         for (;;) {
@@ -69,10 +87,12 @@ struct Bfs {
             ++levels;
             for (head = level_begin; head < level_end; ++head) {
                 const int32_t v = queue[head];
+                if (head + kAhead < tail) g.prefetch(queue[head + kAhead]);
+                if (head + 2 * kAhead < tail) g.prefetch_offset(queue[head + 2 * kAhead]);
                 for (int64_t p = g.off[v]; p < g.off[v + 1]; ++p) {
                     const int32_t w = g.adj[p];
-                    if (!excluded[w] && mark[w] != stamp) {
-                        mark[w] = stamp;
+                    if (!seen.test(w)) {
+                        seen.set(w);
                         queue[tail++] = w;
                     }
                 }
@@ -91,24 +111,26 @@ struct Bfs {
 // reverse_cuthill_mckee (solve.rs:200-245), applied to the node graph. order[new] = old.
 std::vector<int32_t> rcm(const NodeGraph& g) {
     const int32_t n = (int32_t)g.off.size() - 1;
-    std::vector<uint8_t> visited(n, 0);
+    std::vector<int32_t> deg(n);
+    for (int32_t v = 0; v < n; ++v) deg[v] = (int32_t)g.degree(v);
+    Bits visited(n);
     std::vector<int32_t> order;
     order.reserve(n);
     Bfs bfs(n);
     std::vector<int32_t> next;
     int32_t scan = 0;
     for (;;) {
-        while (scan < n && visited[scan]) ++scan;
+        while (scan < n && visited.test(scan)) ++scan;
         int32_t seed = -1;
         for (int32_t v = scan; v < n; ++v)
-            if (!visited[v] && (seed < 0 || g.degree(v) < g.degree(seed))) seed = v;
+            if (!visited.test(v) && (seed < 0 || deg[v] < deg[seed])) seed = v;
         if (seed < 0) break;
         int32_t start = seed;
         int32_t depth = bfs.run(g, start, visited);
         for (;;) {
             int32_t far = -1;
             for (int32_t v : bfs.last)
-                if (far < 0 || g.degree(v) < g.degree(far)) far = v;
+                if (far < 0 || deg[v] < deg[far]) far = v;
             if (far < 0) break;
             const std::vector<int32_t> keep_last = bfs.last;
             const int32_t far_depth = bfs.run(g, far, visited);
@@ -120,27 +142,29 @@ std::vector<int32_t> rcm(const NodeGraph& g) {
             depth = far_depth;
         }
         size_t head = order.size();
-        visited[start] = 1;
+        visited.set(start);
         order.push_back(start);
         while (head < order.size()) {
+            if (head + kAhead < order.size()) g.prefetch(order[head + kAhead]);
+            if (head + 2 * kAhead < order.size()) g.prefetch_offset(order[head + 2 * kAhead]);
             const int32_t v = order[head++];
             next.clear();
             for (int64_t p = g.off[v]; p < g.off[v + 1]; ++p)
-                if (!visited[g.adj[p]]) next.push_back(g.adj[p]);
+                if (!visited.test(g.adj[p])) next.push_back(g.adj[p]);
             // stable insertion sort by degree (neighbour lists are short)
             for (size_t i = 1; i < next.size(); ++i) {
                 const int32_t x = next[i];
-                const int64_t dx = g.degree(x);
+                const int32_t dx = deg[x];
                 size_t j = i;
-                while (j > 0 && g.degree(next[j - 1]) > dx) {
+                while (j > 0 && deg[next[j - 1]] > dx) {
                     next[j] = next[j - 1];
                     --j;
                 }
                 next[j] = x;
             }
             for (int32_t w : next)
-                if (!visited[w]) {
-                    visited[w] = 1;
+                if (!visited.test(w)) {
+                    visited.set(w);
                     order.push_back(w);
                 }
         }
@@ -149,23 +173,39 @@ std::vector<int32_t> rcm(const NodeGraph& g) {
     return order;
 }
 
-// Greedy colouring visiting vertices in `visit` order; returns colours.
-std::vector<int32_t> greedy_colour(const NodeGraph& g, const std::vector<int32_t>& visit) {
+// Greedy colouring visiting vertices in `visit` order (smallest colour no visited neighbour
+// holds); returns colours. A colour never exceeds the vertex degree, so while every degree is
+// below 255 the colours are kept in bytes, which keeps the neighbour lookups in cache.
+template <typename C>
+void greedy_colour_into(const NodeGraph& g, const std::vector<int32_t>& visit, std::vector<int32_t>& out) {
     const int32_t n = (int32_t)visit.size();
-    std::vector<int32_t> colour(n, -1);
+    const C none = (C)~(C)0;
+    std::vector<C> colour(n, none);
     std::vector<int32_t> stamp;  // stamp[c] == v: colour c used by a neighbour of v
-    for (int32_t v : visit) {
+    for (int32_t i = 0; i < n; ++i) {
+        const int32_t v = visit[i];
+        if (i + kAhead < n) g.prefetch(visit[i + kAhead]);
+        if (i + 2 * kAhead < n) g.prefetch_offset(visit[i + 2 * kAhead]);
         for (int64_t p = g.off[v]; p < g.off[v + 1]; ++p) {
-            const int32_t c = colour[g.adj[p]];
-            if (c >= 0) {
-                if ((size_t)c >= stamp.size()) stamp.resize(c + 1, -1);
+            const C c = colour[g.adj[p]];
+            if (c != none) {
+                if ((size_t)c >= stamp.size()) stamp.resize((size_t)c + 1, -1);
                 stamp[c] = v;
             }
         }
         int32_t c = 0;
         while ((size_t)c < stamp.size() && stamp[c] == v) ++c;
-        colour[v] = c;
+        colour[v] = (C)c;
     }
+    out.resize(n);
+    for (int32_t v = 0; v < n; ++v) out[v] = (int32_t)colour[v];
+}
+std::vector<int32_t> greedy_colour(const NodeGraph& g, const std::vector<int32_t>& visit) {
+    int64_t maxdeg = 0;
+    for (size_t v = 0; v + 1 < g.off.size(); ++v) maxdeg = std::max<int64_t>(maxdeg, g.degree((int32_t)v));
+    std::vector<int32_t> colour;
+    if (maxdeg < 255) greedy_colour_into<uint8_t>(g, visit, colour);
+    else greedy_colour_into<int32_t>(g, visit, colour);
     return colour;
 }
 
