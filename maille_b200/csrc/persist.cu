@@ -1,7 +1,9 @@
 // persist.cu -- the whole IC(0)-PCG iteration in one persistent cooperative kernel.
 //
 // One launch runs up to `chunk` iterations of Pcg::solve (iterative.rs:222-243): the SpMV, the
-// x/r update with the stopping test, the IC(0) forward and backward sweeps and the p update.
+// x/r update with the stopping test (fused into the IC(0) forward sweep in the mixed form: each
+// row takes x += alpha p, r -= alpha ap right before it is swept), the forward and backward
+// sweeps and the p update.
 // Phases are separated by grid-wide barriers; every block sums the per-block partials of a
 // reduction in the same fixed order, so alpha, beta and the stopping decisions are bit-identical
 // in every block and the whole grid takes the same branches. The mixed form adds the reliable
@@ -430,13 +432,29 @@ __device__ __forceinline__ uint32_t head_bits(uint4 h, int lane) {
 
 // The right-hand side and diagonal inverse of one sweep row: t = (FWD ? r : y) at the row; D is
 // 9 planes of nb entries, lower triangular (entries 0, 3, 4, 6, 7, 8).
-template <typename T, bool FWD>
+// The PCG update a fused forward sweep applies to each row before sweeping it.
+template <typename T>
+struct XrUpdate {
+    double alpha;
+    T *x, *r;
+    const T *p, *ap;
+};
+
+template <typename T, bool FWD, bool FUSED = false>
 struct RowIn {
     T t0, t1, t2, d0, d3, d4, d6, d7, d8;
-    T q0, q1, q2;  // backward: r at the row, for r . z
-    __device__ __forceinline__ void load(int32_t row, const T* D, int32_t nb, const T* r, const T* z) {
+    T q0, q1, q2;  // backward: r at the row, for r . z; fused forward: x at the row
+    T w0, w1, w2;  // fused forward: ap at the row
+    T s0, s1, s2;  // fused forward: p at the row
+    __device__ __forceinline__ void load(int32_t row, const T* D, int32_t nb, const T* r, const T* z,
+                                         const XrUpdate<T>& upd) {
         if (FWD) {
             node3_cg<T>(r, row, t0, t1, t2);
+            if (FUSED) {
+                node3_cg<T>(upd.x, row, q0, q1, q2);
+                node3_cg<T>(upd.ap, row, w0, w1, w2);
+                node3_cg<T>(upd.p, row, s0, s1, s2);
+            }
         } else {
             double v[3];
             rec_get(z, row, v);
@@ -451,9 +469,23 @@ struct RowIn {
         d7 = __ldg(d + 7 * (int64_t)nb);
         d8 = __ldg(d + 8 * (int64_t)nb);
     }
-    // forward: y = L_II^-1 (r - sum L y); backward: z = L_II^-T (y - sum L^T z) and r . z
+    // forward: y = L_II^-1 (r - sum L y); backward: z = L_II^-T (y - sum L^T z) and r . z.
+    // Fused forward: the row first takes its PCG update x += alpha p, r -= alpha ap (rounded to T
+    // like the separate update phase, iterative.rs:229-232), writes x and r, sweeps with the new r
+    // and returns its ||r||^2 share.
     __device__ __forceinline__ double finish(int32_t row, T a0, T a1, T a2, const T* r, T* z,
-                                             unsigned int epoch) const {
+                                             unsigned int epoch, const XrUpdate<T>& upd) const {
+        if (FWD && FUSED) {
+            const double al = upd.alpha;
+            const T r0 = (T)((double)t0 - al * (double)w0), r1 = (T)((double)t1 - al * (double)w1),
+                    r2 = (T)((double)t2 - al * (double)w2);
+            put3(upd.x, row, (T)((double)q0 + al * (double)s0), (T)((double)q1 + al * (double)s1),
+                 (T)((double)q2 + al * (double)s2));
+            put3(upd.r, row, r0, r1, r2);
+            const T u0 = r0 - a0, u1 = r1 - a1, u2 = r2 - a2;
+            publish_row(z, row, d0 * u0, d3 * u0 + d4 * u1, d6 * u0 + d7 * u1 + d8 * u2, epoch);
+            return (double)r0 * (double)r0 + (double)r1 * (double)r1 + (double)r2 * (double)r2;
+        }
         const T u0 = t0 - a0, u1 = t1 - a1, u2 = t2 - a2;
         if (FWD) {
             publish_row(z, row, d0 * u0, d3 * u0 + d4 * u1, d6 * u0 + d7 * u1 + d8 * u2, epoch);
@@ -500,11 +532,13 @@ __device__ __forceinline__ int4 lane_cols(const PsellDev& A, int64_t g, int lane
 // slots and sums them per row inside the lane; a segmented scan over the warp (fixed order)
 // carries the partial sums across lanes, and the owner of each row fetches the row's total from
 // the lane that holds its last slot. A multi-step slice holds one long row, summed over the warp.
-// Returns this thread's share of r . z (backward); `ok` turns false when a wait hit the spin limit.
-template <typename T, bool FWD>
+// Returns this thread's share of r . z (backward), or of ||r||^2 for a FUSED forward sweep, in
+// which each row first takes the PCG update of `upd` (x += alpha p, r -= alpha ap) and is swept
+// with the new r; `ok` turns false when a wait hit the spin limit.
+template <typename T, bool FWD, bool FUSED = false>
 __device__ __forceinline__ double sweep(const PsellDev& A, unsigned int epoch, const T* vals,
                                         const T* D, int32_t nb, const T* r, T* z, Stage<T>& st,
-                                        bool& ok) {
+                                        bool& ok, const XrUpdate<T>& upd = XrUpdate<T>{}) {
     const int lane = threadIdx.x & 31;
     const int32_t nw = (int32_t)(gridDim.x * kPW), n = A.nslices;
     double loc = 0.0;
@@ -514,8 +548,8 @@ __device__ __forceinline__ double sweep(const PsellDev& A, unsigned int epoch, c
     int4 c0 = lane_cols(A, m0.g0, lane);
     int32_t row0 = lane < m0.r1 - m0.r0 ? __ldg(A.rows + m0.r0 + lane) : -1;
     if (lane == 0) stage_step(vals, m0.g0, st);
-    RowIn<T, FWD> in0{};
-    if (row0 >= 0) in0.load(row0, D, nb, r, z);
+    RowIn<T, FWD, FUSED> in0{};
+    if (row0 >= 0) in0.load(row0, D, nb, r, z, upd);
     for (; k < n; k += nw) {
         const bool more = k + nw < n;
         const SliceMeta m2 = slice_meta(A, k + 2 * nw);
@@ -584,10 +618,10 @@ __device__ __forceinline__ double sweep(const PsellDev& A, unsigned int epoch, c
             }
             lanes_sum<T, 32>(a0, a1, a2);
         }
-        if (row0 >= 0) loc += in0.finish(row0, a0, a1, a2, r, z, epoch);
+        if (row0 >= 0) loc += in0.finish(row0, a0, a1, a2, r, z, epoch, upd);
         // the next slice's right-hand sides and diagonal blocks (its rows arrived meanwhile)
-        RowIn<T, FWD> in1{};
-        if (row1 >= 0) in1.load(row1, D, nb, r, z);
+        RowIn<T, FWD, FUSED> in1{};
+        if (row1 >= 0) in1.load(row1, D, nb, r, z, upd);
         m0 = m1;
         m1 = m2;
         c0 = c1;
@@ -723,6 +757,8 @@ __global__ void __launch_bounds__(kPW * 32, 2) k_pcg(PcgArgs<T> a, int init) {
     int it = 0;
     while (!v.done && (init ? it < 1 : it < a.chunk)) {
         double loc;
+        bool ok = true;
+        bool need_fwd = true;  // the plain forward sweep below (not fused with the update)
         if (!init) {
             // ap = K p, alpha = rz / p.ap (iterative.rs:223-228)
             if constexpr (MIXED)
@@ -740,26 +776,45 @@ __global__ void __launch_bounds__(kPW * 32, 2) k_pcg(PcgArgs<T> a, int init) {
                 break;
             }
             v.alpha = v.rz / pap;
-            // x += alpha p, r -= alpha ap, ||r||^2 (iterative.rs:229-233)
-            loc = 0.0;
-            for (int64_t i = tid; i < a.nb; i += nthreads) {
-                double xv[4], rv[4], pv[4], av[4];
-                get4(a.x, i, xv);
-                get4(a.r, i, rv);
-                get4(a.p, i, pv);
-                get4(a.ap, i, av);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    xv[c] = (double)(T)(xv[c] + v.alpha * pv[c]);
-                    rv[c] = (double)(T)(rv[c] - v.alpha * av[c]);
-                    loc += rv[c] * rv[c];
+            // x += alpha p, r -= alpha ap and ||r||^2 (iterative.rs:229-233). Mixed form: fused into
+            // the forward sweep, each row taking its update right before it is swept with the new
+            // r (one grid pass and one barrier less per iteration). Plain form: a separate pass (the
+            // FP64 sweep's extra registers cost more than the pass; measured both ways).
+            if constexpr (MIXED) {
+                v.epoch += 1;
+                loc = sweep<T, true, true>(a.L, v.epoch, a.Lv, a.D, a.nb, a.r, a.z, stage, ok,
+                                           XrUpdate<T>{v.alpha, a.x, a.r, a.p, a.ap});
+                if (!ok) atomicExch(timeout, 1);
+                publish(loc, a.partials, 1, sh);
+                grid.sync();
+                mark(3);
+                if (__ldcg(timeout)) {
+                    v.done = 1;
+                    v.status = 3;
+                    break;
                 }
-                set4(a.x, i, xv);
-                set4(a.r, i, rv);
+                need_fwd = false;
+            } else {
+                loc = 0.0;
+                for (int64_t i = tid; i < a.nb; i += nthreads) {
+                    double xv[4], rv[4], pv[4], av[4];
+                    get4(a.x, i, xv);
+                    get4(a.r, i, rv);
+                    get4(a.p, i, pv);
+                    get4(a.ap, i, av);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        xv[c] = (double)(T)(xv[c] + v.alpha * pv[c]);
+                        rv[c] = (double)(T)(rv[c] - v.alpha * av[c]);
+                        loc += rv[c] * rv[c];
+                    }
+                    set4(a.x, i, xv);
+                    set4(a.r, i, rv);
+                }
+                publish(loc, a.partials, 1, sh);
+                grid.sync();
+                mark(1);
             }
-            publish(loc, a.partials, 1, sh);
-            grid.sync();
-            mark(1);
             v.rr = grid_total(a.partials, 1);
             const bool small = sqrt(v.rr) <= v.tol * sqrt(v.bb);
             if (!MIXED) {
@@ -809,14 +864,16 @@ __global__ void __launch_bounds__(kPW * 32, 2) k_pcg(PcgArgs<T> a, int init) {
                 }
                 grid.sync();
                 mark(2);
+                need_fwd = true;  // the fused sweep ran on the recurrence residual: again on the true one
             }
         }
         // z = (L L^T)^-1 r (Csr::precondition, iterative.rs:173-188): dataflow sweeps
-        bool ok = true;
-        v.epoch += 1;
-        sweep<T, true>(a.L, v.epoch, a.Lv, a.D, a.nb, a.r, a.z, stage, ok);
-        grid.sync();
-        mark(3);
+        if (need_fwd) {
+            v.epoch += 1;
+            sweep<T, true>(a.L, v.epoch, a.Lv, a.D, a.nb, a.r, a.z, stage, ok);
+            grid.sync();
+            mark(3);
+        }
         v.epoch += 1;
         loc = sweep<T, false>(a.U, v.epoch, a.Uv, a.D, a.nb, a.r, a.z, stage, ok);
         if (!ok) atomicExch(timeout, 1);
