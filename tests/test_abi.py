@@ -109,6 +109,13 @@ def test_invalid_inputs_are_rejected_before_any_device_work(lib):
     assert _solve_status(lib, p) == _lib.MAILLE_INVALID_INPUT
 
 
+def test_handle_entry_points_reject_null_arguments_without_device_work(lib):
+    out = np.zeros(6)
+    assert lib.maille_gpu_nodal_stresses(None, _lib.ptr(out, _lib._d), _lib.ptr(out, _lib._d)) == _lib.MAILLE_INVALID_INPUT
+    assert lib.maille_gpu_wait_selftest(0, 1, None) == _lib.MAILLE_INVALID_INPUT
+    assert "null" in _lib.last_error()
+
+
 def test_missing_device_is_a_cuda_error_not_a_fallback(lib):
     if lib.maille_gpu_device_count() > 0:
         pytest.skip("a device is visible")
