@@ -754,11 +754,9 @@ int32_t maille_gpu_spmv_device(MailleGpuHandle* h, int32_t precision, int32_t co
         CK(cudaSetDevice(h->device));
         for (int32_t k = 0; k < count; ++k) {
             if (precision == MAILLE_MIXED)
-                launch_spmv<float>(h->sk.dev(), h->Ks32, h->p32, h->ap32, h->scal, h->partials,
-                                   h->spmv_grid, true, h->st);
+                launch_spmv<float>(h->sk.dev(), h->Ks32, h->p32, h->ap32, h->spmv_grid, h->st);
             else
-                launch_spmv<double>(h->sk.dev(), h->Ks64, h->p64, h->ap64, h->scal, h->partials,
-                                    h->spmv_grid, true, h->st);
+                launch_spmv<double>(h->sk.dev(), h->Ks64, h->p64, h->ap64, h->spmv_grid, h->st);
         }
         CK(cudaGetLastError());
     } catch (const CudaFailure& e) {
@@ -775,8 +773,7 @@ int32_t maille_gpu_multiply(MailleGpuHandle* h, const double* x, double* y) {
         const int64_t n3 = 3 * h->n_nodes;
         CK(cudaMemcpyAsync(h->y_full, x, n3 * sizeof(double), cudaMemcpyHostToDevice, h->st));
         launch_build_rhs(h->sym.nb, h->perm, h->fixmask, h->y_full, nullptr, h->p64, h->st);
-        launch_spmv<double>(h->sk.dev(), h->Ks64, h->p64, h->ap64, h->scal, h->partials,
-                            h->spmv_grid, true, h->st);
+        launch_spmv<double>(h->sk.dev(), h->Ks64, h->p64, h->ap64, h->spmv_grid, h->st);
         CK(cudaMemsetAsync(h->react, 0, n3 * sizeof(double), h->st));
         launch_gather_u(h->n_nodes, h->inv, h->fixed, h->react, h->ap64, h->y_full, h->st);
         CK(cudaGetLastError());

@@ -119,46 +119,21 @@ __device__ __forceinline__ void row_reduce(T& a0, T& a1, T& a2) {
     }
 }
 
-// ap = K p (Csr::multiply, iterative.rs:131-142, as a gather on the full symmetric pattern),
-// p . ap reduced; the last block sets alpha = rz / (p . ap) and counts the iteration, or flags
-// SINGULAR on curvature <= 0 / NaN (iterative.rs:223-228). `standalone` launches (timing) skip
-// the done check and the scalar update.
+// ap = K p (Csr::multiply, iterative.rs:131-142, as a gather on the full symmetric pattern) on its
+// own: the handle's multiply entry point and the SpMV timing launches. (Inside the solve the SpMV
+// is a phase of the persistent kernel, persist.cu.)
 template <typename T, int LPR>
 __global__ void __launch_bounds__(kThr) k_spmv(SellDev A, const T* __restrict__ vals,
-                                                const T* __restrict__ p, T* __restrict__ ap,
-                                                PcgScalars* s, double* partials, int standalone) {
-    __shared__ double sh[kWarp];
-    if (!standalone && s->done) return;
+                                                const T* __restrict__ p, T* __restrict__ ap) {
     const int lane = threadIdx.x & 31, r = lane / LPR, q = lane % LPR;
     constexpr int S = 32 / LPR;
-    double loc = 0.0;
     for (int32_t sl = (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); sl < A.nslices;
          sl += (int32_t)((gridDim.x * blockDim.x) >> 5)) {
         T a0 = 0, a1 = 0, a2 = 0;
         slice_accum<T>(vals, A.col, A.off[sl], A.off[sl + 1], p, lane, A.pad, a0, a1, a2);
         row_reduce<T, LPR>(a0, a1, a2);
         const int32_t row = A.rowid[(int64_t)sl * S + r];
-        if (q == 0 && row >= 0) {
-            store_node(ap, row, a0, a1, a2);
-            T p0, p1, p2;
-            node3(p, row, p0, p1, p2);
-            loc += (double)p0 * (double)a0 + (double)p1 * (double)a1 + (double)p2 * (double)a2;
-        }
-    }
-    if (standalone) return;
-    if (publish_partial(loc, partials, &s->ticket[0], sh)) {
-        const double pap = gather_sum(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            s->pap = pap;
-            s->iter += 1;
-            if (isnan(pap) || pap <= 0.0) {
-                s->status = 1;
-                s->done = 1;
-            } else {
-                s->alpha = s->rz / pap;
-            }
-            s->ticket[0] = 0;
-        }
+        if (q == 0 && row >= 0) store_node(ap, row, a0, a1, a2);
     }
 }
 
@@ -189,37 +164,6 @@ __global__ void k_norm2(int64_t n, const T* __restrict__ v, double* partials, un
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
          k += (int64_t)gridDim.x * blockDim.x)
         loc += (double)v[k] * (double)v[k];
-    if (publish_partial(loc, partials, ticket, sh)) {
-        const double tot = gather_sum(partials, gridDim.x, sh);
-        if (threadIdx.x == 0) {
-            *out = tot;
-            *ticket = 0;
-        }
-    }
-}
-
-template <int LPR>
-__global__ void __launch_bounds__(kThr) k_residual64(SellDev A, const double* __restrict__ vals,
-                                                      const double* __restrict__ b,
-                                                      const double* __restrict__ u,
-                                                      double* __restrict__ r, double* partials,
-                                                      unsigned int* ticket, double* out) {
-    __shared__ double sh[kWarp];
-    const int lane = threadIdx.x & 31;
-    double loc = 0.0;
-    for (int32_t sl = (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); sl < A.nslices;
-         sl += (int32_t)((gridDim.x * blockDim.x) >> 5)) {
-        double a0 = 0, a1 = 0, a2 = 0;
-        slice_accum<double>(vals, A.col, A.off[sl], A.off[sl + 1], u, lane, A.pad, a0, a1, a2);
-        row_reduce<double, LPR>(a0, a1, a2);
-        const int32_t row = A.rowid[(int64_t)sl * (32 / LPR) + lane / LPR];
-        if (lane % LPR == 0 && row >= 0) {
-            const double q0 = b[4 * (int64_t)row] - a0, q1 = b[4 * (int64_t)row + 1] - a1,
-                         q2 = b[4 * (int64_t)row + 2] - a2;
-            store_node(r, row, q0, q1, q2);
-            loc += q0 * q0 + q1 * q1 + q2 * q2;
-        }
-    }
     if (publish_partial(loc, partials, ticket, sh)) {
         const double tot = gather_sum(partials, gridDim.x, sh);
         if (threadIdx.x == 0) {
@@ -267,10 +211,9 @@ __global__ void k_cast(int64_t n, const double* __restrict__ a, float* __restric
     }
 
 template <typename T>
-void launch_spmv(const SellDev& A, const T* vals, const T* p, T* ap, PcgScalars* s,
-                 double* partials, int grid, bool standalone, cudaStream_t st) {
+void launch_spmv(const SellDev& A, const T* vals, const T* p, T* ap, int grid, cudaStream_t st) {
     counted();
-    MAILLE_LPR_SWITCH(A.lpr, k_spmv, grid, kThr, 0, st>>>(A, vals, p, ap, s, partials, standalone ? 1 : 0));
+    MAILLE_LPR_SWITCH(A.lpr, k_spmv, grid, kThr, 0, st>>>(A, vals, p, ap));
 }
 
 void launch_pcg_init(PcgScalars* s, double tol, int32_t max_iter, double delta, cudaStream_t st) {
@@ -283,18 +226,6 @@ void launch_norm2(int64_t n, const T* v, double* partials, unsigned int* ticket,
                   cudaStream_t st) {
     counted();
     k_norm2<T><<<grid_for(n, kThr, 148 * 4), kThr, 0, st>>>(n, v, partials, ticket, out);
-}
-
-void launch_residual64(const SellDev& A, const double* vals, const double* b, const double* u,
-                       double* r, double* partials, unsigned int* ticket, double* out, int grid,
-                       cudaStream_t st) {
-    counted();
-    switch (A.lpr) {
-        case 1: k_residual64<1><<<grid, kThr, 0, st>>>(A, vals, b, u, r, partials, ticket, out); break;
-        case 2: k_residual64<2><<<grid, kThr, 0, st>>>(A, vals, b, u, r, partials, ticket, out); break;
-        case 4: k_residual64<4><<<grid, kThr, 0, st>>>(A, vals, b, u, r, partials, ticket, out); break;
-        default: k_residual64<8><<<grid, kThr, 0, st>>>(A, vals, b, u, r, partials, ticket, out); break;
-    }
 }
 
 template <typename T>
@@ -316,8 +247,7 @@ void launch_cast(int64_t n, const double* a, float* b, cudaStream_t st) {
 }
 
 #define MAILLE_INST(T)                                                                          \
-    template void launch_spmv<T>(const SellDev&, const T*, const T*, T*, PcgScalars*, double*,  \
-                                 int, bool, cudaStream_t);                                      \
+    template void launch_spmv<T>(const SellDev&, const T*, const T*, T*, int, cudaStream_t);   \
     template void launch_norm2<T>(int64_t, const T*, double*, unsigned int*, double*,           \
                                   cudaStream_t);                                                \
     template void launch_sell_fill<T>(int64_t, const int32_t*, const double*, T*, cudaStream_t); \

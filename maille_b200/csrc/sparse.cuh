@@ -51,17 +51,13 @@ struct PcgScalars {
     unsigned int epoch;  // sweep counter of the row-ready flags; never reset (monotonic)
 };
 
+// ap = K p on its own (the persistent kernel has its own SpMV phase)
 template <typename T>
-void launch_spmv(const SellDev& A, const T* vals, const T* p, T* ap, PcgScalars* s,
-                 double* partials, int grid, bool standalone, cudaStream_t st);
+void launch_spmv(const SellDev& A, const T* vals, const T* p, T* ap, int grid, cudaStream_t st);
 void launch_pcg_init(PcgScalars* s, double tol, int32_t max_iter, double delta, cudaStream_t st);
 template <typename T>
 void launch_norm2(int64_t n, const T* v, double* partials, unsigned int* ticket, double* out,
                   cudaStream_t st);
-// r = b - A u in FP64 with ||r||^2 into *out (A: SELL FP64)
-void launch_residual64(const SellDev& A, const double* vals, const double* b, const double* u,
-                       double* r, double* partials, unsigned int* ticket, double* out, int grid,
-                       cudaStream_t st);
 // vals[slot layout] = csr[src[slot]] (9 entries per block, 0 for padding)
 template <typename T>
 void launch_sell_fill(int64_t steps, const int32_t* src, const double* csr, T* vals, cudaStream_t st);
