@@ -276,3 +276,75 @@ def traction_loads(prob: Problem, axis: int, value: float, traction: np.ndarray)
     for c in range(3):
         out[c::3, :] = share[:, None] * traction[None, :, c]
     return out
+
+
+# --- transient heat conduction -------------------------------------------------------------------
+
+@dataclass
+class ThermalProblem:
+    """A transient thermal Tet4/Tet10 problem (Model with Analysis::Thermal and a transient Step,
+    model.rs:621-706) in the layout of the C ABI's MailleThermalProblem."""
+    coords: np.ndarray                   # (N, 3) float64
+    conn: np.ndarray                     # (E, npe) int64
+    conductivity: np.ndarray             # (E,) k
+    rho_c: np.ndarray                    # (E,) density x specific heat
+    fixed: np.ndarray                    # (N,) uint8 imposed temperature
+    imposed: np.ndarray                  # (N,) float64
+    loads: np.ndarray                    # (N,) float64 nodal heat loads
+    initial: np.ndarray                  # (N,) float64 temperature at t = 0
+    time_period: float = 1.0
+    increments: int = 1
+    theta: float = 1.0
+    s_elem: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    s_value: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float64))
+    c_elem: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    c_face: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    c_film: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float64))
+    c_sink: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float64))
+    name: str = ""
+
+    @property
+    def time_step(self) -> float:
+        """Step::time_step (model.rs:171-173)."""
+        return self.time_period / self.increments
+
+    @property
+    def npe(self) -> int:
+        return int(self.conn.shape[1])
+
+    @property
+    def n_nodes(self) -> int:
+        return int(self.coords.shape[0])
+
+    @property
+    def n_elems(self) -> int:
+        return int(self.conn.shape[0])
+
+    @property
+    def free_nodes(self) -> int:
+        return int(self.fixed.size - np.count_nonzero(self.fixed))
+
+
+def thermal_cube(cells: int = 40, quadratic: bool = True, increments: int = 10,
+                 time_period: float = 0.1, theta: float = 1.0) -> ThermalProblem:
+    """Unit cube heated from below and cooled on top: cells^3 x 6 tets (Tet10 when `quadratic`),
+    per-element conductivity lognormal (median 1, sigma_log 0.5, seeded), rho_c = 1, T = 100
+    imposed on z = 0, convection h = 10 to T_inf = 20 on every face of z = 1, a uniform source
+    of 50 in every element, T = 20 at t = 0; `increments` backward-Euler steps (theta = 1) over
+    `time_period`. 40^3 Tet10: 531 441 nodes, 384 000 tets, 524 800 free nodes."""
+    nodes, tets = box_grid((cells,) * 3, (1.0, 1.0, 1.0))
+    conn = tets
+    if quadratic:
+        nodes, conn = to_quadratic_tet(nodes, tets)
+    n, ne = nodes.shape[0], conn.shape[0]
+    fixed = (np.abs(nodes[:, 2]) < 1e-12).astype(np.uint8)
+    imposed = np.where(fixed != 0, 100.0, 0.0)
+    ce, cf = faces_on(nodes, conn, 2, 1.0)
+    k = np.exp(0.5 * normal(stream=7, count=ne))
+    return ThermalProblem(coords=nodes, conn=conn, conductivity=k, rho_c=np.ones(ne), fixed=fixed,
+                          imposed=imposed, loads=np.zeros(n), initial=np.full(n, 20.0),
+                          time_period=time_period, increments=increments, theta=theta,
+                          s_elem=np.arange(ne, dtype=np.int64), s_value=np.full(ne, 50.0),
+                          c_elem=ce, c_face=cf, c_film=np.full(ce.shape[0], 10.0),
+                          c_sink=np.full(ce.shape[0], 20.0),
+                          name=f"{'tet10' if quadratic else 'tet4'}_{cells}^3_transient")

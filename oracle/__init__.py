@@ -75,6 +75,14 @@ def lib():
         L.oracle_neo_hookean_tet4.argtypes = [_d, ctypes.c_double, ctypes.c_double, _d, _d, _d, _d, _d]
         L.oracle_neo_hookean_tet4.restype = ctypes.c_int
         L.oracle_nodal_stresses.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int64, _i64, _d, _d]
+        L.oracle_thermal_transient.argtypes = [
+            ctypes.c_int64, _d, ctypes.c_int, ctypes.c_int64, _i64, _d, _d, _u8, _d, _d,
+            ctypes.c_int64, _i64, _d, ctypes.c_int64, _i64, _i32, _d, _d, _d,
+            ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_int, ctypes.c_double,
+            ctypes.c_int64, _d, _d, _d, _d, _i64, _d]
+        L.oracle_thermal_transient.restype = ctypes.c_int
+        L.oracle_tetra14.argtypes = [_d]
+        L.oracle_thermal_element.argtypes = [ctypes.c_int, _d, ctypes.c_double, ctypes.c_double, _d, _d]
         _lib = L
     return _lib
 
@@ -292,3 +300,56 @@ def nodal_stresses(prob, gauss):
     lib().oracle_nodal_stresses(prob.coords.shape[0], conn.shape[1], conn.shape[0], _p(conn, _i64),
                                 _p(g, _d), _p(out, _d))
     return out
+
+
+def tetra14():
+    """TETRA_14 as a (14, 4) array of (xi, eta, zeta, weight)."""
+    out = np.zeros((14, 4))
+    lib().oracle_tetra14(_p(out, _d))
+    return out
+
+
+def thermal_element(coords, k, rho_c):
+    """(conduction K_e, capacity C_e) of one Tet4/Tet10 element (coords (npe, 3))."""
+    c = _c(coords, np.float64)
+    npe = c.shape[0]
+    ke = np.zeros((npe, npe))
+    ce = np.zeros((npe, npe))
+    lib().oracle_thermal_element(npe, _p(c, _d), k, rho_c, _p(ke, _d), _p(ce, _d))
+    return ke, ce
+
+
+def thermal_transient(prob, solver: int = 0, tol: float = 1e-12, max_iter: int = 10000,
+                      fluxes: bool = True):
+    """Model::solve_step of a meshgen.ThermalProblem on the CPU. solver: 0 Auto, 1 Direct,
+    2 Iterative. Returns a dict with status, temps (S + 1, N), reactions (S + 1, N), fluxes
+    (S + 1, E, ngp, 6) or None, f, iterations (S,), total_iterations, rel_residual, shift,
+    free, nnz, ms_setup, ms_factor, ms_steps, wall_s."""
+    L = lib()
+    coords = _c(prob.coords, np.float64)
+    conn = _c(prob.conn, np.int64)
+    n, (ne, npe) = coords.shape[0], conn.shape
+    ng = 1 if npe == 4 else 4
+    steps = int(prob.increments)
+    temps = np.zeros((steps + 1, n))
+    reac = np.zeros((steps + 1, n))
+    flux = np.zeros((steps + 1, ne, ng, 6)) if fluxes else None
+    f = np.zeros(n)
+    its = np.zeros(max(steps, 1), np.int64)
+    info = np.zeros(8)
+    se, sv = _c(prob.s_elem, np.int64), _c(prob.s_value, np.float64)
+    ce, cf = _c(prob.c_elem, np.int64), _c(prob.c_face, np.int32)
+    ch, cs = _c(prob.c_film, np.float64), _c(prob.c_sink, np.float64)
+    t0 = time.perf_counter()
+    s = L.oracle_thermal_transient(
+        n, _p(coords, _d), npe, ne, _p(conn, _i64), _p(_c(prob.conductivity, np.float64), _d),
+        _p(_c(prob.rho_c, np.float64), _d), _p(_c(prob.fixed, np.uint8), _u8),
+        _p(_c(prob.imposed, np.float64), _d), _p(_c(prob.loads, np.float64), _d),
+        se.size, _p(se, _i64), _p(sv, _d), ce.size, _p(ce, _i64), _p(cf, _i32), _p(ch, _d), _p(cs, _d),
+        _p(_c(prob.initial, np.float64), _d), prob.time_step, prob.theta, steps, solver, tol,
+        max_iter, _p(temps, _d), _p(reac, _d), _p(flux, _d), _p(f, _d), _p(its, _i64), _p(info, _d))
+    wall = time.perf_counter() - t0
+    return dict(status=s, temps=temps, reactions=reac, fluxes=flux, f=f, iterations=its[:steps],
+                total_iterations=int(info[0]), rel_residual=info[1], shift=info[2],
+                free=int(info[3]), nnz=int(info[4]), ms_setup=info[5], ms_factor=info[6],
+                ms_steps=info[7], wall_s=wall)

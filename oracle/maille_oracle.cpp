@@ -982,6 +982,143 @@ struct QuasiStatic {
     }
 };
 
+// --- transient heat conduction: model.rs:621-706 (solve_step_with), assembly.rs:386-484 and
+// 485-626 (thermal element matrices, sources, convection), element.rs:338-357 and 451-506 -----
+
+// TETRA_14, quadrature.rs:140-177: the published 14-point degree-5 rule on the reference
+// tetrahedron (weights sum to 1/6), points in the reference's order: two orbits of 4 points
+// (a, a, a) and their permutations with 1 - 3a, one orbit of 6 points on the edge midlines.
+constexpr double T14_A1 = 0.09273525031089142, T14_W1 = 0.01224884051939372;
+constexpr double T14_A2 = 0.3108859192633008, T14_W2 = 0.01878132095300283;
+constexpr double T14_B = 0.04550370412564851, T14_W3 = 0.00709100346284674;
+struct Tetra14 {
+    TetGP p[14];
+    Tetra14() {
+        int k = 0;
+        auto orbit4 = [&](double a, double w) {  // (a, a, a) and its three moves to 1 - 3a
+            const double c = 1.0 - 3.0 * a;
+            p[k++] = {a, a, a, w};
+            p[k++] = {c, a, a, w};
+            p[k++] = {a, c, a, w};
+            p[k++] = {a, a, c, w};
+        };
+        orbit4(T14_A1, T14_W1);
+        orbit4(T14_A2, T14_W2);
+        const double b = T14_B, d = 0.5 - T14_B;  // the six (b, b, d) permutations
+        p[k++] = {b, b, d, T14_W3};
+        p[k++] = {b, d, b, T14_W3};
+        p[k++] = {d, b, b, T14_W3};
+        p[k++] = {d, d, b, T14_W3};
+        p[k++] = {d, b, d, T14_W3};
+        p[k++] = {b, d, d, T14_W3};
+    }
+};
+const Tetra14 TETRA_14;
+
+// GaussData of solid_gauss, element.rs:338-357: weight w |det J|, N, dN/dx, position sum N x.
+struct GaussData {
+    double w;
+    double n[10];
+    double g[10][3];
+    double at[3];
+};
+
+int solid_gauss(int npe, const double (*c)[3], const TetGP* rule, int ng, GaussData* out) {
+    double dn[10][3];
+    for (int gp = 0; gp < ng; ++gp) {
+        GaussData& d = out[gp];
+        tet_shape(npe, rule[gp].xi, rule[gp].eta, rule[gp].zeta, d.n, dn);
+        const double det = mapping3d(npe, c, dn, d.g);
+        d.w = rule[gp].w * std::fabs(det);
+        for (int k = 0; k < 3; ++k) {
+            double s = d.n[0] * c[0][k];
+            for (int a = 1; a < npe; ++a) s = s + d.n[a] * c[a][k];
+            d.at[k] = s;
+        }
+    }
+    return ng;
+}
+
+// conduction, element.rs:451-463: K = sum_g w k grad N grad N^T (npe x npe row-major)
+void conduction(int npe, const GaussData* p, int ng, double k, double* ke) {
+    std::fill(ke, ke + npe * npe, 0.0);
+    for (int gp = 0; gp < ng; ++gp)
+        for (int a = 0; a < npe; ++a)
+            for (int b = 0; b < npe; ++b) {
+                const double* ga = p[gp].g[a];
+                const double* gb = p[gp].g[b];
+                double s = ga[0] * gb[0];
+                s = s + ga[1] * gb[1];
+                s = s + ga[2] * gb[2];
+                ke[a * npe + b] += p[gp].w * k * s;
+            }
+}
+
+// capacity, element.rs:465-477: C = sum_g w rho_c N N^T, on a rule exact for N N^T
+// (element_capacity, assembly.rs:413-433: TETRA_4 for Tet4, TETRA_14 for Tet10)
+void capacity(int npe, const GaussData* p, int ng, double rho_c, double* ce) {
+    std::fill(ce, ce + npe * npe, 0.0);
+    for (int gp = 0; gp < ng; ++gp)
+        for (int a = 0; a < npe; ++a)
+            for (int b = 0; b < npe; ++b) ce[a * npe + b] += p[gp].w * rho_c * p[gp].n[a] * p[gp].n[b];
+}
+
+// FaceConvection of face_convection, assembly.rs:486-509 and 595-626: matrix = h int N N^T dS,
+// load = h T_inf int N dS over the face rule of face_rule (the geometry of face_pressure above).
+struct Convection {
+    int nn = 0;
+    int pos[6];
+    double matrix[36];
+    double load[6];
+};
+
+bool face_convection(int npe, const double (*ecoords)[3], int face, double film, double sink, Convection& out) {
+    const int nn = face_positions(npe, face, out.pos);
+    if (nn == 0) return false;
+    out.nn = nn;
+    double c[6][3];
+    for (int k = 0; k < nn; ++k)
+        for (int q = 0; q < 3; ++q) c[k][q] = ecoords[out.pos[k]][q];
+    double u[3], v[3];
+    for (int k = 0; k < 3; ++k) {
+        u[k] = c[1][k] - c[0][k];
+        v[k] = c[2][k] - c[0][k];
+    }
+    const double cross[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2],
+                             u[0] * v[1] - u[1] * v[0]};
+    double sq = cross[0] * cross[0];
+    sq = sq + cross[1] * cross[1];
+    sq = sq + cross[2] * cross[2];
+    const double twice_area = std::sqrt(sq);
+    const TriGP* rule = (nn == 3) ? TRIANGLE_3 : TRIANGLE_6;
+    const int np = (nn == 3) ? 3 : 6;
+    std::fill(out.matrix, out.matrix + 36, 0.0);
+    std::fill(out.load, out.load + 6, 0.0);
+    for (int g = 0; g < np; ++g) {
+        const double w = rule[g].w * twice_area;
+        double nv[6];
+        tri_values(nn, rule[g].xi, rule[g].eta, nv);
+        for (int a = 0; a < nn; ++a) {
+            out.load[a] += film * sink * w * nv[a];
+            for (int b = 0; b < nn; ++b) out.matrix[a * nn + b] += film * w * nv[a] * nv[b];
+        }
+    }
+    return true;
+}
+
+// heat_fluxes, element.rs:480-506: per Gauss point x, y, z, qx, qy, qz with q = -k grad T
+void heat_fluxes(int npe, const GaussData* p, int ng, double k, const double* t_e, double* out) {
+    for (int gp = 0; gp < ng; ++gp) {
+        double* o = out + 6 * gp;
+        for (int c = 0; c < 3; ++c) o[c] = p[gp].at[c];
+        for (int c = 0; c < 3; ++c) {
+            double s = p[gp].g[0][c] * t_e[0];
+            for (int a = 1; a < npe; ++a) s = s + p[gp].g[a][c] * t_e[a];
+            o[3 + c] = -k * s;
+        }
+    }
+}
+
 }  // namespace
 
 // ============================================================================================
@@ -1431,6 +1568,263 @@ int oracle_neo_hookean_tet4(const double* coords12, double lambda, double mu, co
     for (int a = 0; a < 4; ++a)
         for (int k = 0; k < 3; ++k) c[a][k] = coords12[3 * a + k];
     return neo_hookean_tet4(c, lambda, mu, ue, fe, ke, dfe_dmu, dfe_dlambda) ? OK : INVALID;
+}
+
+// Model::solve_step (model.rs:621-706) of a Tet4/Tet10 thermal model on the CPU: the theta-method
+// (C/dt + theta K) T_{n+1} = (C/dt - (1 - theta) K) T_n + F with K = conduction + convection,
+// one factorisation (FreeSystem::new) reused by every increment, reactions
+// R = (left T_{n+1} - right T_n - F) on imposed nodes and heat fluxes per increment.
+//   per node: fixed, imposed, loads (nodal heat loads Load{dof: T}); per element: conductivity,
+//   rho_c (density x specific heat); sources (element, value) (HeatSource, element_heat_source);
+//   convection (element, face, film, sink) (Convection, face_convection).
+//   initial: T at t = 0 (imposed values replace it at fixed nodes). solver: 0 Auto, 1 Direct,
+//   2 Iterative. tol: PCG tolerance (0 selects 1e-12).
+//   out: temps / reactions [(increments + 1) n_nodes], fluxes [(increments + 1) n_elems ngp 6]
+//   (x, y, z, qx, qy, qz), f_out [n_nodes] the assembled F, iterations [increments],
+//   info[0..7] = total PCG iterations, largest final relative residual, shift, free nodes,
+//   nnz(L), ms setup, ms factor, ms increments.
+// With rho_c = 0, theta = 1 and one increment the left matrix is K and the carried vector is
+// zero: that run is the steady solve (Model::solve with Analysis::Thermal, model.rs:548-610).
+int oracle_thermal_transient(int64_t n_nodes, const double* coords, int npe, int64_t n_elems,
+                             const int64_t* conn, const double* conductivity, const double* rho_c,
+                             const uint8_t* fixed, const double* imposed, const double* loads,
+                             int64_t n_src, const int64_t* s_elem, const double* s_value,
+                             int64_t n_conv, const int64_t* c_elem, const int32_t* c_face,
+                             const double* c_film, const double* c_sink, const double* initial,
+                             double dt, double theta, int64_t increments, int solver, double tol,
+                             int64_t max_iter, double* temps, double* reactions, double* fluxes,
+                             double* f_out, int64_t* iterations, double* info) {
+    if (tol <= 0.0) tol = TOLERANCE;
+    if (max_iter <= 0) max_iter = (int64_t)MAX_ITERATIONS;
+    if (npe != 4 && npe != 10) return INVALID;
+    const double t0 = now_ms();
+    const size_t n = (size_t)n_nodes, ne = (size_t)n_elems;
+    auto node = [&](size_t e, int a) { return (size_t)conn[e * npe + a]; };
+    auto elem_coords = [&](size_t e, double (*c)[3]) {
+        for (int a = 0; a < npe; ++a)
+            for (int k = 0; k < 3; ++k) c[a][k] = coords[3 * node(e, a) + k];
+    };
+    const TetGP* rule;
+    const int ng = rule_of(npe, &rule);
+    const TetGP* crule = npe == 4 ? TETRA_4 : TETRA_14.p;
+    const int cng = npe == 4 ? 4 : 14;
+
+    // assemble, model.rs:1070-1147 (thermal: one DOF per node)
+    std::vector<std::vector<Convection>> faces(ne);
+    for (int64_t k = 0; k < n_conv; ++k) {
+        const int64_t e = c_elem[k];
+        if (e < 0 || e >= n_elems) continue;
+        double c[10][3];
+        elem_coords((size_t)e, c);
+        Convection cv;
+        if (face_convection(npe, c, c_face[k], c_film[k], c_sink[k], cv)) faces[(size_t)e].push_back(cv);
+    }
+    Vec f(n, 0.0);
+    for (size_t g = 0; g < n; ++g) f[g] += loads ? loads[g] : 0.0;
+    GaussData gd[14];
+    for (int64_t k = 0; k < n_src; ++k) {
+        const size_t e = (size_t)s_elem[k];
+        double c[10][3];
+        elem_coords(e, c);
+        solid_gauss(npe, c, rule, ng, gd);
+        double fs[10] = {0};
+        for (int gp = 0; gp < ng; ++gp)
+            for (int a = 0; a < npe; ++a) fs[a] += gd[gp].w * gd[gp].n[a] * s_value[k];
+        for (int a = 0; a < npe; ++a) f[node(e, a)] += fs[a];
+    }
+    for (size_t e = 0; e < ne; ++e)
+        for (const Convection& cv : faces[e])
+            for (int a = 0; a < cv.nn; ++a) f[node(e, cv.pos[a])] += cv.load[a];
+
+    // left / right element matrices, model.rs:646-663
+    const int m = npe;
+    Vec left(ne * m * m), right(ne * m * m), kk(m * m), cc(m * m);
+    for (size_t e = 0; e < ne; ++e) {
+        double c[10][3];
+        elem_coords(e, c);
+        solid_gauss(npe, c, rule, ng, gd);
+        conduction(npe, gd, ng, conductivity[e], kk.data());
+        for (const Convection& cv : faces[e])
+            for (int a = 0; a < cv.nn; ++a)
+                for (int b = 0; b < cv.nn; ++b) kk[cv.pos[a] * m + cv.pos[b]] += cv.matrix[a * cv.nn + b];
+        solid_gauss(npe, c, crule, cng, gd);
+        capacity(npe, gd, cng, rho_c[e], cc.data());
+        for (int q = 0; q < m * m; ++q) {
+            left[e * m * m + q] = cc[q] / dt + theta * kk[q];
+            right[e * m * m + q] = cc[q] / dt + (theta - 1.0) * kk[q];
+        }
+    }
+    Vec t(initial, initial + n);
+    for (size_t g = 0; g < n; ++g)
+        if (fixed[g]) t[g] = imposed[g];
+
+    // FreeSystem::new, model.rs:1442-1499, on the left matrix
+    IVec free(n, NONE);
+    size_t count = 0;
+    for (size_t g = 0; g < n; ++g)
+        if (!fixed[g]) free[g] = count++;
+    IVec eoff(ne + 1, 0), eidx;
+    for (size_t e = 0; e < ne; ++e) {
+        for (int a = 0; a < m; ++a)
+            if (free[node(e, a)] != NONE) eidx.push_back(free[node(e, a)]);
+        eoff[e + 1] = eidx.size();
+    }
+    Graph graph = graph_from_elements(count, eoff, eidx);
+    IVec order = reverse_cuthill_mckee(graph);
+    IVec rank(count);
+    for (size_t r = 0; r < count; ++r) rank[order[r]] = r;
+    const bool iterative = solver == 2 || (solver == 0 && count >= ITERATIVE_FROM);
+    Csr csr;
+    std::optional<Skyline> sky;
+    if (iterative) {
+        csr = Csr::zeros(graph, order, rank);
+    } else {
+        IVec first(count);
+        for (size_t a = 0; a < count; ++a) first[a] = a;
+        for (size_t a = 0; a < count; ++a)
+            for (size_t p = graph.offsets[a]; p < graph.offsets[a + 1]; ++p)
+                first[rank[a]] = std::min(first[rank[a]], rank[graph.targets[p]]);
+        sky.emplace(first);
+    }
+    graph = Graph{};
+    Vec coupling(count, 0.0);
+    for (size_t e = 0; e < ne; ++e)
+        for (int r = 0; r < m; ++r) {
+            const size_t a = free[node(e, r)];
+            if (a == NONE) continue;
+            for (int c = 0; c < m; ++c) {
+                const size_t b = free[node(e, c)];
+                const double k = left[e * m * m + r * m + c];
+                if (b != NONE) {
+                    if (rank[b] <= rank[a]) {
+                        if (iterative) csr.add(rank[a], rank[b], k);
+                        else sky->add(rank[a], rank[b], k);
+                    }
+                } else {
+                    coupling[rank[a]] += k * t[node(e, c)];
+                }
+            }
+        }
+    const double t1 = now_ms();
+    Vec l;
+    SolveStats st;
+    if (iterative) {
+        bool ok = false;
+        for (double shift : SHIFTS) {
+            auto got = csr.incomplete_cholesky(shift);
+            if (got) {
+                l = std::move(*got);
+                st.shift = shift;
+                ok = true;
+                break;
+            }
+        }
+        if (!ok) return SINGULAR;
+    } else if (sky->factorize() != OK) {
+        return SINGULAR;
+    }
+    const double t2 = now_ms();
+
+    // product, model.rs:1353-1369: (sum_e M_e x_e) on the rows `rows` (nullptr = every row)
+    auto product = [&](const Vec& mats, const Vec& x, const uint8_t* rows, Vec& y) {
+        std::fill(y.begin(), y.end(), 0.0);
+        for (size_t e = 0; e < ne; ++e) {
+            bool any = rows == nullptr;
+            for (int a = 0; a < m && !any; ++a) any = rows[node(e, a)] != 0;
+            if (!any) continue;
+            for (int r = 0; r < m; ++r) {
+                const size_t g = node(e, r);
+                if (rows && !rows[g]) continue;
+                const double* row = &mats[e * m * m + r * m];
+                double s = row[0] * x[node(e, 0)];
+                for (int c = 1; c < m; ++c) s = s + row[c] * x[node(e, c)];
+                y[g] += s;
+            }
+        }
+    };
+    auto write_fluxes = [&](const Vec& temp, double* out) {
+        if (!out) return;
+        for (size_t e = 0; e < ne; ++e) {
+            double c[10][3], te[10];
+            elem_coords(e, c);
+            solid_gauss(npe, c, rule, ng, gd);
+            for (int a = 0; a < m; ++a) te[a] = temp[node(e, a)];
+            heat_fluxes(npe, gd, ng, conductivity[e], te, out + e * ng * 6);
+        }
+    };
+    if (temps) std::copy(t.begin(), t.end(), temps);
+    if (reactions) std::fill(reactions, reactions + n, 0.0);
+    write_fluxes(t, fluxes);
+    int64_t total = 0;
+    double worst = 0.0;
+    Vec carried(n), rhs(n), y(n), b(count), x;
+    for (int64_t s = 1; s <= increments; ++s) {
+        product(right, t, nullptr, carried);
+        for (size_t g = 0; g < n; ++g) rhs[g] = carried[g] + f[g];
+        // FreeSystem::solve, model.rs:1502-1516
+        for (size_t k = 0; k < count; ++k) b[k] = -coupling[k];
+        for (size_t g = 0; g < n; ++g)
+            if (free[g] != NONE) b[rank[free[g]]] += rhs[g];
+        if (iterative) {
+            SolveStats ss;
+            const int status = pcg_solve(csr, b, tol, (size_t)max_iter, x, ss, &l);
+            total += (int64_t)ss.iterations;
+            worst = std::max(worst, ss.rel_residual);
+            if (iterations) iterations[s - 1] = (int64_t)ss.iterations;
+            if (status != OK) {
+                if (info) info[0] = (double)total;
+                return status;
+            }
+        } else {
+            x = sky->solve(b);
+            if (iterations) iterations[s - 1] = 0;
+        }
+        for (size_t g = 0; g < n; ++g)
+            if (free[g] != NONE) t[g] = x[rank[free[g]]];
+        if (temps) std::copy(t.begin(), t.end(), temps + (size_t)s * n);
+        if (reactions) {
+            product(left, t, fixed, y);
+            for (size_t g = 0; g < n; ++g)
+                if (fixed[g]) y[g] -= rhs[g];
+            std::copy(y.begin(), y.end(), reactions + (size_t)s * n);
+        }
+        if (fluxes) write_fluxes(t, fluxes + (size_t)s * ne * ng * 6);
+    }
+    const double t3 = now_ms();
+    if (f_out) std::copy(f.begin(), f.end(), f_out);
+    if (info) {
+        info[0] = (double)total;
+        info[1] = worst;
+        info[2] = st.shift;
+        info[3] = (double)count;
+        info[4] = iterative ? (double)csr.cols.size() : (double)sky->data.size();
+        info[5] = t1 - t0;
+        info[6] = t2 - t1;
+        info[7] = t3 - t2;
+    }
+    return OK;
+}
+
+// TETRA_14 points (xi, eta, zeta, w) x 14, for the quadrature known-answer test
+void oracle_tetra14(double* out) {
+    for (int k = 0; k < 14; ++k) {
+        out[4 * k] = TETRA_14.p[k].xi;
+        out[4 * k + 1] = TETRA_14.p[k].eta;
+        out[4 * k + 2] = TETRA_14.p[k].zeta;
+        out[4 * k + 3] = TETRA_14.p[k].w;
+    }
+}
+
+// Element conduction K_e and capacity C_e (npe x npe each) of one element (coords npe x 3)
+void oracle_thermal_element(int npe, const double* coords, double k, double rho_c, double* ke, double* ce) {
+    const double (*c)[3] = reinterpret_cast<const double (*)[3]>(coords);
+    GaussData gd[14];
+    const TetGP* rule;
+    const int ng = rule_of(npe, &rule);
+    solid_gauss(npe, c, rule, ng, gd);
+    conduction(npe, gd, ng, k, ke);
+    solid_gauss(npe, c, npe == 4 ? TETRA_4 : TETRA_14.p, npe == 4 ? 4 : 14, gd);
+    capacity(npe, gd, npe == 4 ? 4 : 14, rho_c, ce);
 }
 
 }  // extern "C"
