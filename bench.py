@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost section")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched section")
     ap.add_argument("--no-large-strain", action="store_true", help="skip the large-strain section")
+    ap.add_argument("--no-thermal", action="store_true", help="skip the transient thermal section")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--adjoint-cells", type=int, default=48)
     ap.add_argument("--only", choices=["mixed", "plain"], default=None,
@@ -342,6 +343,54 @@ def large_strain_section(mb, mg, steps, device):
     return out
 
 
+def thermal_section(mg, steps, device, hbm):
+    """Transient heat conduction on the Tet10 unit cube 40^3 (531 441 nodes, 524 880 free): 10
+    backward-Euler increments of (C/dt + K) T_{n+1} = C/dt T_n + F, each solved by IC(0)-PCG from
+    zero to 1e-12 (Model::solve_step). One step = the whole transient through the C ABI from host
+    buffers (element matrices, assembly, IC(0), the increments, the history copied back); the
+    device time of the increments comes from the library's CUDA events. Roofline of the
+    persistent scalar PCG: algorithmic bytes per iteration = the left matrix (values + columns)
+    once for the SpMV and its strict triangles once per sweep, plus about 16 vector passes."""
+    from maille_b200 import thermal as th
+    p = mg.thermal_cube(40, True, increments=10, time_period=0.1)
+    f = p.loads + th.thermal_loads(p.coords, p.conn, list(zip(p.s_elem, p.s_value)),
+                                   list(zip(p.c_elem, p.c_face, p.c_film, p.c_sink)))
+    s, out = th.solve_problem(p, f=f, fluxes=False, device=device)  # warm-up
+    if s != 0:
+        return {"workload": p.name, "error": s}
+    walls, dev = [], []
+    for _ in range(max(1, steps)):
+        t0 = time.perf_counter()
+        s, out = th.solve_problem(p, f=f, fluxes=False, device=device)
+        walls.append((time.perf_counter() - t0) * 1e3)
+        dev.append(out["info"]["ms_steps"])
+    info = out["info"]
+    nnz, nb, its = info["nonzeros"], info["free_nodes"], info["iterations_total"]
+    bytes_it = 12 * nnz + 12 * (nnz - nb) + 16 * 8 * nb
+    ms_it = statistics.median(dev) / its
+    wall = statistics.median(walls)
+    res = {"workload": p.name + "_10inc", "free_nodes": nb, "nonzeros": nnz, "levels": info["levels"],
+           "increments": p.increments, "iterations_total": its, "iterations": out["iterations"].tolist(),
+           "e2e_ms": wall, "e2e_value": nb * p.increments / (wall / 1e3), "unit": "DOF*increments/s",
+           "ms_increments_device": statistics.median(dev), "ms_setup": info["ms_setup"],
+           "ms_upload": info["ms_upload"], "ms_assembly": info["ms_assembly"], "ms_factor": info["ms_factor"],
+           "ms_download": info["ms_download"],
+           "roofline": {"bound": "hbm", "kernel": "k_heat_pcg (persistent FP64 scalar IC(0)-PCG)",
+                        "bytes_per_iteration": bytes_it, "ms_per_iteration": ms_it,
+                        "achieved": bytes_it / (ms_it * 1e6), "peak": hbm,
+                        "frac": bytes_it / (ms_it * 1e6) / hbm}}
+    path = os.path.join(ROOT, "tests", "golden", "thermal_40_oracle_summary.json")
+    if os.path.exists(path):
+        g = json.load(open(path))
+        sample = out["temps"][-1][::g["t_final_stride"]]
+        res["max_abs_err_vs_oracle_final_T"] = float(np.max(np.abs(sample - np.array(g["t_final_sample"]))))
+        res["oracle_iterations_total"] = g["total_iterations"]
+        res["oracle_cpu_s"] = g["wall_s"]
+        res["speedup_e2e_vs_oracle"] = g["wall_s"] * 1e3 / wall
+        res["oracle_cpu_note"] = "oracle wall time from the golden summary (1 core, build container)"
+    return res
+
+
 def spmv_roofline(torch, h, L, precision, blocks, nb, reps=50):
     """Average duration of the PCG SpMV kernel over `reps` launches (CUDA events on the
     library's stream) and its algorithmic bytes: per block 9 values + one int32 column index,
@@ -562,6 +611,10 @@ def run_ours(args):
     if not args.no_large_strain:
         large_strain = large_strain_section(mb, mg, args.steps, local)
 
+    thermal = None
+    if not args.no_thermal:
+        thermal = thermal_section(mg, args.steps, local, hbm)
+
     adjoint = None
     if not args.no_adjoint:
         adjoint = adjoint_section(torch, mb, mg, L, args.adjoint_cells, args.tol, args.steps,
@@ -607,6 +660,7 @@ def run_ours(args):
         "batched": batched,
         "large_strain": large_strain,
         "adjoint": adjoint,
+        "thermal": thermal,
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
     }
     print(json.dumps(line))

@@ -341,6 +341,87 @@ int32_t maille_gpu_large_strain_set_materials(MailleGpuLargeStrain* s, const dou
                                               const double* poisson);
 void maille_gpu_large_strain_destroy(MailleGpuLargeStrain* s);
 
+/* ---- Transient heat conduction: the theta-method ---------------------------------------------
+ * Replaces, for a Tet4/Tet10 model with Analysis::Thermal, Model::solve_step / solve_step_with
+ * (model.rs:621-706) on the iterative FreeSystem: element conduction K_e (conduction,
+ * element.rs:451-463, rule TETRA_1 / TETRA_4) plus the convection terms h int N N^T dS of the
+ * model's Convection faces (FaceConvection::add_matrix, assembly.rs:495-503), consistent capacity
+ * C_e (capacity, element.rs:465-477, rule TETRA_4 / TETRA_14, element_capacity,
+ * assembly.rs:413-433), then per increment
+ *   (C/dt + theta K) T_{n+1} = (C/dt - (1 - theta) K) T_n + F
+ * with the left matrix assembled and IC(0)-factorised once (FreeSystem::new, model.rs:1442-1499;
+ * Pcg::new) and each increment solved by IC(0)-PCG from a zero start to ||r|| <= rel_tol ||b||
+ * (Pcg::solve, iterative.rs:210-248); reactions R = C (T_{n+1} - T_n)/dt + K (theta T_{n+1} +
+ * (1 - theta) T_n) - F on imposed nodes and the heat fluxes q = -k grad T (heat_fluxes,
+ * element.rs:480-506) of every increment. Imposed temperatures replace the initial field at
+ * their nodes from t = 0. The whole step runs on the device: one host synchronisation at the
+ * end, the history kept in device memory until then. */
+typedef struct {
+    int64_t n_nodes;
+    const double* coords;         /* [3 n_nodes] */
+    int32_t nodes_per_elem;       /* 4 or 10 */
+    int64_t n_elems;
+    const int64_t* conn;          /* [n_elems * nodes_per_elem], Maille node order */
+    const double* conductivity;   /* [n_elems] k of each element's Material */
+    const double* rho_c;          /* [n_elems] density x specific heat */
+    const uint8_t* fixed;         /* [n_nodes] 1 where a Bc imposes T (Dof::T) */
+    const double* imposed;        /* [n_nodes] imposed T at fixed nodes (ignored elsewhere) */
+    const double* f;              /* [n_nodes] assembled heat loads F: nodal loads, heat sources
+                                     and the convection loads h T_inf int N dS (assemble,
+                                     model.rs:1070-1147; maille_gpu_thermal_loads adds the last
+                                     two), or NULL for zero */
+    int64_t n_convection;         /* convection faces whose h int N N^T dS joins K */
+    const int64_t* conv_elem;     /* [n_convection] element */
+    const int32_t* conv_face;     /* [n_convection] face 0..3 (0-1-2, 0-3-1, 1-3-2, 2-3-0); an
+                                     out-of-range face adds nothing, like face_rule's None */
+    const double* conv_film;      /* [n_convection] h */
+    const double* initial;        /* [n_nodes] T at t = 0 */
+    double time_step;             /* dt > 0 (Step::time_step, model.rs:171-173) */
+    double theta;                 /* 0.5 <= theta <= 1 (Step::with_theta, model.rs:151-156) */
+    int32_t increments;           /* > 0 */
+    double rel_tol;               /* <= 0 selects 1e-12 */
+    int32_t max_iter;             /* per increment; <= 0 selects 10000 */
+    int32_t ordering;             /* MailleOrdering of the free nodes */
+    int32_t device;
+} MailleThermalProblem;
+
+typedef struct {
+    double* temperatures;   /* [(increments + 1) n_nodes] T of every increment, t = 0 first, or NULL */
+    double* reactions;      /* [(increments + 1) n_nodes] R at imposed nodes, 0 elsewhere and at
+                               t = 0, or NULL */
+    double* heat_fluxes;    /* [(increments + 1) n_elems ngp 6] per Gauss point x, y, z, qx, qy,
+                               qz (HeatFlux, results.rs); ngp = 1 (Tet4) or 4 (Tet10); or NULL */
+    int32_t* iterations;    /* [increments] PCG iterations of each increment, or NULL */
+    /* filled by the library */
+    int64_t iterations_total;
+    double max_rel_residual;  /* largest final ||r|| / ||b|| over the increments */
+    double shift;             /* diagonal shift IC(0) succeeded with */
+    int64_t free_nodes;
+    int64_t nonzeros;         /* entries of the full symmetric pattern of the free nodes */
+    int32_t levels;           /* levels of the IC(0) sweeps */
+    double ms_setup;          /* host ordering */
+    double ms_upload;         /* host -> device copies and device analysis */
+    double ms_assembly;       /* element matrices + assembly of the left and right matrices */
+    double ms_factor;         /* IC(0) incl. shift retries */
+    double ms_steps;          /* every increment: right-hand side, PCG, reactions, fluxes */
+    double ms_download;       /* device -> host copies of the history */
+} MailleThermalResult;
+
+/* The whole transient step (Model::solve_step). MAILLE_SINGULAR / MAILLE_NOT_CONVERGED name the
+ * first increment whose solve failed; the history before it is returned. */
+int32_t maille_gpu_thermal_transient(const MailleThermalProblem* problem, MailleThermalResult* result);
+
+/* Host helper: adds to f ([n_nodes]) the heat-source loads int N q dV of uniform sources
+ * (element, q) (element_heat_source / nodal_source, assembly.rs:466-484, element rule TETRA_1 /
+ * TETRA_4) and the convection loads h T_inf int N dS of faces (element, face, h, T_inf)
+ * (face_convection, assembly.rs:595-626; FaceConvection::add_load), in the order of the
+ * reference's assemble (model.rs:1101-1140). Elements or faces out of range add nothing. */
+int32_t maille_gpu_thermal_loads(int64_t n_nodes, const double* coords, int32_t npe, int64_t n_elems,
+                                 const int64_t* conn, int64_t n_sources, const int64_t* s_elem,
+                                 const double* s_value, int64_t n_convection, const int64_t* c_elem,
+                                 const int32_t* c_face, const double* c_film, const double* c_sink,
+                                 double* f);
+
 /* Largest n_block_rows that maille_gpu_bsr3_spmv_dot_noalloc accepts (2^26 block rows, i.e.
  * about 2e8 DOFs, inside the 32-bit column indices of the matrix). */
 #define MAILLE_NOALLOC_MAX_BLOCK_ROWS (INT64_C(1) << 26)

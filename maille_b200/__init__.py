@@ -10,3 +10,4 @@ from ._lib import MAILLE_FP64, MAILLE_MIXED, MAILLE_ORDER_AUTO, MAILLE_ORDER_MUL
 __version__ = "0.1.0"
 from .batch import BatchField, BatchSolver, partition_lpt, solve_sharded  # noqa: F401,E402
 from .large_strain import LargeStrainHistory, LargeStrainSolver  # noqa: F401,E402
+from .thermal import Convection, HeatSource, Increment, Step, ThermalModel, thermal_loads  # noqa: F401,E402

@@ -92,6 +92,29 @@ class LargeStrainResult(ctypes.Structure):
     ]
 
 
+class ThermalProblem(ctypes.Structure):
+    _fields_ = [
+        ("n_nodes", ctypes.c_int64), ("coords", _d), ("nodes_per_elem", ctypes.c_int32),
+        ("n_elems", ctypes.c_int64), ("conn", _i64), ("conductivity", _d), ("rho_c", _d),
+        ("fixed", _u8), ("imposed", _d), ("f", _d), ("n_convection", ctypes.c_int64),
+        ("conv_elem", _i64), ("conv_face", _i32), ("conv_film", _d), ("initial", _d),
+        ("time_step", ctypes.c_double), ("theta", ctypes.c_double), ("increments", ctypes.c_int32),
+        ("rel_tol", ctypes.c_double), ("max_iter", ctypes.c_int32), ("ordering", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+class ThermalResult(ctypes.Structure):
+    _fields_ = [
+        ("temperatures", _d), ("reactions", _d), ("heat_fluxes", _d), ("iterations", _i32),
+        ("iterations_total", ctypes.c_int64), ("max_rel_residual", ctypes.c_double),
+        ("shift", ctypes.c_double), ("free_nodes", ctypes.c_int64), ("nonzeros", ctypes.c_int64),
+        ("levels", ctypes.c_int32), ("ms_setup", ctypes.c_double), ("ms_upload", ctypes.c_double),
+        ("ms_assembly", ctypes.c_double), ("ms_factor", ctypes.c_double), ("ms_steps", ctypes.c_double),
+        ("ms_download", ctypes.c_double),
+    ]
+
+
 # every symbol include/maille_gpu.h declares, with its ctypes signature
 SIGNATURES = {
     "maille_gpu_last_error": ([], ctypes.c_char_p),
@@ -134,6 +157,10 @@ SIGNATURES = {
     "maille_gpu_large_strain_backward": ([ctypes.c_void_p, _d, _d, _d], ctypes.c_int32),
     "maille_gpu_large_strain_set_materials": ([ctypes.c_void_p, _d, _d], ctypes.c_int32),
     "maille_gpu_large_strain_destroy": ([ctypes.c_void_p], None),
+    "maille_gpu_thermal_transient": ([ctypes.POINTER(ThermalProblem), ctypes.POINTER(ThermalResult)],
+                                     ctypes.c_int32),
+    "maille_gpu_thermal_loads": ([ctypes.c_int64, _d, ctypes.c_int32, ctypes.c_int64, _i64, ctypes.c_int64,
+                                  _i64, _d, ctypes.c_int64, _i64, _i32, _d, _d, _d], ctypes.c_int32),
 }
 
 _lib = None

@@ -49,7 +49,8 @@ def test_version_and_device_count_need_no_gpu(lib):
 STRUCTS = (("MailleElasticProblem", _lib.ElasticProblem), ("MailleElasticResult", _lib.ElasticResult),
            ("MailleBatchProblem", _lib.BatchProblem), ("MailleBatchResult", _lib.BatchResult),
            ("MailleLargeStrainProblem", _lib.LargeStrainProblem),
-           ("MailleLargeStrainResult", _lib.LargeStrainResult))
+           ("MailleLargeStrainResult", _lib.LargeStrainResult),
+           ("MailleThermalProblem", _lib.ThermalProblem), ("MailleThermalResult", _lib.ThermalResult))
 
 
 def test_struct_layouts_match_the_header(tmp_path):
@@ -203,3 +204,76 @@ def test_workload_generators_are_seeded_and_shaped():
     assert p.free_dofs == 26460 and p.p_elem.size == 800
     p, rho = mg.simp_tet4(4)
     assert np.allclose(p.young, 210000 * rho ** 3) and rho.min() >= 0.01 and rho.max() <= 1.0
+
+
+# --- transient thermal: host helper and input checks ---------------------------------------------
+
+@pytest.mark.parametrize("quadratic", [False, True])
+def test_thermal_load_helper_matches_the_oracle(lib, oracle_lib, quadratic):
+    from maille_b200 import thermal as th
+    p = mg.thermal_cube(3, quadratic, increments=1)
+    f = th.thermal_loads(p.coords, p.conn, list(zip(p.s_elem, p.s_value)),
+                         list(zip(p.c_elem, p.c_face, p.c_film, p.c_sink)))
+    ref = oracle_lib.thermal_transient(p, solver=1, fluxes=False)
+    assert ref["status"] == 0
+    assert np.abs(f - ref["f"]).max() <= 1e-13 * np.abs(ref["f"]).max()
+    # totals: source q V over the unit cube plus h T_inf over the unit top face
+    assert abs(f.sum() - (50.0 + 10.0 * 20.0)) < 1e-10
+
+
+def test_thermal_inputs_are_rejected_before_any_device_work(lib):
+    from maille_b200 import thermal as th
+    p0 = mg.thermal_cube(2, False, increments=2)
+    good = dict(coords=p0.coords, conn=p0.conn, conductivity=p0.conductivity, rho_c=p0.rho_c,
+                fixed=p0.fixed, imposed=p0.imposed, f=None, initial=p0.initial, time_step=0.1,
+                theta=1.0, increments=2)
+
+    def status(**kw):
+        args = dict(good)
+        args.update(kw)
+        p, keep = th.thermal_problem_struct(**args)
+        r = _lib.ThermalResult()
+        return lib.maille_gpu_thermal_transient(ctypes.byref(p), ctypes.byref(r))
+
+    assert status(theta=0.4) == _lib.MAILLE_INVALID_INPUT and "theta" in _lib.last_error()
+    assert status(theta=float("nan")) == _lib.MAILLE_INVALID_INPUT
+    assert status(increments=0) == _lib.MAILLE_INVALID_INPUT
+    assert status(time_step=0.0) == _lib.MAILLE_INVALID_INPUT
+    bad = p0.initial.copy()
+    bad[2] = np.nan
+    assert status(initial=bad) == _lib.MAILLE_INVALID_INPUT and "node 2" in _lib.last_error()
+    conn = p0.conn.copy()
+    conn[1, 1] = p0.coords.shape[0]
+    assert status(conn=conn) == _lib.MAILLE_INVALID_INPUT and "unknown node" in _lib.last_error()
+    assert status(fixed=np.ones_like(p0.fixed)) == _lib.MAILLE_INVALID_INPUT
+    assert lib.maille_gpu_thermal_transient(None, None) == _lib.MAILLE_INVALID_INPUT
+    if lib.maille_gpu_device_count() == 0:
+        assert status() == _lib.MAILLE_CUDA_ERROR  # a valid problem needs a device: no fallback
+
+
+def test_thermal_step_validation_mirrors_the_reference():
+    # tests/transient.rs:476-500
+    from maille_b200.thermal import Step
+    with pytest.raises(mb.MailleError) as e:
+        Step.transient(0.0, 10)
+    assert e.value.kind == "InvalidProperty"
+    with pytest.raises(mb.MailleError) as e:
+        Step.transient(1.0, 0)
+    assert e.value.kind == "NoIncrements"
+    step = Step.transient(1.0, 10)
+    with pytest.raises(mb.MailleError) as e:
+        step.with_theta(0.4)
+    assert e.value.kind == "ThetaOutOfRange"
+    with pytest.raises(mb.MailleError):
+        step.with_theta(float("nan"))
+    assert abs(step.with_theta(0.5).time_step - 0.1) < 1e-15
+    nodes, tets = mg.box_grid((1, 1, 1), (1.0, 1.0, 1.0))
+    model = mb.ThermalModel(nodes, tets, 1.0, 1.0)
+    with pytest.raises(mb.MailleError) as e:
+        model.solve_step(step, [0.0])
+    assert e.value.kind == "TemperatureCount"
+    t = np.zeros(nodes.shape[0])
+    t[2] = np.nan
+    with pytest.raises(mb.MailleError) as e:
+        model.solve_step(step, t)
+    assert e.value.kind == "NonFiniteTemperature"

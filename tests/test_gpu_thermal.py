@@ -1,0 +1,144 @@
+"""GPU parity of the transient heat conduction path (maille_gpu_thermal_transient) against the
+oracle's restatement of Model::solve_step (model.rs:621-706), and the reference's transient
+known-answer tests (tests/transient.rs) run through the GPU path.
+
+Tolerances: the GPU and the oracle both run IC(0)-PCG to ||r|| <= 1e-12 ||b|| per increment but
+with different orderings (multicolour vs RCM), so their temperatures agree to the solver
+tolerance times the conditioning: 1e-9 relative to the largest temperature; reactions (sums of
+element products of those temperatures) to 1e-8 of the largest reaction; Gauss-point fluxes to
+1e-8 of the largest flux.
+"""
+import numpy as np
+import pytest
+
+from maille_b200 import meshgen as mg, thermal as th, _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _check(out, ref, t_tol=1e-9, r_tol=1e-8, q_tol=1e-8):
+    assert _rel(out["temps"], ref["temps"]) < t_tol, _rel(out["temps"], ref["temps"])
+    assert _rel(out["reactions"], ref["reactions"]) < r_tol, _rel(out["reactions"], ref["reactions"])
+    if ref["fluxes"] is not None and out["fluxes"] is not None:
+        assert _rel(out["fluxes"], ref["fluxes"]) < q_tol, _rel(out["fluxes"], ref["fluxes"])
+
+
+@pytest.mark.parametrize("quadratic,cells", [(False, 8), (True, 4)])
+def test_transient_matches_the_oracle(gpu, oracle_lib, quadratic, cells):
+    p = mg.thermal_cube(cells, quadratic, increments=4, time_period=0.04)
+    ref = oracle_lib.thermal_transient(p, solver=2)
+    assert ref["status"] == 0
+    s, out = th.solve_problem(p, f=ref["f"])
+    assert s == 0, _lib.last_error()
+    _check(out, ref)
+    info = out["info"]
+    assert info["free_nodes"] == ref["free"]
+    assert info["iterations_total"] > 0 and info["max_rel_residual"] <= 1e-12
+    assert np.all(out["iterations"] > 0)
+
+
+def test_crank_nicolson_with_rcm_ordering_and_no_fluxes(gpu, oracle_lib):
+    p = mg.thermal_cube(6, False, increments=3, time_period=0.03, theta=0.5)
+    ref = oracle_lib.thermal_transient(p, solver=2, fluxes=False)
+    s, out = th.solve_problem(p, f=ref["f"], fluxes=False, ordering=_lib.MAILLE_ORDER_RCM)
+    assert s == 0, _lib.last_error()
+    _check(out, ref)
+    assert out["info"]["levels"] > 20  # RCM: level-scheduled, many levels
+
+
+def test_host_loads_and_device_path_agree_with_the_oracle_end_to_end(gpu, oracle_lib):
+    # f assembled by the library's host helper (sources + convection), not taken from the oracle
+    p = mg.thermal_cube(4, True, increments=2, time_period=0.05)
+    ref = oracle_lib.thermal_transient(p, solver=2)
+    s, out = th.solve_problem(p)
+    assert s == 0, _lib.last_error()
+    _check(out, ref)
+
+
+def test_repeated_runs_are_bit_identical(gpu):
+    p = mg.thermal_cube(5, True, increments=3, time_period=0.03)
+    s1, a = th.solve_problem(p)
+    s2, b = th.solve_problem(p)
+    assert s1 == 0 and s2 == 0
+    assert np.array_equal(a["temps"], b["temps"])
+    assert np.array_equal(a["reactions"], b["reactions"])
+    assert np.array_equal(a["fluxes"], b["fluxes"])
+
+
+def _slab(name, nx, k=1.0):
+    nodes, tets = mg.box_grid((nx, 1, 1), (1.0, 0.25, 0.25))
+    conn = tets
+    if name == "Tet10":
+        nodes, conn = mg.to_quadratic_tet(nodes, tets)
+    return nodes, conn, k
+
+
+def test_quenched_slab_follows_the_fourier_series_on_the_gpu(gpu):
+    # transient.rs:281-295 through the GPU path (solver tolerance 1e-12 as the reference's PCG)
+    from maille_b200.thermal import Step, ThermalModel
+    for name, nx in (("Tet4", 40), ("Tet10", 10)):
+        nodes, conn, k = _slab(name, nx)
+        ends = np.nonzero((np.abs(nodes[:, 0]) < 1e-12) | (np.abs(nodes[:, 0] - 1.0) < 1e-12))[0]
+        model = ThermalModel(nodes, conn, k, 1.0, bcs=[(int(v), 100.0) for v in ends])
+        hist = model.solve_step(Step.transient(0.1, 400), np.zeros(nodes.shape[0]), fluxes=False)
+        n = 2 * np.arange(500) + 1.0
+        for s in (80, 200, 400):
+            t = hist[s].time
+            exact = 100.0 * (1.0 - (4.0 / (n * np.pi) * np.sin(np.outer(nodes[:, 0], n) * np.pi)
+                                    * np.exp(-(n * np.pi) ** 2 * t)).sum(axis=1))
+            assert np.max(np.abs(hist[s].temperatures - exact)) / 100.0 < 4e-3
+
+
+def test_energy_balance_is_exact_on_the_gpu(gpu):
+    # transient.rs:445-474 (sum over increments of dt (reactions + sources) = heat stored)
+    from maille_b200.thermal import HeatSource, Step, ThermalModel
+    for name in ("Tet4", "Tet10"):
+        nodes, conn, k = _slab(name, 4)
+        left = np.nonzero(np.abs(nodes[:, 0]) < 1e-12)[0]
+        model = ThermalModel(nodes, conn, k, 1.0, bcs=[(int(v), 80.0) for v in left])
+        model.with_heat_sources([HeatSource(e, 50.0) for e in range(conn.shape[0])])
+        step = Step.transient(0.3, 12).with_theta(0.5)
+        hist = model.solve_step(step, 20.0 + 5.0 * nodes[:, 0])
+        w = np.zeros(nodes.shape[0])  # rho c int N dV
+        for e in conn:
+            p0 = nodes[e[0]]
+            vol = abs(np.dot(nodes[e[1]] - p0, np.cross(nodes[e[2]] - p0, nodes[e[3]] - p0))) / 6.0
+            if conn.shape[1] == 4:
+                w[e] += vol * 0.25
+            else:
+                w[e[:4]] += vol * -0.05
+                w[e[4:]] += vol * 0.2
+        stored = float(np.dot(hist[12].temperatures - hist[0].temperatures, w))
+        supplied = sum(step.time_step * (h.reactions.sum() + 50.0 * 0.0625) for h in hist[1:])
+        assert abs(stored - supplied) < 1e-9 * abs(stored), (stored, supplied)
+
+
+def test_iteration_cap_reports_not_converged(gpu):
+    p = mg.thermal_cube(4, True, increments=3, time_period=0.3)
+    s, out = th.solve_problem(p, max_iter=2)
+    assert s == _lib.MAILLE_NOT_CONVERGED
+    assert "increment 1" in _lib.last_error()
+
+
+def test_full_size_transient_matches_the_oracle_summary(gpu):
+    # the 40^3 Tet10 workload (7.7 M lower slots, more than one thread each in any capped grid):
+    # iterations per increment, reaction sums and sampled final temperatures against the
+    # oracle's run (tests/golden/make_thermal_40_summary.py)
+    import json
+    import os
+    g = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                    "thermal_40_oracle_summary.json")))
+    p = mg.thermal_cube(40, True, increments=g["increments"], time_period=g["time_period"])
+    s, out = th.solve_problem(p, fluxes=False)
+    assert s == 0, _lib.last_error()
+    assert out["info"]["free_nodes"] == g["free_nodes"]
+    sample = out["temps"][-1][::g["t_final_stride"]]
+    assert np.max(np.abs(sample - np.array(g["t_final_sample"]))) < 1e-9 * 100.0
+    sums = out["reactions"].sum(axis=1)
+    assert np.max(np.abs(sums - np.array(g["reaction_sum"]))) < 1e-7 * np.max(np.abs(g["reaction_sum"]))
+    assert np.allclose(out["temps"].min(axis=1), g["t_min"], rtol=0, atol=1e-9 * 100.0)
+    assert np.allclose(out["temps"].max(axis=1), g["t_max"], rtol=0, atol=1e-9 * 100.0)
