@@ -737,11 +737,26 @@ __global__ void __launch_bounds__(kT, 2) k_heat_pcg(HeatPcg a) {
             }
             const double alpha = rz / pap;
             loc = 0.0;
-            for (int64_t i = tid; i < a.nb; i += nth) {
-                a.x[i] = __ldcg(a.x + i) + alpha * __ldcg(a.p + i);
-                const double ri = __ldcg(a.r + i) - alpha * __ldcg(a.ap + i);
-                a.r[i] = ri;
-                loc += ri * ri;
+            // two entries per thread and pass (16-byte accesses; the vectors hold nb + 1 >= 2 entries
+            // and start 256-byte aligned); an odd last entry is taken alone
+            for (int64_t i2 = tid; 2 * i2 < a.nb; i2 += nth) {
+                const int64_t i = 2 * i2;
+                if (i + 1 < a.nb) {
+                    const double2 xv = __ldcg(reinterpret_cast<const double2*>(a.x + i));
+                    const double2 pv = __ldcg(reinterpret_cast<const double2*>(a.p + i));
+                    const double2 rv = __ldcg(reinterpret_cast<const double2*>(a.r + i));
+                    const double2 av = __ldcg(reinterpret_cast<const double2*>(a.ap + i));
+                    const double r0 = rv.x - alpha * av.x, r1 = rv.y - alpha * av.y;
+                    *reinterpret_cast<double2*>(a.x + i) = make_double2(xv.x + alpha * pv.x, xv.y + alpha * pv.y);
+                    *reinterpret_cast<double2*>(a.r + i) = make_double2(r0, r1);
+                    loc += r0 * r0;
+                    loc += r1 * r1;
+                } else {
+                    a.x[i] = __ldcg(a.x + i) + alpha * __ldcg(a.p + i);
+                    const double ri = __ldcg(a.r + i) - alpha * __ldcg(a.ap + i);
+                    a.r[i] = ri;
+                    loc += ri * ri;
+                }
             }
             heat_publish(loc, a.partials, 1, sh);
             grid.sync();
@@ -764,7 +779,16 @@ __global__ void __launch_bounds__(kT, 2) k_heat_pcg(HeatPcg a) {
             const double rz_next = heat_total(a.partials, 2);
             const double beta = rz_next / rz;
             rz = rz_next;
-            for (int64_t i = tid; i < a.nb; i += nth) a.p[i] = __ldcg(&a.zrec[i].x) + beta * __ldcg(a.p + i);
+            for (int64_t i2 = tid; 2 * i2 < a.nb; i2 += nth) {
+                const int64_t i = 2 * i2;
+                if (i + 1 < a.nb) {
+                    const double z0 = __ldcg(&a.zrec[i].x), z1 = __ldcg(&a.zrec[i + 1].x);
+                    const double2 pv = __ldcg(reinterpret_cast<const double2*>(a.p + i));
+                    *reinterpret_cast<double2*>(a.p + i) = make_double2(z0 + beta * pv.x, z1 + beta * pv.y);
+                } else {
+                    a.p[i] = __ldcg(&a.zrec[i].x) + beta * __ldcg(a.p + i);
+                }
+            }
             grid.sync();
             mark(3);
         }
