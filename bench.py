@@ -53,9 +53,10 @@ def parse():
     ap.add_argument("--no-thermal", action="store_true", help="skip the transient thermal section")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--adjoint-cells", type=int, default=48)
-    ap.add_argument("--only", choices=["mixed", "plain"], default=None,
+    ap.add_argument("--only", choices=["mixed", "plain", "thermal"], default=None,
                     help="profiling mode: time one form only (no reference solve, e2e or CPU); "
                          "prints a short line, not the benchmark line")
+    ap.add_argument("--thermal-cells", type=int, default=40, help="cube side of the thermal section")
     return ap.parse_args()
 
 
@@ -343,7 +344,7 @@ def large_strain_section(mb, mg, steps, device):
     return out
 
 
-def thermal_section(mg, steps, device, hbm):
+def thermal_section(mg, steps, device, hbm, cells=40):
     """Transient heat conduction on the Tet10 unit cube 40^3 (531 441 nodes, 524 880 free): 10
     backward-Euler increments of (C/dt + K) T_{n+1} = C/dt T_n + F, each solved by IC(0)-PCG from
     zero to 1e-12 (Model::solve_step). One step = the whole transient through the C ABI from host
@@ -352,7 +353,7 @@ def thermal_section(mg, steps, device, hbm):
     persistent scalar PCG: algorithmic bytes per iteration = the left matrix (values + columns)
     once for the SpMV and its strict triangles once per sweep, plus about 16 vector passes."""
     from maille_b200 import thermal as th
-    p = mg.thermal_cube(40, True, increments=10, time_period=0.1)
+    p = mg.thermal_cube(cells, True, increments=10, time_period=0.1)
     f = p.loads + th.thermal_loads(p.coords, p.conn, list(zip(p.s_elem, p.s_value)),
                                    list(zip(p.c_elem, p.c_face, p.c_film, p.c_sink)))
     s, out = th.solve_problem(p, f=f, fluxes=False, device=device)  # warm-up
@@ -380,7 +381,7 @@ def thermal_section(mg, steps, device, hbm):
                         "achieved": bytes_it / (ms_it * 1e6), "peak": hbm,
                         "frac": bytes_it / (ms_it * 1e6) / hbm}}
     path = os.path.join(ROOT, "tests", "golden", "thermal_40_oracle_summary.json")
-    if os.path.exists(path):
+    if cells == 40 and os.path.exists(path):
         g = json.load(open(path))
         sample = out["temps"][-1][::g["t_final_stride"]]
         res["max_abs_err_vs_oracle_final_T"] = float(np.max(np.abs(sample - np.array(g["t_final_sample"]))))
@@ -484,7 +485,21 @@ def run_reference(args):
 
 
 def run_only(args):
-    """One form, W + K steps of refactor + solve, nothing else (for profiler launch lists)."""
+    """One form, W + K steps of refactor + solve, nothing else (for profiler launch lists); with
+    --only thermal, the thermal section's transient (W + K runs of the whole step)."""
+    if args.only == "thermal":
+        from maille_b200 import meshgen as mg, thermal as th
+        p = mg.thermal_cube(args.thermal_cells, True, increments=10, time_period=0.1)
+        f = p.loads + th.thermal_loads(p.coords, p.conn, list(zip(p.s_elem, p.s_value)),
+                                       list(zip(p.c_elem, p.c_face, p.c_film, p.c_sink)))
+        for _ in range(args.warmup + args.steps):
+            s, out = th.solve_problem(p, f=f, fluxes=False)
+            if s != 0:
+                raise SystemExit(f"thermal transient failed with status {s}")
+        print(json.dumps({"only": "thermal", "workload": p.name + "_10inc",
+                          "iterations": out["info"]["iterations_total"],
+                          "ms_increments_device": out["info"]["ms_steps"]}))
+        return
     import torch
     import maille_b200 as mb
     from maille_b200 import meshgen as mg
@@ -613,7 +628,7 @@ def run_ours(args):
 
     thermal = None
     if not args.no_thermal:
-        thermal = thermal_section(mg, args.steps, local, hbm)
+        thermal = thermal_section(mg, args.steps, local, hbm, args.thermal_cells)
 
     adjoint = None
     if not args.no_adjoint:

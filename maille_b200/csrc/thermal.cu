@@ -1216,7 +1216,10 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
                                                                 flux + (size_t)s * ne * ng * 6);
         };
         // the persistent kernel: every block co-resident
+        // two blocks of 256 threads per SM (128 registers a thread): 3 or 4 blocks (80 or 64
+        // registers) spill and make every grid barrier dearer, measured slower in every phase
         int per_sm = 0, sms = 0, dev = p->device;
+        void* pcg_fn = (void*)k_heat_pcg;
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_heat_pcg, kT, 0));
         const int grid = sms * std::min(per_sm, 2);
@@ -1241,7 +1244,7 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
                       timing};
             void* args[] = {&a};
             counted();
-            CK(cudaLaunchCooperativeKernel((void*)k_heat_pcg, dim3(grid), dim3(kT), args, 0, st));
+            CK(cudaLaunchCooperativeKernel(pcg_fn, dim3(grid), dim3(kT), args, 0, st));
             counted();
             k_heat_scatter<<<grid_of(n), kT, 0, st>>>(n, inv, fixed, imp, x, temps + (size_t)s * n);
             if (!fixed_nodes.empty()) {
