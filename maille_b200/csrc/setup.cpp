@@ -173,6 +173,46 @@ std::vector<int32_t> rcm(const NodeGraph& g) {
     return order;
 }
 
+// The visit order of the MULTICOLOR_BFS ordering's greedy colouring: a breadth-first search from
+// a minimum-degree vertex (the first minimum by index), neighbours in adjacency order, one
+// connected component at a time, reversed. Measured with the oracle's IC(0)-PCG on the
+// lognormal Tet10 cube (10^3, 16^3, 24^3 cells): one colour fewer than colouring in RCM order
+// (16-17 against 18) and 7 % fewer FP64 iterations, for one breadth-first pass instead of RCM's
+// pseudo-peripheral searches and degree sorts. On Tet10 40^3 on the GPU: plain FP64 8 % fewer
+// iterations, the thermal step 12 % fewer, but the mixed form 5 % more (its FP32 Krylov space
+// converges differently), so the elastic solves keep MULTICOLOR.
+std::vector<int32_t> reverse_bfs(const NodeGraph& g) {
+    const int32_t n = (int32_t)g.off.size() - 1;
+    std::vector<int32_t> order;
+    order.reserve(n);
+    Bits visited(n);
+    int32_t scan = 0;
+    for (;;) {
+        while (scan < n && visited.test(scan)) ++scan;
+        if (scan >= n) break;
+        int32_t seed = scan;
+        for (int32_t v = scan + 1; v < n; ++v)
+            if (!visited.test(v) && g.degree(v) < g.degree(seed)) seed = v;
+        visited.set(seed);
+        size_t head = order.size();
+        order.push_back(seed);
+        while (head < order.size()) {
+            if (head + kAhead < order.size()) g.prefetch(order[head + kAhead]);
+            if (head + 2 * kAhead < order.size()) g.prefetch_offset(order[head + 2 * kAhead]);
+            const int32_t v = order[head++];
+            for (int64_t p = g.off[v]; p < g.off[v + 1]; ++p) {
+                const int32_t w = g.adj[p];
+                if (!visited.test(w)) {
+                    visited.set(w);
+                    order.push_back(w);
+                }
+            }
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    return order;
+}
+
 // Greedy colouring visiting vertices in `visit` order (smallest colour no visited neighbour
 // holds); returns colours. A colour never exceeds the vertex degree, so while every degree is
 // below 255 the colours are kept in bytes, which keeps the neighbour lookups in cache.
@@ -332,11 +372,11 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
 
     stage("graph");
     // ordering over kept nodes: order[new] = kept index
-    std::vector<int32_t> order = rcm(g);
+    std::vector<int32_t> order = ordering == MAILLE_ORDER_MULTICOLOR_BFS ? reverse_bfs(g) : rcm(g);
     std::vector<int32_t> colour;
     if (ordering != MAILLE_ORDER_RCM) {
         colour = greedy_colour(g, order);
-        // rows by colour, RCM order inside a colour (a stable counting sort)
+        // rows by colour, visit order inside a colour (a stable counting sort)
         int32_t nc = 0;
         for (int32_t k = 0; k < nk; ++k) nc = std::max(nc, colour[k] + 1);
         std::vector<int64_t> pos((size_t)nc + 1, 0);

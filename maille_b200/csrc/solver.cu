@@ -193,6 +193,10 @@ bool check_problem(const MailleElasticProblem* p, Error& err) {
         err = {MAILLE_INVALID_INPUT, "unknown precision"};
         return false;
     }
+    if (p->ordering < MAILLE_ORDER_AUTO || p->ordering > MAILLE_ORDER_MULTICOLOR_BFS) {
+        err = {MAILLE_INVALID_INPUT, "unknown ordering"};
+        return false;
+    }
     for (int64_t k = 0; k < 3 * p->n_nodes; ++k)
         if (!std::isfinite(p->coords[k])) {
             err = {MAILLE_INVALID_INPUT, "non-finite coordinate at node " + std::to_string(k / 3)};

@@ -103,6 +103,9 @@ def test_invalid_inputs_are_rejected_before_any_device_work(lib):
     assert status(f=f) == _lib.MAILLE_INVALID_INPUT
     assert status(fixed=np.ones_like(p0.fixed)) == _lib.MAILLE_INVALID_INPUT  # nothing free
     assert lib.maille_gpu_elastic_solve(None, None) == _lib.MAILLE_INVALID_INPUT
+    p, keep = problem_struct(**good)
+    p.ordering = 4
+    assert _solve_status(lib, p) == _lib.MAILLE_INVALID_INPUT and "ordering" in _lib.last_error()
     # wrong element family
     p, keep = problem_struct(**good)
     p.nodes_per_elem = 5
@@ -246,6 +249,7 @@ def test_thermal_inputs_are_rejected_before_any_device_work(lib):
     conn[1, 1] = p0.coords.shape[0]
     assert status(conn=conn) == _lib.MAILLE_INVALID_INPUT and "unknown node" in _lib.last_error()
     assert status(fixed=np.ones_like(p0.fixed)) == _lib.MAILLE_INVALID_INPUT
+    assert status(ordering=-1) == _lib.MAILLE_INVALID_INPUT and "ordering" in _lib.last_error()
     assert lib.maille_gpu_thermal_transient(None, None) == _lib.MAILLE_INVALID_INPUT
     if lib.maille_gpu_device_count() == 0:
         assert status() == _lib.MAILLE_CUDA_ERROR  # a valid problem needs a device: no fallback

@@ -11,7 +11,7 @@ import cases
 import maille_b200 as mb
 from maille_b200 import meshgen as mg
 from maille_b200._lib import (MAILLE_FP64, MAILLE_MIXED, MAILLE_ORDER_MULTICOLOR,
-                              MAILLE_ORDER_RCM)
+                              MAILLE_ORDER_MULTICOLOR_BFS, MAILLE_ORDER_RCM)
 
 pytestmark = pytest.mark.gpu
 
@@ -116,7 +116,7 @@ def test_iterative_solution_matches_the_oracle_direct_one(gpu, oracle_lib):
 
 # --- parity with the oracle on the benchmark configurations (reduced sizes) -----------------
 
-@pytest.mark.parametrize("ordering", [MAILLE_ORDER_MULTICOLOR, MAILLE_ORDER_RCM])
+@pytest.mark.parametrize("ordering", [MAILLE_ORDER_MULTICOLOR, MAILLE_ORDER_RCM, MAILLE_ORDER_MULTICOLOR_BFS])
 def test_plain_tet4_config_matches_the_oracle(gpu, oracle_lib, ordering):
     # Plain FP64 Tet4 20^3, pressure 10 on z = 1, z = 0 clamped, reference tolerance 1e-12
     p = mg.plain_tet4(20)
