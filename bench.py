@@ -424,8 +424,8 @@ def pcg_bytes_per_iteration(blocks, nb, vb):
 
 
 # DRAM traffic of the persistent PCG kernel per iteration over its algorithmic bytes, from one ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum of one 8-iteration launch, Tet10 30^3,
-# profiles/k_pcg_tet10_30_full.md: 0.587 GB against 0.560 GB); traffic grows with the blocks, so
+# capture (dram__bytes_read.sum + dram__bytes_write.sum of one 8-iteration launch, Tet10 30^3:
+# 0.587 GB against 0.560 GB, kept in the profile summary of k_pcg); traffic grows with the blocks, so
 # the ratio scales the capture to the benchmark size.
 PCG_TRAFFIC_RATIO = 0.587 / 0.560
 
@@ -666,7 +666,7 @@ def run_ours(args):
                      "ms_per_iteration": info_m["ms_solve"] / info_m["iterations"],
                      "traffic": PCG_TRAFFIC_RATIO * it_bytes,
                      "traffic_note": "bytes per iteration, ncu DRAM bytes of a Tet10 30^3 launch "
-                                     "scaled by blocks (profiles/k_pcg_tet10_30_full.md)"},
+                                     "scaled by blocks (the k_pcg Tet10 30^3 profile summary)"},
         "spmv": {"kernel": "k_spmv<float> (SELL 3x3-block SpMV, FP32, standalone)",
                  "achieved": gbs32, "frac": gbs32 / hbm, "bytes_per_launch": bytes32,
                  "ms_per_launch": ms32,
