@@ -281,3 +281,22 @@ def test_thermal_step_validation_mirrors_the_reference():
     with pytest.raises(mb.MailleError) as e:
         model.solve_step(step, t)
     assert e.value.kind == "NonFiniteTemperature"
+
+
+def test_thermal_load_helper_ignores_out_of_range_items_and_integrates_exactly(lib):
+    # face_rule gives None for a face outside 0..3; an unknown element adds nothing either. On a
+    # unit top face, sum of h T_inf int N dS is h T_inf (area 1) for Tet4 and Tet10 faces alike,
+    # and a uniform source q over the unit cube gives q in total.
+    from maille_b200 import thermal as th
+    for quadratic in (False, True):
+        nodes, tets = mg.box_grid((2, 2, 2), (1.0, 1.0, 1.0))
+        conn = tets
+        if quadratic:
+            nodes, conn = mg.to_quadratic_tet(nodes, tets)
+        ce, cf = mg.faces_on(nodes, conn, 2, 1.0)
+        conv = [(int(e), int(f), 2.0, 30.0) for e, f in zip(ce, cf)]
+        base = th.thermal_loads(nodes, conn, [(e, 5.0) for e in range(conn.shape[0])], conv)
+        assert abs(base.sum() - (5.0 + 2.0 * 30.0)) < 1e-12
+        noisy = th.thermal_loads(nodes, conn, [(e, 5.0) for e in range(conn.shape[0])] + [(conn.shape[0] + 3, 1.0)],
+                                 conv + [(0, 7, 2.0, 30.0), (conn.shape[0], 0, 2.0, 30.0)])
+        assert np.array_equal(base, noisy)
