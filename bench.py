@@ -352,17 +352,26 @@ def thermal_section(mg, steps, device, hbm, cells=40):
     device time of the increments comes from the library's CUDA events. Roofline of the
     persistent scalar PCG: algorithmic bytes per iteration = the left matrix (values + columns)
     once for the SpMV and its strict triangles once per sweep, plus about 16 vector passes."""
+    import torch
     from maille_b200 import thermal as th
     p = mg.thermal_cube(cells, True, increments=10, time_period=0.1)
     f = p.loads + th.thermal_loads(p.coords, p.conn, list(zip(p.s_elem, p.s_value)),
                                    list(zip(p.c_elem, p.c_face, p.c_film, p.c_sink)))
-    s, out = th.solve_problem(p, f=f, fluxes=False, device=device)  # warm-up
+    # inputs and outputs in pinned host memory, as for the elastic end-to-end figure
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    for name in ("coords", "conn", "conductivity", "rho_c", "fixed", "imposed", "initial"):
+        setattr(p, name, pin(getattr(p, name)))
+    f = pin(f)
+    res = dict(temps=pin(np.zeros((p.increments + 1, p.n_nodes))),
+               reactions=pin(np.zeros((p.increments + 1, p.n_nodes))), fluxes=None,
+               iterations=np.zeros(p.increments, np.int32))
+    s, out = th.solve_problem(p, f=f, fluxes=False, device=device, out=res)  # warm-up
     if s != 0:
         return {"workload": p.name, "error": s}
     walls, dev = [], []
     for _ in range(max(1, steps)):
         t0 = time.perf_counter()
-        s, out = th.solve_problem(p, f=f, fluxes=False, device=device)
+        s, out = th.solve_problem(p, f=f, fluxes=False, device=device, out=res)
         walls.append((time.perf_counter() - t0) * 1e3)
         dev.append(out["info"]["ms_steps"])
     info = out["info"]

@@ -123,11 +123,13 @@ def thermal_problem_struct(coords, conn, conductivity, rho_c, fixed, imposed, f,
 
 
 def solve_problem(prob, f=None, tol=1e-12, max_iter=10000, fluxes=True, device=0,
-                  ordering=MAILLE_ORDER_AUTO):
+                  ordering=MAILLE_ORDER_AUTO, out=None):
     """The transient step of a meshgen.ThermalProblem on the GPU. `f` is the assembled heat-load
     vector (None: nodal loads plus the problem's sources and convection through
-    thermal_loads). Returns (status, dict of temps (S + 1, N), reactions (S + 1, N), fluxes
-    (S + 1, E, ngp, 6) or None, iterations (S,), info)."""
+    thermal_loads). `out` may hold preallocated result arrays (temps, reactions, fluxes,
+    iterations; pinned host memory makes the copies back faster). Returns (status, dict of temps
+    (S + 1, N), reactions (S + 1, N), fluxes (S + 1, E, ngp, 6) or None, iterations (S,),
+    info)."""
     L = _lib.load()
     n, ne, npe = prob.n_nodes, prob.n_elems, prob.npe
     ng = 1 if npe == 4 else 4
@@ -139,9 +141,10 @@ def solve_problem(prob, f=None, tol=1e-12, max_iter=10000, fluxes=True, device=0
     p, keep = thermal_problem_struct(prob.coords, prob.conn, prob.conductivity, prob.rho_c, prob.fixed,
                                      prob.imposed, f, prob.initial, prob.time_step, prob.theta, steps,
                                      prob.c_elem, prob.c_face, prob.c_film, tol, max_iter, ordering, device)
-    out = dict(temps=np.zeros((steps + 1, n)), reactions=np.zeros((steps + 1, n)),
-               fluxes=np.zeros((steps + 1, ne, ng, 6)) if fluxes else None,
-               iterations=np.zeros(steps, np.int32))
+    if out is None:
+        out = dict(temps=np.zeros((steps + 1, n)), reactions=np.zeros((steps + 1, n)),
+                   fluxes=np.zeros((steps + 1, ne, ng, 6)) if fluxes else None,
+                   iterations=np.zeros(steps, np.int32))
     r = ThermalResult(temperatures=ptr(out["temps"], _lib._d), reactions=ptr(out["reactions"], _lib._d),
                       heat_fluxes=ptr(out["fluxes"], _lib._d), iterations=ptr(out["iterations"], _lib._i32))
     s = L.maille_gpu_thermal_transient(ctypes.byref(p), ctypes.byref(r))
