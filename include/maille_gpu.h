@@ -1,5 +1,6 @@
 /* maille_gpu.h -- C ABI of the B200 linear-elastic solve path (Tet4/Tet10 stiffness, deterministic
- * sparse assembly, IC(0)-preconditioned conjugate gradients, Gauss-point stresses).
+ * sparse assembly, IC(0)-preconditioned conjugate gradients, Gauss-point stresses), and of the
+ * transient heat conduction step built on the same machinery (maille_gpu_thermal_transient).
  *
  * The entry points replace the iterative branch of maille-core's solve (reference paths, relative
  * to the reference project root):

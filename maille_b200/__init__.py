@@ -1,7 +1,8 @@
 """maille_b200 -- B200 (sm_100a) implementation of maille-core's linear-elastic solve path:
 Tet4/Tet10 element stiffness, deterministic sparse assembly and IC(0)-preconditioned conjugate
-gradients, with Gauss-point stresses. The compute runs in libmaille_gpu.so (CUDA, C ABI in
-include/maille_gpu.h); this package is the host-side mirror of the reference's solve interface.
+gradients, with Gauss-point stresses; and the transient heat conduction step (theta-method) on
+the same machinery. The compute runs in libmaille_gpu.so (CUDA, C ABI in include/maille_gpu.h);
+this package is the host-side mirror of the reference's solve interface.
 """
 from .model import (Bc, Dof, Field, ITERATIVE_FROM, Load, MailleError, Material, Mesh, Model,  # noqa: F401
                     Pressure, SolverHandle, SolverKind, face_pressure_loads)
