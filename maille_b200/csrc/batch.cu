@@ -923,11 +923,13 @@ int32_t refactor_batch(MailleGpuBatch* b, const double* young, const double* poi
 extern "C" {
 
 int32_t maille_gpu_batch_create(const MailleBatchProblem* problem, MailleGpuBatch** out) {
+    NvtxRange nvtx("maille batch create");
     set_last_error("");
     return create_batch(problem, out);
 }
 
 int32_t maille_gpu_batch_solve(MailleGpuBatch* b, const double* f, MailleBatchResult* result) {
+    NvtxRange nvtx("maille batch solve");
     set_last_error("");
     return solve_batch(b, f, result);
 }

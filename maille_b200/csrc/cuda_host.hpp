@@ -7,8 +7,18 @@
 #include <string>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 namespace maille {
+
+// A named range on a profiler's host timeline (NVTX, header-only: without a tool attached the
+// calls do nothing). One per entry point and per major phase.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct CudaFailure {
     std::string what;

@@ -408,6 +408,7 @@ int32_t advance(MailleGpuLargeStrain* s, double t0, double t1, int cuts, int32_t
 }
 
 int32_t ls_run(MailleGpuLargeStrain* s, MailleLargeStrainResult* res) {
+    NvtxRange nvtx("maille large-strain run");
     MailleGpuHandle* h = s->h;
     cudaStream_t st = h->st;
     const int64_t n3 = 3 * s->n_nodes;
@@ -453,6 +454,7 @@ int32_t ls_run(MailleGpuLargeStrain* s, MailleLargeStrainResult* res) {
 }
 
 int32_t ls_backward(MailleGpuLargeStrain* s, const double* dJdR, double* dJdmu, double* dJdlambda) {
+    NvtxRange nvtx("maille large-strain backward");
     if (!s->ran) return ls_fail(MAILLE_INVALID_INPUT, "backward needs a completed run");
     MailleGpuHandle* h = s->h;
     cudaStream_t st = h->st;

@@ -298,6 +298,7 @@ int env_int(const char* name, int dflt) {
 }
 
 int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, MailleElasticResult* res) {
+    NvtxRange nvtx("maille create: analysis, upload, assembly, IC(0)");
     Error err{MAILLE_OK, ""};
     if (!out) return fail({MAILLE_INVALID_INPUT, "null handle pointer"});
     *out = nullptr;
@@ -522,6 +523,7 @@ const char* status_message(int32_t status, int32_t iters, double rel) {
 }
 
 int32_t solve_impl(MailleGpuHandle* h, const double* f, MailleElasticResult* res) {
+    NvtxRange nvtx("maille solve: PCG, reactions, stresses");
     if (!h) return fail({MAILLE_INVALID_INPUT, "null handle"});
     try {
         CK(cudaSetDevice(h->device));

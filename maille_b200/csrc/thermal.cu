@@ -968,6 +968,7 @@ int32_t check_thermal(const MailleThermalProblem* p, std::string& why) {
 }
 
 int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* res) {
+    NvtxRange nvtx("maille thermal transient");
     std::string why;
     if (const int32_t s = check_thermal(p, why); s != MAILLE_OK) return th_fail(s, why);
     const int npe = p->nodes_per_elem;
