@@ -194,6 +194,17 @@ class ThermalModel:
         self.convection = list(convection)
         return self
 
+    def solve(self, device: int = 0, fluxes: bool = True) -> Increment:
+        """Model::solve of the thermal model (model.rs:548-610): K T = F with the imposed
+        temperatures, reactions K T - F on the imposed nodes and the heat fluxes. It is the
+        transient step with no capacity, theta = 1 and one increment (left matrix K, right
+        matrix 0), so it runs on the same device path."""
+        steady = ThermalModel.__new__(ThermalModel)
+        steady.__dict__.update(self.__dict__)
+        steady.rho_c = np.zeros_like(self.rho_c)
+        hist = steady.solve_step(Step(1.0, 1, 1.0), np.zeros(self.coords.shape[0]), device=device, fluxes=fluxes)
+        return hist[1]
+
     def solve_step(self, step: Step, initial, device: int = 0, fluxes: bool = True) -> list[Increment]:
         """Model::solve_step (model.rs:621-706): the t = 0 increment, then one per step."""
         initial = np.asarray(initial, np.float64)

@@ -142,3 +142,32 @@ def test_full_size_transient_matches_the_oracle_summary(gpu):
     assert np.max(np.abs(sums - np.array(g["reaction_sum"]))) < 1e-7 * np.max(np.abs(g["reaction_sum"]))
     assert np.allclose(out["temps"].min(axis=1), g["t_min"], rtol=0, atol=1e-9 * 100.0)
     assert np.allclose(out["temps"].max(axis=1), g["t_max"], rtol=0, atol=1e-9 * 100.0)
+
+
+def test_steady_solve_matches_the_oracle_and_keeps_the_linear_field(gpu, oracle_lib):
+    # Model::solve with Analysis::Thermal through ThermalModel.solve (the transient path with no
+    # capacity, theta = 1, one increment), against the oracle's own steady run, and the slab
+    # between two temperatures with a source (transient.rs:196-223's steady state)
+    from maille_b200.thermal import HeatSource, ThermalModel
+    for name in ("Tet4", "Tet10"):
+        nodes, conn, k = _slab(name, 6)
+        ends = [(int(v), 100.0) for v in np.nonzero(np.abs(nodes[:, 0]) < 1e-12)[0]]
+        ends += [(int(v), 20.0) for v in np.nonzero(np.abs(nodes[:, 0] - 1.0) < 1e-12)[0]]
+        model = ThermalModel(nodes, conn, 2.5, 1.0, bcs=ends)
+        model.with_heat_sources([HeatSource(e, 300.0) for e in range(conn.shape[0])])
+        inc = model.solve()
+        p = mg.ThermalProblem(coords=nodes, conn=conn, conductivity=np.full(conn.shape[0], 2.5),
+                              rho_c=np.zeros(conn.shape[0]), fixed=model.fixed, imposed=model.imposed,
+                              loads=np.zeros(nodes.shape[0]), initial=np.zeros(nodes.shape[0]),
+                              s_elem=np.arange(conn.shape[0], dtype=np.int64),
+                              s_value=np.full(conn.shape[0], 300.0))
+        ref = oracle_lib.thermal_transient(p, solver=1)
+        assert ref["status"] == 0
+        assert _rel(inc.temperatures, ref["temps"][1]) < 1e-9
+        assert _rel(inc.reactions, ref["reactions"][1]) < 1e-8
+        assert _rel(inc.heat_fluxes, ref["fluxes"][1]) < 1e-8
+        # without the source the field is linear and the flux uniform: q = -k dT/dx = 2.5 * 80
+        model.with_heat_sources([])
+        lin = model.solve()
+        assert np.max(np.abs(lin.temperatures - (100.0 - 80.0 * nodes[:, 0]))) < 1e-8
+        assert np.max(np.abs(lin.heat_fluxes[..., 3] - 200.0)) < 1e-6
