@@ -133,9 +133,11 @@ void build_psell(const Symbolic& s, SellKind kind, PsellHost& out);
 // Builds the symbolic analysis. conn is [n_elems * npe] in the caller's node numbering. With
 // pattern = false it stops after the ordering, the levels and the boundary lists (perm, inv,
 // fixmask, level_ptr, incidence, belem, bnodes): the block pattern and the scatter map are then
-// built on the device (analysis.cu).
+// built on the device (analysis.cu). With boundary_lists = false, belem and bnodes (the elements
+// and nodes of the elastic reactions) are left empty.
 bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
-             const uint8_t* fixed, int ordering, Symbolic& s, Error& err, bool pattern = true);
+             const uint8_t* fixed, int ordering, Symbolic& s, Error& err, bool pattern = true,
+             bool boundary_lists = true);
 
 // Face pressure loads f_a -= p * integral(N_a n dS) added into f (assembly.rs:650-674 with the
 // tet branch of face_rule, assembly.rs:556-585). Host-side: part of the host program's assemble.

@@ -272,7 +272,7 @@ void boundary(Symbolic& s, int64_t n_nodes, int npe, int64_t n_elems, const int6
 }  // namespace
 
 bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
-             const uint8_t* fixed, int ordering, Symbolic& s, Error& err, bool pattern) {
+             const uint8_t* fixed, int ordering, Symbolic& s, Error& err, bool pattern, bool boundary_lists) {
     const double t0 = now_ms();
     if (npe != 4 && npe != 10) {
         err = {MAILLE_INVALID_INPUT, "nodes_per_elem must be 4 or 10"};
@@ -436,7 +436,7 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
     stage("levels");
     if (!pattern) {
         g = NodeGraph{};
-        boundary(s, n_nodes, npe, n_elems, conn, fixed);
+        if (boundary_lists) boundary(s, n_nodes, npe, n_elems, conn, fixed);
         stage("boundary");
         s.ms = now_ms() - t0;
         return true;
@@ -528,7 +528,7 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
     s.nl = nl;
 
     stage("scatter map");
-    boundary(s, n_nodes, npe, n_elems, conn, fixed);
+    if (boundary_lists) boundary(s, n_nodes, npe, n_elems, conn, fixed);
     stage("boundary");
     s.ms = now_ms() - t0;
     return true;

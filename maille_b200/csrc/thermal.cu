@@ -994,7 +994,8 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
         // AUTO: MULTICOLOR_BFS (on Tet10 40^3: 17 levels against 18 and 12 % fewer iterations
         // than MULTICOLOR, the step 21 % shorter)
         const int ordering = p->ordering == MAILLE_ORDER_AUTO ? MAILLE_ORDER_MULTICOLOR_BFS : p->ordering;
-        analysed = analyse(n, npe, ne, p->conn, fixed3.data(), ordering, sym, err, /*pattern=*/false);
+        analysed = analyse(n, npe, ne, p->conn, fixed3.data(), ordering, sym, err, /*pattern=*/false,
+                           /*boundary_lists=*/false);
         t_setup1 = now_ms();
     });
     struct Joiner {
