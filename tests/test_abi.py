@@ -300,3 +300,25 @@ def test_thermal_load_helper_ignores_out_of_range_items_and_integrates_exactly(l
         noisy = th.thermal_loads(nodes, conn, [(e, 5.0) for e in range(conn.shape[0])] + [(conn.shape[0] + 3, 1.0)],
                                  conv + [(0, 7, 2.0, 30.0), (conn.shape[0], 0, 2.0, 30.0)])
         assert np.array_equal(base, noisy)
+
+
+def _build_harness(tmp_path):
+    import subprocess
+    exe = tmp_path / "abi_harness"
+    libdir = os.path.join(ROOT, "maille_b200")
+    subprocess.run(["gcc", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "abi_harness.c"), "-L", libdir, "-lmaille_gpu",
+                    f"-Wl,-rpath,{libdir}", "-lm", "-o", str(exe)], check=True)
+    return exe
+
+
+def test_c_harness_drives_the_abi_without_python(lib, tmp_path):
+    # the C ABI from C (as a foreign binding calls it): compiles warning-free against the header,
+    # links against the library, and without a device every call reports MAILLE_CUDA_ERROR
+    import subprocess
+    exe = _build_harness(tmp_path)
+    if lib.maille_gpu_device_count() > 0:
+        pytest.skip("a device is visible (tests/test_gpu_abi_harness.py runs it)")
+    out = subprocess.run([str(exe), "3"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "elastic status 4" in out.stdout and "thermal status 4" in out.stdout
