@@ -171,3 +171,44 @@ def test_steady_solve_matches_the_oracle_and_keeps_the_linear_field(gpu, oracle_
         lin = model.solve()
         assert np.max(np.abs(lin.temperatures - (100.0 - 80.0 * nodes[:, 0]))) < 1e-8
         assert np.max(np.abs(lin.heat_fluxes[..., 3] - 200.0)) < 1e-6
+
+
+def test_steady_known_answers_of_the_reference_through_the_gpu(gpu):
+    # tests/thermal.rs:424-456 (convection-cooled wall, exact) and 472-505 (thin Tet10 fin vs fin
+    # theory) through ThermalModel.solve, with the convection loads from the library's helper
+    import math
+    from maille_b200.thermal import Convection, ThermalModel
+    from test_oracle_thermal import face_positions
+    K, T, L, H = 50.0, 2.0, 4.0, 1.0
+
+    def faces(nodes, conn, on):
+        return [(e, f) for e in range(conn.shape[0]) for f in range(4)
+                if all(on(nodes[v]) for v in conn[e, face_positions(conn.shape[1], f)])]
+
+    t1, h, sink = 20.0, 30.0, 300.0
+    for quadratic in (False, True):
+        nodes, tets = mg.box_grid((4, 1, 2), (L, H, T))
+        conn = tets
+        if quadratic:
+            nodes, conn = mg.to_quadratic_tet(nodes, tets)
+        left = np.nonzero(np.abs(nodes[:, 0]) < 1e-12)[0]
+        model = ThermalModel(nodes, conn, K, 1.0, bcs=[(int(v), t1) for v in left])
+        model.with_convection([Convection(e, f, h, sink)
+                               for e, f in faces(nodes, conn, lambda q: abs(q[0] - L) < 1e-12)])
+        inc = model.solve()
+        exact = t1 + (sink - t1) * h * nodes[:, 0] / (K + h * L)
+        assert np.max(np.abs(inc.temperatures - exact)) < 1e-9
+        power = H * T * K * h * (sink - t1) / (K + h * L)
+        assert abs(inc.reactions[left].sum() + power) < 1e-8 * power
+    hf, length = 0.1, 16.0
+    nodes, tets = mg.box_grid((16, 1, 1), (length, H, T))
+    nodes, conn = mg.to_quadratic_tet(nodes, tets)
+    side = lambda c, lim: abs(c) < 1e-12 or abs(c - lim) < 1e-12  # noqa: E731
+    base = np.nonzero(np.abs(nodes[:, 0]) < 1e-12)[0]
+    model = ThermalModel(nodes, conn, K, 1.0, bcs=[(int(v), 100.0) for v in base])
+    model.with_convection([Convection(e, f, hf, 20.0)
+                           for e, f in faces(nodes, conn, lambda q: side(q[1], H) or side(q[2], T))])
+    inc = model.solve(fluxes=False)
+    m = math.sqrt(hf * 2.0 * (H + T) / (K * H * T))
+    exact = 20.0 + 80.0 * np.cosh(m * (length - nodes[:, 0])) / math.cosh(m * length)
+    assert np.max(np.abs(inc.temperatures - exact)) / 80.0 < 0.002

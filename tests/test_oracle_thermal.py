@@ -5,8 +5,10 @@ The transient tests restate tests/transient.rs of the reference (crate maille-co
 and Tet10 meshes: the same slab L x H x THICKNESS, material (k = 1, rho = 2, c = 0.5, so the
 diffusivity is 1), boundary conditions, steps and tolerances, checked against the same analytic
 solutions (Fourier series of the quenched slab, Heisler series, the amplification factor of the
-theta-method, exact energy balance). The quadrature and capacity tests restate
-quadrature.rs:240-272 and assembly.rs:880-977.
+theta-method, exact energy balance). The steady tests restate tests/thermal.rs (imposed-
+temperature wall, uniform source, convection-cooled wall, thin fin) on the oracle's steady run
+(the step with no capacity, theta = 1, one increment). The quadrature and capacity tests
+restate quadrature.rs:240-272 and assembly.rs:880-977.
 """
 import math
 
@@ -321,3 +323,135 @@ def test_linear_field_gives_the_exact_flux_and_the_iterative_solver_agrees(oracl
         qx = direct["fluxes"][1][..., 3]
         assert np.max(np.abs(qx - 2.5 * 60.0)) < 1e-8
         assert np.max(np.abs(direct["fluxes"][1][..., 4:])) < 1e-8
+
+
+# --- tests/thermal.rs: steady conduction (Model::solve, Analysis::Thermal) -----------------------
+
+KS, TS, LS, HS = 50.0, 2.0, 4.0, 1.0  # tests/thermal.rs:13-17: k, thickness (z), length (x), height (y)
+
+
+def steady_mesh(n, quadratic):
+    nodes, tets = mg.box_grid(n, (LS, HS, TS))
+    conn = tets
+    if quadratic:
+        nodes, conn = mg.to_quadratic_tet(nodes, tets)
+    return nodes, conn
+
+
+def face_positions(npe, face):
+    """Element node positions of a face (mesh.rs:184-198): its corners, then for Tet10 the
+    mid-edge nodes of its edges a-b, b-c, c-a."""
+    a, b, c = (int(v) for v in mg.TET_FACES[face])
+    if npe == 4:
+        return [a, b, c]
+    edges = [tuple(e) for e in mg.TET10_EDGES.tolist()]
+    mid = lambda p, q: 4 + (edges.index((p, q)) if (p, q) in edges else edges.index((q, p)))  # noqa: E731
+    return [a, b, c, mid(a, b), mid(b, c), mid(c, a)]
+
+
+def steady_problem(nodes, conn, bcs=(), source=0.0, convection=None):
+    n, ne = nodes.shape[0], conn.shape[0]
+    fixed = np.zeros(n, np.uint8)
+    imposed = np.zeros(n)
+    for x, value in bcs:
+        on = np.abs(nodes[:, 0] - x) < 1e-12
+        fixed[on] = 1
+        imposed[on] = value
+    p = mg.ThermalProblem(coords=nodes, conn=conn, conductivity=np.full(ne, KS), rho_c=np.zeros(ne),
+                          fixed=fixed, imposed=imposed, loads=np.zeros(n), initial=np.zeros(n))
+    if source:
+        p.s_elem = np.arange(ne, dtype=np.int64)
+        p.s_value = np.full(ne, float(source))
+    if convection is not None:
+        on_face, film, sink = convection
+        ce, cf = [], []
+        for e in range(ne):
+            for f in range(4):
+                # every node of the face (Element::face_nodes: Tet10 faces include their mid-edge
+                # nodes), so an interior face whose corners all lie on the sides is left out
+                if all(on_face(nodes[v]) for v in conn[e, face_positions(conn.shape[1], f)]):
+                    ce.append(e)
+                    cf.append(f)
+        p.c_elem = np.array(ce, np.int64)
+        p.c_face = np.array(cf, np.int32)
+        p.c_film = np.full(len(ce), film)
+        p.c_sink = np.full(len(ce), sink)
+    return p
+
+
+def run_steady(oracle_lib, p):
+    out = oracle_lib.thermal_transient(p, solver=1)
+    assert out["status"] == 0
+    return out["temps"][1], out["reactions"][1], out["fluxes"][1]
+
+
+@pytest.mark.parametrize("quadratic", [False, True])
+def test_wall_with_imposed_temperatures_is_exact_with_the_right_heat_flow(oracle_lib, quadratic):
+    # tests/thermal.rs:99-137 (Tet4 / Tet10 [4, 1, 2])
+    t1, t2 = 100.0, 20.0
+    q = -KS * (t2 - t1) / LS
+    power = q * HS * TS
+    nodes, conn = steady_mesh((4, 1, 2), quadratic)
+    t, r, fl = run_steady(oracle_lib, steady_problem(nodes, conn, bcs=[(0.0, t1), (LS, t2)]))
+    assert np.max(np.abs(t - (t1 + (t2 - t1) * nodes[:, 0] / LS))) < 1e-10
+    assert np.max(np.abs(fl[..., 3] - q)) < 1e-9 * q
+    assert np.max(np.abs(fl[..., 4:])) < 1e-9 * q
+    at = lambda x: np.abs(nodes[:, 0] - x) < 1e-12  # noqa: E731
+    assert abs(r[at(0.0)].sum() - power) < 1e-9 * power
+    assert abs(r[at(LS)].sum() + power) < 1e-9 * power
+
+
+def slab_errors(oracle_lib, nodes, conn):
+    # tests/thermal.rs:286-318: uniform source q, T = 0 on x = 0 and x = L
+    q = 1e3
+    t, r, fl = run_steady(oracle_lib, steady_problem(nodes, conn, bcs=[(0.0, 0.0), (LS, 0.0)], source=q))
+    produced = q * LS * HS * TS
+    assert abs(r.sum() + produced) < 1e-9 * produced
+    x = nodes[:, 0]
+    terr = np.max(np.abs(t - q * x * (LS - x) / (2.0 * KS)))
+    qerr = np.max(np.abs(fl[..., 3] - q * (fl[..., 0] - LS / 2.0)))
+    return terr / (q * LS * LS / (8.0 * KS)), qerr / (q * LS / 2.0)
+
+
+def test_quadratic_elements_are_exact_for_a_uniform_heat_source(oracle_lib):
+    # tests/thermal.rs:320-327 (the Tet10 half)
+    t, q = slab_errors(oracle_lib, *steady_mesh((2, 1, 1), True))
+    assert t < 1e-10 and q < 1e-10, (t, q)
+
+
+def test_linear_elements_are_exact_at_the_nodes_and_their_flux_converges(oracle_lib):
+    # tests/thermal.rs:329-358 (the Tet4 half)
+    errors = [slab_errors(oracle_lib, *steady_mesh((nx, 1, 1), False)) for nx in (4, 8, 16)]
+    for t, q in errors:
+        assert t < 1e-10 and q > 1e-3, errors
+    for a, b in zip(errors, errors[1:]):
+        assert 1.8 < a[1] / b[1] < 2.2, errors
+
+
+@pytest.mark.parametrize("quadratic", [False, True])
+def test_wall_cooled_by_convection_is_exact(oracle_lib, quadratic):
+    # tests/thermal.rs:424-456 (Tet4 / Tet10 [4, 1, 2])
+    t1, h, sink = 20.0, 30.0, 300.0
+    power = HS * TS * KS * h * (sink - t1) / (KS + h * LS)
+    nodes, conn = steady_mesh((4, 1, 2), quadratic)
+    p = steady_problem(nodes, conn, bcs=[(0.0, t1)], convection=(lambda q: abs(q[0] - LS) < 1e-12, h, sink))
+    assert p.c_elem.size > 0
+    t, r, _ = run_steady(oracle_lib, p)
+    assert np.max(np.abs(t - (t1 + (sink - t1) * h * nodes[:, 0] / (KS + h * LS)))) < 1e-10
+    out = r[np.abs(nodes[:, 0]) < 1e-12].sum()
+    assert abs(out + power) < 1e-9 * power
+
+
+def test_thin_fins_match_fin_theory(oracle_lib):
+    # tests/thermal.rs:472-505 (the Tet10 bar: 16 x 1 x 1 cells of 16 x H x T, four lateral faces)
+    h, length = 0.1, 16.0
+    nodes, tets = mg.box_grid((16, 1, 1), (length, HS, TS))
+    nodes, conn = mg.to_quadratic_tet(nodes, tets)
+    m = math.sqrt(h * 2.0 * (HS + TS) / (KS * HS * TS))
+    side = lambda c, lim: abs(c) < 1e-12 or abs(c - lim) < 1e-12  # noqa: E731
+    t0, sink = 100.0, 20.0
+    p = steady_problem(nodes, conn, bcs=[(0.0, t0)],
+                       convection=(lambda q: side(q[1], HS) or side(q[2], TS), h, sink))
+    t, _, _ = run_steady(oracle_lib, p)
+    exact = sink + (t0 - sink) * np.cosh(m * (length - nodes[:, 0])) / math.cosh(m * length)
+    assert np.max(np.abs(t - exact)) / (t0 - sink) < 0.002
