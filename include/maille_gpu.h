@@ -101,13 +101,22 @@ typedef struct {
     int64_t block_rows;         /* free nodes in the 3x3-block system */
     int64_t blocks;             /* 3x3 blocks of the full symmetric pattern */
     int32_t levels;             /* levels of the IC(0) sweeps */
-    double ms_setup;            /* host symbolic analysis (graph, ordering, pattern, scatter map) */
-    double ms_upload;           /* host -> device copies */
-    double ms_assembly;         /* element integration + scatter-reduce assembly */
+    double ms_setup;            /* host ordering (node graph, RCM / colouring), on a host thread that
+                                   runs while the device takes the inputs (create) */
+    double ms_upload;           /* host -> device copies of the inputs (create) */
+    double ms_assembly;         /* scatter-reduce assembly of the element matrices (create,
+                                   refactor) */
     double ms_factor;           /* IC(0) factorisation incl. shift retries */
     double ms_solve;            /* PCG iterations (mixed: incl. refinement) */
     double ms_post;             /* reactions + stresses + von Mises */
     double ms_download;         /* device -> host copies */
+    /* the rest of create, in order on the device stream (each 0 after solve-only calls): */
+    double ms_element;          /* element integration (Ke of every element) */
+    double ms_analysis_wait;    /* host wall time create waited for the ordering thread after
+                                   the element integration was enqueued */
+    double ms_symbolic;         /* device pattern and scatter map (radix sorts), the host plan of
+                                   the sliced layouts and their slot fills */
+    double ms_buffers;          /* numeric buffers and the remaining index uploads */
 } MailleElasticResult;
 
 typedef struct MailleGpuHandle MailleGpuHandle;
@@ -135,6 +144,15 @@ int32_t maille_gpu_create(const MailleElasticProblem* problem, MailleGpuHandle**
 /* Solve K_ff u_f = F_f - K_fc u_c for a new load vector f ([3 n_nodes], NULL = the problem's),
  * then reactions and stresses into `result` (FreeSystem::solve + product + element_stresses). */
 int32_t maille_gpu_solve(MailleGpuHandle* h, const double* f, MailleElasticResult* result);
+
+/* The same solve with device-resident buffers, for callers that chain solves on the GPU (load
+ * cases, an optimisation loop): f_dev [3 n_nodes] device pointer on the handle's device (NULL =
+ * the problem's loads), the displacements (imposed values at fixed DOFs) written to u_dev
+ * [3 n_nodes] device pointer; no reactions, stresses or host copies (FreeSystem::solve,
+ * model.rs:1502-1516, without product and element_stresses). The loads are not checked on the
+ * host: non-finite values end in MAILLE_SINGULAR. Returns when u_dev is written; a backward may
+ * follow. */
+int32_t maille_gpu_solve_device(MailleGpuHandle* h, const double* f_dev, double* u_dev);
 
 /* Adjoint of the last solve: with g = dJ/du ([3 n_nodes], host), solves K_ff lambda_f = g_f with
  * the same PCG and factor (lambda = 0 on fixed DOFs), then
@@ -295,7 +313,9 @@ void maille_gpu_batch_destroy(MailleGpuBatch* b);
  * with the linear amplitude (0,0)-(1,1): each increment is Newton-Raphson to F_int(u) = lambda F
  * with imposed values lambda * imposed (equilibrium, model.rs:923-1022: relative residual
  * ||r_free|| / scale <= newton_tol after at least two residuals, at most newton_max_iter, the
- * increment halved up to 5 times when Newton fails, advance, model.rs:820-870), each linear step
+ * increment halved up to 5 times when Newton does not converge or the tangent is not positive
+ * definite, advance, model.rs:820-870; an inner PCG at its cap ends the run without a cut, as the
+ * reference's IterativeNotConverged does), each linear step
  * K_ff du_f = -r_f - K_fc du_c solved by this library's assembly + IC(0)-PCG. The element
  * response is large_strain_response (finite_strain.rs:119-214) with the neo-Hookean law
  * (finite_strain.rs:40-86), lambda and mu = lame(E, nu) per element (finite_strain.rs:30-35).
@@ -328,7 +348,8 @@ typedef struct {
     double* u;                  /* [increments][3 n_nodes] converged displacements, or NULL */
     double* reactions;          /* [increments][3 n_nodes] F_int - lambda F at fixed DOFs, or NULL */
     int32_t* newton_iterations; /* [increments] residuals of the last equilibrium, or NULL */
-    int32_t* cuts;              /* [increments] interval halvings, or NULL */
+    int32_t* cuts;              /* [increments] interval halvings, or NULL; when the run fails,
+                                   the failing increment's entry holds its halvings so far */
     int64_t newton_total;       /* filled: Newton iterations over the step */
     int64_t pcg_total;          /* filled: PCG iterations over the step */
     double ms_total;
@@ -345,6 +366,12 @@ int32_t maille_gpu_large_strain_backward(MailleGpuLargeStrain* s, const double* 
 /* New per-element E and nu (NULL keeps them); the next run starts from rest. */
 int32_t maille_gpu_large_strain_set_materials(MailleGpuLargeStrain* s, const double* young,
                                               const double* poisson);
+/* Raise (1) or clear (0) the run's cancel flag (the observer's Flow::Stop of
+ * solve_quasi_static_with, model.rs:732, 1203-1218): checked before every Newton iteration and
+ * between the inner PCG's launches; the run then returns MAILLE_CANCELLED (MailleError::Cancelled,
+ * error.rs:156) without a cut. Safe to call from another thread while a run is in progress; a
+ * raised flag stays raised until cleared. */
+void maille_gpu_large_strain_cancel(MailleGpuLargeStrain* s, int32_t flag);
 void maille_gpu_large_strain_destroy(MailleGpuLargeStrain* s);
 
 /* ---- Transient heat conduction: the theta-method ---------------------------------------------
@@ -414,8 +441,18 @@ typedef struct {
 } MailleThermalResult;
 
 /* The whole transient step (Model::solve_step). MAILLE_SINGULAR / MAILLE_NOT_CONVERGED name the
- * first increment whose solve failed; the history before it is returned. */
+ * first increment whose solve failed; MAILLE_CANCELLED the first increment the cancel flag
+ * stopped; the history before it is returned. */
 int32_t maille_gpu_thermal_transient(const MailleThermalProblem* problem, MailleThermalResult* result);
+
+/* Raise (1) or clear (0) the thermal cancel flag of `device` (the observer's Flow::Stop of
+ * solve_step_with, model.rs:628, 1203-1218): every thermal step running or started on that device
+ * checks it on the device before each increment's solve and, when raised, skips that increment
+ * and the rest and returns MAILLE_CANCELLED (MailleError::Cancelled, error.rs:156), with the
+ * history of the increments completed before it. The flag is per device, not per call: it stops
+ * every thermal step on the device and stays raised until cleared. Safe to call from another
+ * thread while a step runs. MAILLE_INVALID_INPUT for a device ordinal outside 0..63. */
+int32_t maille_gpu_thermal_cancel(int32_t device, int32_t flag);
 
 /* Host helper: adds to f ([n_nodes]) the heat-source loads int N q dV of uniform sources
  * (element, q) (element_heat_source / nodal_source, assembly.rs:466-484, element rule TETRA_1 /
@@ -438,9 +475,11 @@ int32_t maille_gpu_thermal_loads(int64_t n_nodes, const double* coords, int32_t 
  * A held by the caller on `device` -- row_ptr [n_block_rows + 1] (int64), col [blocks] (int32
  * block columns), vals [9 * blocks] (row-major blocks), x and y [3 * n_block_rows], xy [1], all
  * device pointers the caller owns -- enqueued on `stream` (cudaStream_t, NULL = the legacy
- * default stream) without waiting. It calls no cudaMalloc, cudaFree or allocating routine: the
- * reduction's partial sums and ticket live in a fixed 8.5 KB device array inside the library,
- * shared by all calls, so calls that overlap on the GPU race and must be ordered by the caller.
+ * default stream) without waiting. x, y and xy must not overlap (an in-place product is refused
+ * with MAILLE_INVALID_INPUT). It calls no cudaMalloc, cudaFree or allocating routine: the
+ * reduction's partial sums and ticket live in a fixed device array inside the library (8200
+ * bytes: 1024 FP64 partial sums and a 4-byte ticket, at a 256-byte boundary), shared by all
+ * calls, so calls that overlap on the GPU race and must be ordered by the caller.
  * The first call on a device looks up that array's address (cudaGetSymbolAddress) with the
  * device current: make it before any stream capture. Sizes beyond
  * MAILLE_NOALLOC_MAX_BLOCK_ROWS are rejected with MAILLE_INVALID_INPUT. The current device of

@@ -44,7 +44,9 @@ class ElasticResult(ctypes.Structure):
         ("levels", ctypes.c_int32), ("ms_setup", ctypes.c_double), ("ms_upload", ctypes.c_double),
         ("ms_assembly", ctypes.c_double), ("ms_factor", ctypes.c_double),
         ("ms_solve", ctypes.c_double), ("ms_post", ctypes.c_double),
-        ("ms_download", ctypes.c_double),
+        ("ms_download", ctypes.c_double), ("ms_element", ctypes.c_double),
+        ("ms_analysis_wait", ctypes.c_double), ("ms_symbolic", ctypes.c_double),
+        ("ms_buffers", ctypes.c_double),
     ]
 
 
@@ -126,6 +128,7 @@ SIGNATURES = {
                           ctypes.c_int32),
     "maille_gpu_solve": ([ctypes.c_void_p, _d, ctypes.POINTER(ElasticResult)], ctypes.c_int32),
     "maille_gpu_backward": ([ctypes.c_void_p, _d, _d, _d], ctypes.c_int32),
+    "maille_gpu_solve_device": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int32),
     "maille_gpu_cancel": ([ctypes.c_void_p, ctypes.c_int32], None),
     "maille_gpu_stream": ([ctypes.c_void_p], ctypes.c_void_p),
     "maille_gpu_destroy": ([ctypes.c_void_p], None),
@@ -156,9 +159,11 @@ SIGNATURES = {
     "maille_gpu_large_strain_run": ([ctypes.c_void_p, ctypes.POINTER(LargeStrainResult)], ctypes.c_int32),
     "maille_gpu_large_strain_backward": ([ctypes.c_void_p, _d, _d, _d], ctypes.c_int32),
     "maille_gpu_large_strain_set_materials": ([ctypes.c_void_p, _d, _d], ctypes.c_int32),
+    "maille_gpu_large_strain_cancel": ([ctypes.c_void_p, ctypes.c_int32], None),
     "maille_gpu_large_strain_destroy": ([ctypes.c_void_p], None),
     "maille_gpu_thermal_transient": ([ctypes.POINTER(ThermalProblem), ctypes.POINTER(ThermalResult)],
                                      ctypes.c_int32),
+    "maille_gpu_thermal_cancel": ([ctypes.c_int32, ctypes.c_int32], ctypes.c_int32),
     "maille_gpu_thermal_loads": ([ctypes.c_int64, _d, ctypes.c_int32, ctypes.c_int64, _i64, ctypes.c_int64,
                                   _i64, _d, ctypes.c_int64, _i64, _i32, _d, _d, _d], ctypes.c_int32),
 }

@@ -185,3 +185,35 @@ def solve_sharded(problems: Sequence, loads: Sequence[np.ndarray], rank: int, wo
         return mine, None
     with BatchSolver([problems[k] for k in mine], [loads[k] for k in mine], device=device, **kw) as b:
         return mine, b.solve()
+
+
+def gather_sharded(mine: List[int], part: Optional[BatchField], n_instances: int, n_rhs: int,
+                   dst: int = 0, group=None) -> Optional[BatchField]:
+    """Collects every rank's (instance ids, BatchField) of solve_sharded on rank `dst` through
+    torch.distributed (any backend; one gather of host objects after the solves, not on the data
+    path) and returns the whole batch's BatchField in instance order there, None on the other
+    ranks. Every rank of the group must call it."""
+    import torch.distributed as dist
+    item = (list(mine), None if part is None else (part.displacements, part.iterations, part.rel_residual,
+                                                  part.status))
+    world = dist.get_world_size(group)
+    out = [None] * world if dist.get_rank(group) == dst else None
+    dist.gather_object(item, out, dst=dst, group=group)
+    if out is None:
+        return None
+    disp: List[Optional[np.ndarray]] = [None] * n_instances
+    it = np.zeros((n_instances, n_rhs), np.int32)
+    rr = np.zeros((n_instances, n_rhs))
+    st = np.zeros(n_instances, np.int32)
+    seen = 0
+    for ids, fields in out:
+        if fields is None:
+            continue
+        d, i, r, s = fields
+        for j, k in enumerate(ids):
+            disp[k] = d[j]
+            it[k], rr[k], st[k] = i[j], r[j], s[j]
+            seen += 1
+    if seen != n_instances:
+        raise MailleError("InvalidInput", f"the ranks returned {seen} of {n_instances} instances")
+    return BatchField(disp, it, rr, st, {"ranks": world})

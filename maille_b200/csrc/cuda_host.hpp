@@ -43,6 +43,9 @@ void* device_alloc(size_t bytes);
 void device_free(void* p);
 // Returns the pool's unused memory of `device` to the device (0, or -1 on a CUDA error).
 int32_t trim_device_memory(int device);
+// Streaming multiprocessors of the current device (cudaDevAttrMultiProcessorCount, cached per
+// device): grid caps are multiples of it.
+int device_sms();
 
 template <typename T>
 T* dalloc(size_t n) {

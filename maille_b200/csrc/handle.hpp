@@ -88,7 +88,7 @@ struct PsellBuf {
 struct MailleGpuHandle {
     int device = 0;
     cudaStream_t st = nullptr;
-    cudaEvent_t ev[8] = {};
+    cudaEvent_t ev[12] = {};  // 0-7: phases of create and solve; 8-11: the set-up split of create
     Symbolic sym;
     int npe = 0;
     int64_t n_nodes = 0, n_elems = 0;

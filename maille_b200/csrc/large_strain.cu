@@ -260,6 +260,10 @@ unsigned blocks_of(int64_t n, int threads) { return (unsigned)std::max<int64_t>(
 constexpr double kNewtonTol = 1e-8;   // model.rs:1220
 constexpr int kNewtonIters = 25;      // model.rs:1222
 constexpr int kMaxCuts = 5;           // model.rs:1224
+// Status of an inner PCG that hit its iteration cap inside the Newton loop: the reference's
+// IterativeNotConverged (error.rs:226-229), which advance passes up without a cut (model.rs:839-842
+// cuts on NotConverged, Singular and PlasticCollapse only). Reported as MAILLE_NOT_CONVERGED.
+constexpr int32_t kIterativeNotConverged = 100;
 
 }  // namespace
 }  // namespace maille
@@ -281,7 +285,7 @@ struct MailleGpuLargeStrain {
     double scale = 0.0;
     int64_t newton_total = 0, pcg_total = 0;
     std::vector<int32_t> newton_iters, cuts;
-    int norm_grid = 148 * 4;
+    int norm_grid = 0;  // 4 blocks per SM, set at creation
     ~MailleGpuLargeStrain() {
         if (h) {
             cudaSetDevice(h->device);
@@ -342,7 +346,7 @@ int32_t ls_linear_solve(MailleGpuLargeStrain* s, const double* rhs, const double
     s->pcg_total += iters;
     if (status != MAILLE_OK) {
         msg = maille::handle_status_message(status, iters, rel);
-        return status;
+        return status == MAILLE_NOT_CONVERGED ? maille::kIterativeNotConverged : status;
     }
     maille::launch_gather_u(s->n_nodes, h->inv, h->fixed, xc, h->x64, out, h->st);
     CK(cudaGetLastError());
@@ -356,6 +360,10 @@ int32_t equilibrium(MailleGpuLargeStrain* s, double lam, double& sc, int32_t& it
     const int64_t n3 = 3 * s->n_nodes;
     int32_t count = 0;
     for (;;) {
+        if (h->cancel.load()) {  // the observer's Flow::Stop between Newton iterations (model.rs:1203-1218)
+            msg = "Cancelled";
+            return MAILLE_CANCELLED;
+        }
         double nr[3];
         ls_responses(s, s->u_trial, lam, nr);
         sc = std::max(std::max(sc, std::sqrt(nr[0])), std::sqrt(nr[1]));
@@ -384,7 +392,9 @@ int32_t equilibrium(MailleGpuLargeStrain* s, double lam, double& sc, int32_t& it
     }
 }
 
-// advance (model.rs:820-870): halves the interval up to kMaxCuts times when Newton fails.
+// advance (model.rs:820-870): halves the interval up to kMaxCuts times when Newton does not
+// converge or meets a tangent that is not positive definite (IC(0) failing every shift, or
+// p.Ap <= 0 in the PCG); an inner PCG at its cap is passed up without a cut.
 int32_t advance(MailleGpuLargeStrain* s, double t0, double t1, int cuts, int32_t& iterations, int32_t& cut_count,
                 std::string& msg) {
     const int64_t n3 = 3 * s->n_nodes;
@@ -426,9 +436,20 @@ int32_t ls_run(MailleGpuLargeStrain* s, MailleLargeStrainResult* res) {
         int32_t iterations = 0, cut_count = 0;
         std::string msg;
         const int32_t status = advance(s, time - dt, time, 0, iterations, cut_count, msg);
-        if (status != MAILLE_OK) return ls_fail(status, "increment " + std::to_string(inc) + ": " + msg);
-        s->newton_iters[inc - 1] = iterations;
         s->cuts[inc - 1] = cut_count;
+        if (status != MAILLE_OK) {
+            if (res) {  // the failing increment's halvings and the counts so far
+                if (res->newton_iterations)
+                    std::memcpy(res->newton_iterations, s->newton_iters.data(), s->increments * sizeof(int32_t));
+                if (res->cuts) std::memcpy(res->cuts, s->cuts.data(), s->increments * sizeof(int32_t));
+                res->newton_total = s->newton_total;
+                res->pcg_total = s->pcg_total;
+                res->ms_total = maille::now_ms() - t0;
+            }
+            return ls_fail(status == maille::kIterativeNotConverged ? MAILLE_NOT_CONVERGED : status,
+                           "increment " + std::to_string(inc) + ": " + msg);
+        }
+        s->newton_iters[inc - 1] = iterations;
         // checkpoint and reactions of the converged increment (resid holds F_int - lam F at u)
         CK(cudaMemcpyAsync(s->ckpt + (size_t)(inc - 1) * n3, s->u, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
         maille::k_ls_reactions<<<maille::blocks_of(n3, 256), 256, 0, st>>>(n3, h->fixed, s->resid,
@@ -574,6 +595,7 @@ int32_t ls_create(const MailleLargeStrainProblem* p, MailleGpuLargeStrain** out)
         s->react = maille::dalloc<double>((size_t)p->increments * n3);
         s->gmu = maille::dalloc<double>(p->n_elems);
         s->glam = maille::dalloc<double>(p->n_elems);
+        s->norm_grid = 4 * maille::device_sms();
         s->partials = maille::dalloc<double>(3 * (size_t)s->norm_grid);
         s->norms = maille::dalloc<double>(4);
         s->ticket = maille::dalloc<unsigned int>(2);
@@ -629,6 +651,10 @@ int32_t maille_gpu_large_strain_set_materials(MailleGpuLargeStrain* s, const dou
     } catch (const CudaFailure& e) {
         return ls_fail(MAILLE_CUDA_ERROR, e.what);
     }
+}
+
+void maille_gpu_large_strain_cancel(MailleGpuLargeStrain* s, int32_t flag) {
+    if (s && s->h) s->h->cancel.store(flag ? 1 : 0);
 }
 
 void maille_gpu_large_strain_destroy(MailleGpuLargeStrain* s) { delete s; }

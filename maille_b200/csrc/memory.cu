@@ -13,6 +13,7 @@
 // implicit synchronisation cudaFree performs), so no kernel still uses the memory when the pool
 // may hand it out again.
 
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 #include <vector>
@@ -67,6 +68,24 @@ void device_free(void* p) {
     cudaDeviceSynchronize();
     cudaFreeAsync(p, d.stream);
     cudaStreamSynchronize(d.stream);
+}
+
+int device_sms() {
+    constexpr int kMaxDevices = 64;
+    static std::atomic<int> cached[kMaxDevices];
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        int sms = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        return sms;
+    }
+    int sms = cached[dev].load(std::memory_order_relaxed);
+    if (sms <= 0) {
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        cached[dev].store(sms, std::memory_order_relaxed);
+    }
+    return sms;
 }
 
 int32_t trim_device_memory(int device) {

@@ -16,6 +16,7 @@
 // (cudaGetSymbolAddress) and caches it. Make that first call before starting any stream capture.
 
 #include <atomic>
+#include <cstddef>
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -36,12 +37,20 @@ constexpr int kNaThreads = 256;
 constexpr int kNaWarps = kNaThreads / 32;
 constexpr int kNaMaxBlocks = 1024;  // partial sums held in the scratch array
 
-// Scratch of the reduction: kNaMaxBlocks partial sums, then the ticket counter (8 KB + 256 B).
+// Scratch of the reduction: kNaMaxBlocks partial sums, then the ticket counter: 8200 bytes (8192
+// + 4, padded to the struct's 8-byte alignment), placed at a 256-byte boundary.
 struct NoallocScratch {
     double partials[kNaMaxBlocks];
     unsigned int ticket;
 };
+static_assert(sizeof(NoallocScratch) == 8200, "the scratch size stated in maille_gpu.h");
 static __device__ __align__(256) NoallocScratch g_noalloc_scratch;
+
+// [a, a + na) and [b, b + nb) share a byte
+bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+    const uintptr_t pa = reinterpret_cast<uintptr_t>(a), pb = reinterpret_cast<uintptr_t>(b);
+    return pa < pb + nb && pb < pa + na;
+}
 
 // y_I = sum_J A_IJ x_J for block rows I (one warp per row, lanes over the row's blocks), the
 // partial sums of x . y per block in the scratch, the ordered total by the last block to finish.
@@ -102,6 +111,14 @@ extern "C" int32_t maille_gpu_bsr3_spmv_dot_noalloc(int32_t device, int64_t n_bl
     }
     if (!row_ptr || !col || !vals || !x || !y || !xy) {
         maille::set_last_error("null device pointer");
+        return MAILLE_INVALID_INPUT;
+    }
+    // warps write rows of y while others still read x: an in-place or overlapping call would
+    // read half-updated entries (the kernel's pointers are __restrict__)
+    const size_t vec_bytes = 3 * (size_t)n_block_rows * sizeof(double);
+    if (overlaps(x, vec_bytes, y, vec_bytes) || overlaps(xy, sizeof(double), y, vec_bytes) ||
+        overlaps(xy, sizeof(double), x, vec_bytes)) {
+        maille::set_last_error("x, y and xy must not overlap");
         return MAILLE_INVALID_INPUT;
     }
     if (device < 0 || device >= 64) {

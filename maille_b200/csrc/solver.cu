@@ -77,7 +77,8 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 
 int grid_for_slices(int64_t slices) {
     int64_t g = (slices + kWarps - 1) / kWarps;
-    if (g > 148 * 8) g = 148 * 8;
+    const int64_t cap = 8 * (int64_t)device_sms();
+    if (g > cap) g = cap;
     return (int)(g < 1 ? 1 : g);
 }
 
@@ -389,12 +390,17 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         h->h_f0 = h->h_f;
         h->fixed = dupload(h->h_fixed.data(), n3, st);
         h->ke = dalloc<double>((size_t)p->n_elems * np * 9);
+        CK(cudaEventRecord(h->ev[8], st));  // inputs copied
         {
             ElemIn in{h->n_elems, h->coords, h->conn, h->young, h->poisson};
             launch_elem_stiffness(h->npe, in, h->ke, st);
         }
+        CK(cudaEventRecord(h->ev[9], st));  // element matrices integrated
+        const double t_wait0 = now_ms();
         analysis.join();
+        const double t_wait1 = now_ms();
         if (!analysed) return fail(err);
+        CK(cudaEventRecord(h->ev[10], st));  // symbolic: the ordering is known
         if (h->sym.levels >= kMaxLevels) return fail({MAILLE_INVALID_INPUT, "too many IC(0) levels"});
         // symbolic
         h->perm = dupload(s.perm.data(), s.perm.size(), st);
@@ -429,6 +435,7 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
             h->pl.upload(pt, s.nb, st);
             h->pu.upload(pt, s.nb, st);
         }
+        CK(cudaEventRecord(h->ev[11], st));  // pattern and layouts on the device
         h->inc_ptr = dupload(s.inc_ptr.data(), s.inc_ptr.size(), st);
         h->inc = dupload(s.inc.data(), s.inc.size(), st);
         h->belem = dupload(s.belem.data(), s.belem.size(), st);
@@ -477,7 +484,6 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         CK(cudaMemsetAsync(h->scal, 0, sizeof(PcgScalars), st));
         CK(cudaMallocHost(&h->h_scal, sizeof(PcgScalars)));
         CK(cudaMallocHost(&h->h_sum, 4 * sizeof(double)));
-        h->partials = dalloc<double>(4 * 148 * 8);  // >= 4 slots x the persistent grid
         h->dsum = dalloc<double>(4);
         h->dticket = dalloc<unsigned int>(1);
         CK(cudaMemsetAsync(h->dticket, 0, sizeof(unsigned int), st));
@@ -487,7 +493,10 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         CK(cudaMemsetAsync(h->claim, 0, 4 * sizeof(int32_t), st));
         h->persist_grid = is_mixed(h.get()) ? pcg_persistent_grid<float, true>(h->sk.h.lpr)
                                             : pcg_persistent_grid<double, false>(h->sk.h.lpr);
-        h->persist_grid = std::min(h->persist_grid, 148 * 8);  // partials hold 4 x 1184 blocks
+        // 4 reduction slots for every block of the persistent grid and of the norm kernels
+        // (grids capped at 8 and 4 blocks per SM)
+        h->persist_grid = std::min(h->persist_grid, 8 * device_sms());
+        h->partials = dalloc<double>((size_t)4 * 8 * device_sms());
         if (env_int("MAILLE_PHASE_TIMING", 0)) {
             h->timing = dalloc<unsigned long long>(8);
             CK(cudaMemsetAsync(h->timing, 0, 8 * sizeof(unsigned long long), st));
@@ -500,7 +509,11 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         CK(cudaStreamSynchronize(st));
         if (res) {
             res->ms_setup = t_setup1 - t_setup0;
-            res->ms_upload = elapsed(h->ev[0], h->ev[1]);
+            res->ms_upload = elapsed(h->ev[0], h->ev[8]);
+            res->ms_element = elapsed(h->ev[8], h->ev[9]);
+            res->ms_analysis_wait = t_wait1 - t_wait0;
+            res->ms_symbolic = elapsed(h->ev[10], h->ev[11]);
+            res->ms_buffers = elapsed(h->ev[11], h->ev[1]);
             res->ms_assembly = elapsed(h->ev[1], h->ev[2]);
             res->ms_factor = elapsed(h->ev[2], h->ev[3]);
         }
@@ -614,6 +627,41 @@ int32_t solve_impl(MailleGpuHandle* h, const double* f, MailleElasticResult* res
     return MAILLE_OK;
 }
 
+// FreeSystem::solve with device-resident loads and displacements: no reactions, stresses or host
+// copies (the chained-solve form of solve_impl).
+int32_t solve_device_impl(MailleGpuHandle* h, const double* f_dev, double* u_dev) {
+    NvtxRange nvtx("maille solve (device buffers)");
+    if (!h || !u_dev) return fail({MAILLE_INVALID_INPUT, "null handle or displacement buffer"});
+    try {
+        CK(cudaSetDevice(h->device));
+        cudaStream_t st = h->st;
+        const int64_t n3 = 3 * h->n_nodes;
+        if (f_dev) {
+            CK(cudaMemcpyAsync(h->f, f_dev, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            h->f_cur = h->f;
+        } else {
+            h->h_f = h->h_f0;
+            h->f_cur = h->f0;
+        }
+        build_rhs(h);
+        int32_t iters = 0, outer = 1;
+        double rel = 0.0;
+        const int32_t status = run_pcg(h, &iters, &outer, &rel);
+        if (status != MAILLE_OK) {
+            CK(cudaStreamSynchronize(st));
+            set_error(status_message(status, iters, rel));
+            return status;
+        }
+        launch_gather_u(h->n_nodes, h->inv, h->fixed, h->imposed, h->x64, h->u_full, st);
+        CK(cudaMemcpyAsync(u_dev, h->u_full, n3 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        h->solved = true;
+    } catch (const CudaFailure& e) {
+        return fail({MAILLE_CUDA_ERROR, e.what});
+    }
+    return MAILLE_OK;
+}
+
 int32_t backward_impl(MailleGpuHandle* h, const double* dJdu, double* dJdE, double* lambda) {
     if (!h || !dJdu || !dJdE) return fail({MAILLE_INVALID_INPUT, "null argument"});
     if (!h->solved) return fail({MAILLE_INVALID_INPUT, "backward needs a solve first"});
@@ -696,6 +744,11 @@ int32_t maille_gpu_create(const MailleElasticProblem* problem, MailleGpuHandle**
 int32_t maille_gpu_solve(MailleGpuHandle* h, const double* f, MailleElasticResult* result) {
     g_last_error.clear();
     return solve_impl(h, f, result);
+}
+
+int32_t maille_gpu_solve_device(MailleGpuHandle* h, const double* f_dev, double* u_dev) {
+    g_last_error.clear();
+    return solve_device_impl(h, f_dev, u_dev);
 }
 
 int32_t maille_gpu_backward(MailleGpuHandle* h, const double* dJdu, double* dJdE, double* lambda) {

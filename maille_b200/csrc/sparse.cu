@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cmath>
 
+#include "cuda_host.hpp"
 #include "reduce.cuh"
 #include "sparse.cuh"
 
@@ -15,10 +16,12 @@ namespace {
 
 constexpr int kThr = 256;
 constexpr int kWarp = kThr / 32;
-constexpr int kMaxGrid = 148 * 8;
+// blocks per SM at most for the grid-stride kernels (the grid is this times the SM count)
+constexpr int kMaxBlocksPerSm = 8;
 
-inline int grid_for(int64_t items, int per_block, int cap = kMaxGrid) {
+inline int grid_for(int64_t items, int per_block, int blocks_per_sm = kMaxBlocksPerSm) {
     int64_t g = (items + per_block - 1) / per_block;
+    const int64_t cap = (int64_t)blocks_per_sm * device_sms();
     if (g > cap) g = cap;
     return (int)(g < 1 ? 1 : g);
 }
@@ -225,7 +228,7 @@ template <typename T>
 void launch_norm2(int64_t n, const T* v, double* partials, unsigned int* ticket, double* out,
                   cudaStream_t st) {
     counted();
-    k_norm2<T><<<grid_for(n, kThr, 148 * 4), kThr, 0, st>>>(n, v, partials, ticket, out);
+    k_norm2<T><<<grid_for(n, kThr, 4), kThr, 0, st>>>(n, v, partials, ticket, out);
 }
 
 template <typename T>
@@ -243,7 +246,7 @@ void launch_diag_fill(int32_t nb, const int64_t* diag, const double* F, T* D, cu
 
 void launch_cast(int64_t n, const double* a, float* b, cudaStream_t st) {
     counted();
-    k_cast<<<grid_for(n, kThr, 148 * 32), kThr, 0, st>>>(n, a, b);
+    k_cast<<<grid_for(n, kThr, 32), kThr, 0, st>>>(n, a, b);
 }
 
 #define MAILLE_INST(T)                                                                          \

@@ -30,6 +30,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -53,7 +54,9 @@ namespace {
 constexpr int kT = 256;  // threads per block of every kernel here
 
 inline void counted() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
-inline int grid_of(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + kT - 1) / kT, 148 * 64)); }
+inline int grid_of(int64_t n) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + kT - 1) / kT, 64 * (int64_t)device_sms()));
+}
 
 // ---- quadrature (quadrature.rs) and faces (shape.rs:129-135, mesh.rs:184-198) --------------
 
@@ -492,9 +495,9 @@ struct HeatPcg {
     unsigned long long epoch0;       // the launch's sweeps tag their records epoch0 + 1, + 2, ...
     double tol;
     int32_t max_iter;
-    const int32_t* prev_status;      // status of the previous increment (nullptr for the first)
     int32_t* status;                 // this increment: 0 ok, 1 singular, 2 cap reached, 3 wait
-                                     // timeout, 5 skipped after an earlier failure
+                                     // timeout; set before the launch by k_heat_gate to 5 (skipped
+                                     // after an earlier failure) or 6 (cancelled), else 0
     int32_t* iterations;
     double* rel;
     unsigned long long* timing;      // optional [4] ns per phase (block 0): spmv, update, sweeps, p
@@ -659,6 +662,18 @@ __device__ __forceinline__ double heat_sweeps(const HeatPcg& a, unsigned long lo
     return rz;
 }
 
+// Decides, before increment s's PCG launch, whether it runs: 5 when an earlier increment failed or
+// was cancelled, 6 when the cancel flag (mapped host memory) is raised, 0 otherwise. One thread
+// reads the flag once, so every block of the cooperative launch that follows sees one decision.
+__global__ void k_heat_gate(const volatile int32_t* cancel, const int32_t* prev_status, int32_t* status) {
+    int32_t g = 0;
+    if (prev_status && *prev_status != 0)
+        g = 5;
+    else if (cancel && *cancel != 0)
+        g = 6;
+    *status = g;
+}
+
 // IC(0)-PCG of one increment from x = 0 (Pcg::solve, iterative.rs:210-248) in one cooperative
 // launch: SpMV, the x / r update, the dataflow preconditioner and the p update, each closed by a
 // grid barrier (four per iteration). (Fusing the two updates into the SpMV and the sweeps saves
@@ -668,9 +683,8 @@ __global__ void __launch_bounds__(kT, 2) k_heat_pcg(HeatPcg a) {
     __shared__ double sh[kT / 32];
     cg::grid_group grid = cg::this_grid();
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
-    if (a.prev_status && *a.prev_status != 0) {  // an earlier increment failed: nothing to solve
+    if (*a.status != 0) {  // gated off before the launch (an earlier failure, or cancelled)
         if (lead) {
-            *a.status = 5;
             *a.iterations = 0;
             *a.rel = 0.0;
         }
@@ -885,6 +899,35 @@ __global__ void k_heat_flux(int64_t ne, const double* __restrict__ coords, const
 }
 
 // ---- host driver -----------------------------------------------------------------------------
+
+// Cancel flags of the thermal step, one per device, in mapped pinned host memory: the host raises
+// one with maille_gpu_thermal_cancel and k_heat_gate reads it on the device before every
+// increment, so the whole step stays enqueued at once without a host synchronisation per
+// increment.
+constexpr int kMaxCancelDevices = 64;
+std::mutex g_cancel_mutex;
+int32_t* g_cancel_host = nullptr;
+
+int32_t* cancel_flags() {
+    std::lock_guard<std::mutex> lock(g_cancel_mutex);
+    if (!g_cancel_host) {
+        void* p = nullptr;
+        CK(cudaHostAlloc(&p, kMaxCancelDevices * sizeof(int32_t), cudaHostAllocMapped | cudaHostAllocPortable));
+        std::memset(p, 0, kMaxCancelDevices * sizeof(int32_t));
+        g_cancel_host = static_cast<int32_t*>(p);
+    }
+    return g_cancel_host;
+}
+
+// The device's flag as the current device addresses it (nullptr past kMaxCancelDevices: such a
+// device's steps cannot be cancelled).
+const int32_t* cancel_flag_device(int device) {
+    if (device < 0 || device >= kMaxCancelDevices) return nullptr;
+    int32_t* h = cancel_flags() + device;
+    void* d = nullptr;
+    CK(cudaHostGetDevicePointer(&d, h, 0));
+    return static_cast<const int32_t*>(d);
+}
 
 int32_t th_fail(int32_t status, const std::string& m) {
     set_last_error(m);
@@ -1237,6 +1280,7 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
             timing = mem.take(dalloc<unsigned long long>(4));
             CK(cudaMemsetAsync(timing, 0, 4 * sizeof(unsigned long long), st));
         }
+        const int32_t* d_cancel = cancel_flag_device(p->device);
         CK(cudaEventRecord(ev[4], st));
         counted();
         k_heat_initial<<<grid_of(n), kT, 0, st>>>(n, inv, fixed, imp, initial, temps, x);
@@ -1244,10 +1288,11 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
         for (int32_t s = 1; s <= steps; ++s) {
             counted();
             k_heat_rhs<<<grid_of((int64_t)sk.h.nslices() * 32), kT, 0, st>>>(sk.dev(), Rv, x, g, b);
+            counted();
+            k_heat_gate<<<1, 1, 0, st>>>(d_cancel, s > 1 ? d_status + (s - 2) : nullptr, d_status + (s - 1));
             HeatPcg a{nb, sk.dev(), sl.dev(), su.dev(), bwd_slice, Av, Lv, Uv, D, b, x, r, pp, ap, yrec, zrec,
-                      partials, timeout, (unsigned long long)s << 32, tol, max_iter,
-                      s > 1 ? d_status + (s - 2) : nullptr, d_status + (s - 1), d_iters + (s - 1), d_rel + (s - 1),
-                      timing};
+                      partials, timeout, (unsigned long long)s << 32, tol, max_iter, d_status + (s - 1),
+                      d_iters + (s - 1), d_rel + (s - 1), timing};
             void* args[] = {&a};
             counted();
             CK(cudaLaunchCooperativeKernel(pcg_fn, dim3(grid), dim3(kT), args, 0, st));
@@ -1313,6 +1358,8 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
             res->ms_download = now_ms() - t_dl0;
         }
         for (int32_t s = 0; s < steps; ++s) {
+            if (h_status[s] == 6)
+                return th_fail(MAILLE_CANCELLED, "Cancelled before increment " + std::to_string(s + 1));
             if (h_status[s] == 1) return th_fail(MAILLE_SINGULAR, "Singular at increment " + std::to_string(s + 1));
             if (h_status[s] == 3)
                 return th_fail(MAILLE_CUDA_ERROR, "a sweep record wait timed out at increment " + std::to_string(s + 1));
@@ -1352,6 +1399,17 @@ int32_t maille_gpu_thermal_transient(const MailleThermalProblem* problem, Maille
     set_last_error("");
     if (!problem) return th_fail(MAILLE_INVALID_INPUT, "null problem");
     return thermal_transient(problem, result);
+}
+
+int32_t maille_gpu_thermal_cancel(int32_t device, int32_t flag) {
+    set_last_error("");
+    if (device < 0 || device >= kMaxCancelDevices) return th_fail(MAILLE_INVALID_INPUT, "device out of range");
+    try {
+        *(volatile int32_t*)(cancel_flags() + device) = flag ? 1 : 0;
+    } catch (const CudaFailure& e) {
+        return th_fail(MAILLE_CUDA_ERROR, e.what);
+    }
+    return MAILLE_OK;
 }
 
 int32_t maille_gpu_thermal_loads(int64_t n_nodes, const double* coords, int32_t npe, int64_t n_elems,

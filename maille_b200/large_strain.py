@@ -79,8 +79,19 @@ class LargeStrainSolver:
         cuts = np.zeros(self.increments, np.int32)
         res = _lib.LargeStrainResult(u=ptr(u, _d), reactions=ptr(r, _d), newton_iterations=ptr(it, _i32),
                                      cuts=ptr(cuts, _i32))
-        _raise_for(self._L.maille_gpu_large_strain_run(self._h, ctypes.byref(res)))
-        return LargeStrainHistory(u, r, it, cuts, res.newton_total, res.pcg_total, res.ms_total)
+        status = self._L.maille_gpu_large_strain_run(self._h, ctypes.byref(res))
+        history = LargeStrainHistory(u, r, it, cuts, res.newton_total, res.pcg_total, res.ms_total)
+        try:
+            _raise_for(status)
+        except MailleError as e:
+            e.history = history  # the counts up to the failing increment, its cuts included
+            raise
+        return history
+
+    def cancel(self, flag: bool = True):
+        """Raises (or clears) the cancel flag: the run stops before its next Newton iteration or
+        inner PCG launch with MailleError("Cancelled")."""
+        self._L.maille_gpu_large_strain_cancel(self._h, 1 if flag else 0)
 
     def backward(self, dJdR):
         g = np.ascontiguousarray(dJdR, np.float64).reshape(self.increments, self.n3)

@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import MAILLE_ORDER_AUTO, ThermalProblem, ThermalResult, ptr
-from .model import MailleError, _STATUS_KIND
+from .model import MailleError, _STATUS_KIND, _raise_for
 
 
 @dataclass
@@ -151,6 +151,14 @@ def solve_problem(prob, f=None, tol=1e-12, max_iter=10000, fluxes=True, device=0
     out["info"] = {k: getattr(r, k) for k, _ in ThermalResult._fields_
                    if k not in ("temperatures", "reactions", "heat_fluxes", "iterations")}
     return s, out
+
+
+def cancel(flag: bool = True, device: int = 0):
+    """Raises (or clears) the thermal cancel flag of `device`: every transient step on that device
+    stops before its next increment and returns status MAILLE_CANCELLED (MailleError("Cancelled")
+    from ThermalModel.solve_step), with the increments completed before it. The flag stays raised
+    until cleared."""
+    _raise_for(_lib.load().maille_gpu_thermal_cancel(device, 1 if flag else 0))
 
 
 class ThermalModel:

@@ -260,7 +260,8 @@ def large_strain_run(prob, increments: int = 10, newton_tol: float = 1e-8, newto
     """Model::solve_quasi_static of a neo-Hookean Tet4 Problem (Kinematics::Large, linear ramp of
     the loads and imposed values over `increments` equal increments). Returns a dict: status,
     u_hist (increments, 3N) checkpoints, reactions (increments, 3N), newton (increments,), cuts,
-    newton_total, pcg_total, wall_s."""
+    newton_total, pcg_total, wall_s, and for the increment the run stopped at (the last one on
+    success): stop_increment and stop_cuts (its interval halvings)."""
     coords = _c(prob.coords, np.float64)
     conn = _c(prob.conn, np.int64)
     n = coords.size
@@ -268,7 +269,7 @@ def large_strain_run(prob, increments: int = 10, newton_tol: float = 1e-8, newto
     rh = np.zeros((increments, n))
     it = np.zeros(increments, np.int32)
     cuts = np.zeros(increments, np.int32)
-    info = np.zeros(2)
+    info = np.zeros(4)
     t0 = time.perf_counter()
     s = lib().oracle_large_strain_run(
         coords.shape[0], _p(coords, _d), conn.shape[0], _p(conn, _i64), _p(_c(prob.young, np.float64), _d),
@@ -276,7 +277,8 @@ def large_strain_run(prob, increments: int = 10, newton_tol: float = 1e-8, newto
         _p(_c(prob.imposed, np.float64), _d), _p(_c(prob.loads, np.float64), _d), increments, newton_tol,
         newton_max, pcg_tol, pcg_max, _p(uh, _d), _p(rh, _d), _p(it, _i32), _p(cuts, _i32), _p(info, _d))
     return dict(status=s, u_hist=uh, reactions=rh, newton=it, cuts=cuts, newton_total=int(info[0]),
-                pcg_total=int(info[1]), wall_s=time.perf_counter() - t0)
+                pcg_total=int(info[1]), stop_cuts=int(info[2]), stop_increment=int(info[3]),
+                wall_s=time.perf_counter() - t0)
 
 
 def large_strain_gradient(prob, u_hist, dJdR, pcg_tol: float = 1e-12, pcg_max: int = 10000):

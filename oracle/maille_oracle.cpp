@@ -44,6 +44,10 @@ constexpr size_t ITERATIVE_FROM = 100000;
 
 // status codes shared with the tests (mirror of MailleError on this path, src/error.rs:224-229)
 enum Status : int { OK = 0, SINGULAR = 1, NOT_CONVERGED = 2, INVALID = 3 };
+// Inside the quasi-static Newton loop only: an inner PCG that hit its cap
+// (MailleError::IterativeNotConverged, error.rs:226-229), which advance (model.rs:839-842) does
+// not answer with a cut, unlike Newton's NotConverged; reported to callers as NOT_CONVERGED.
+constexpr int ITERATIVE_NOT_CONVERGED = 4;
 
 // --- quadrature: src/quadrature.rs ------------------------------------------------------------
 
@@ -955,13 +959,15 @@ struct QuasiStatic {
                 minus[g] = -residual[g];
             }
             const int st = free_solve(t, m, tangents, minus, du, pcg_tol, pcg_max, pcg_iters);
+            if (st == NOT_CONVERGED) return ITERATIVE_NOT_CONVERGED;
             if (st != OK) return st;
             for (size_t g = 0; g < n; ++g) uu[g] += du[g];
         }
     }
 
     // advance, model.rs:820-870: Newton from the committed state, halving the interval up to
-    // MAX_CUTS times when Newton fails or meets a non-positive-definite tangent.
+    // MAX_CUTS times when Newton fails or meets a non-positive-definite tangent (NotConverged or
+    // Singular, model.rs:839-842); an inner PCG at its cap is passed up without a cut.
     int advance(double t0, double t1, int cuts, Vec& reactions, size_t& iterations, int& cut_count) {
         Vec trial = u;
         double sc = scale;
@@ -1476,7 +1482,8 @@ void oracle_nodal_stresses(int64_t n_nodes, int npe, int64_t n_elems, const int6
 // imposed values scaled by lambda(t) = t), with IC(0)-PCG inner solves to pcg_tol. Per increment:
 // the converged displacements (the checkpoints, [increments][3 n_nodes]), the reactions
 // F_int - lambda F at fixed DOFs ([increments][3 n_nodes]), the Newton iterations of the last
-// equilibrium and the cuts. info: [0] total Newton iterations, [1] total PCG iterations.
+// equilibrium and the cuts. info: [0] total Newton iterations, [1] total PCG iterations, [2] the
+// cuts of the increment the run stopped at (the last one on success), [3] that increment.
 int oracle_large_strain_run(int64_t n_nodes, const double* coords, int64_t n_elems, const int64_t* conn,
                             const double* young, const double* poisson, const uint8_t* fixed,
                             const double* imposed, const double* loads, int increments, double newton_tol,
@@ -1498,6 +1505,13 @@ int oracle_large_strain_run(int64_t n_nodes, const double* coords, int64_t n_ele
         size_t iterations = 0;
         int cut_count = 0;
         const int st = qs.advance(time - dt, time, 0, reactions, iterations, cut_count);
+        if (info) {
+            info[0] = (double)qs.newton_total;
+            info[1] = (double)qs.pcg_iters;
+            info[2] = (double)cut_count;
+            info[3] = (double)inc;
+        }
+        if (st == ITERATIVE_NOT_CONVERGED) return NOT_CONVERGED;
         if (st != OK) return st;
         std::copy(qs.u.begin(), qs.u.end(), u_hist + (size_t)(inc - 1) * n);
         std::copy(reactions.begin(), reactions.end(), r_hist + (size_t)(inc - 1) * n);

@@ -2,8 +2,10 @@
 to crates/maille-core of the reference): the uniform-strain patch test (tests/solid.rs:52-116),
 uniaxial traction (tests/solid.rs:118-175), the cantilever vs beam theory (tests/solid.rs:186-279),
 the hydrostatic cube under face pressure (tests/pressure.rs:194-224), the PCG-vs-direct Tet10
-cantilever and the unconstrained structure (tests/iterative.rs:45-83, 199-224), and the
-reference's examples/cube model (tests/golden/cube_example.json)."""
+cantilever and the unconstrained structure (tests/iterative.rs:45-83, 199-224), the
+reference's examples/cube model (tests/golden/cube_example.json), and a nearly incompressible
+block on which IC(0) breaks down at the first diagonal shifts (the ladder of Pcg::new,
+iterative.rs:14, 201-207)."""
 from __future__ import annotations
 
 import json
@@ -182,3 +184,20 @@ def grid_laplacian_elements(n):
     idx = lambda i, j: i + n * j  # noqa: E731
     return [[idx(i, j), idx(i + 1, j), idx(i + 1, j + 1), idx(i, j + 1)]
             for j in range(n - 1) for i in range(n - 1)]
+
+
+def nearly_incompressible(cells, quadratic: bool, nu: float, size=(1.0, 1.0, 1.0)) -> Problem:
+    """A box clamped on z = 0 under one downward point load at its highest node, every element
+    with Poisson ratio `nu` close to 1/2. IC(0) of such a matrix meets a pivot <= 1e-12 a_ii
+    (iterative.rs:160-163) at shift 0 and at the first shifts of the ladder, and succeeds later:
+    Tet10 2^3 at nu = 0.49 needs shift 0.1 under RCM (1 under multicolouring); Tet4 4^3 at
+    nu = 0.4999 needs 0.1 under every ordering tried (scalar and node RCM, multicolour, natural)."""
+    nodes, conn = box(cells, size, quadratic)
+    n = nodes.shape[0]
+    fixed = np.zeros(3 * n, np.uint8)
+    bottom = np.nonzero(np.abs(nodes[:, 2]) < 1e-12)[0]
+    for c in range(3):
+        fixed[3 * bottom + c] = 1
+    loads = np.zeros(3 * n)
+    loads[3 * int(np.argmax(nodes[:, 2])) + 2] = -1.0
+    return problem(nodes, conn, nu=nu, fixed=fixed, loads=loads, name=f"incompressible_{nu}")

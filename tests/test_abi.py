@@ -118,6 +118,25 @@ def test_handle_entry_points_reject_null_arguments_without_device_work(lib):
     assert lib.maille_gpu_nodal_stresses(None, _lib.ptr(out, _lib._d), _lib.ptr(out, _lib._d)) == _lib.MAILLE_INVALID_INPUT
     assert lib.maille_gpu_wait_selftest(0, 1, None) == _lib.MAILLE_INVALID_INPUT
     assert "null" in _lib.last_error()
+    # cancel flags: a null handle is ignored, a device ordinal out of range is refused
+    assert lib.maille_gpu_solve_device(None, None, None) == _lib.MAILLE_INVALID_INPUT
+    lib.maille_gpu_large_strain_cancel(None, 1)
+    lib.maille_gpu_cancel(None, 1)
+    lib.maille_gpu_batch_cancel(None, 1)
+    assert lib.maille_gpu_thermal_cancel(64, 1) == _lib.MAILLE_INVALID_INPUT
+    assert lib.maille_gpu_thermal_cancel(-1, 0) == _lib.MAILLE_INVALID_INPUT
+
+
+def test_no_alloc_entry_point_checks_its_arguments_without_device_work(lib):
+    # the pointers are never dereferenced: every check runs on the host before the device is used
+    f = lib.maille_gpu_bsr3_spmv_dot_noalloc
+    base = 1 << 20
+    assert f(0, 4, base, base, base, base, base + 8, base + 4096, None) == _lib.MAILLE_INVALID_INPUT
+    assert "overlap" in _lib.last_error()
+    assert f(0, 4, base, base, base, base, base + 96, base + 100, None) == _lib.MAILLE_INVALID_INPUT
+    assert f(0, -1, base, base, base, base, base + 96, base + 200, None) == _lib.MAILLE_INVALID_INPUT
+    assert f(0, 4, None, base, base, base, base + 96, base + 200, None) == _lib.MAILLE_INVALID_INPUT
+    assert f(64, 4, base, base, base, base, base + 96, base + 200, None) == _lib.MAILLE_INVALID_INPUT
 
 
 def test_missing_device_is_a_cuda_error_not_a_fallback(lib):
@@ -322,3 +341,39 @@ def test_c_harness_drives_the_abi_without_python(lib, tmp_path):
     out = subprocess.run([str(exe), "3"], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "elastic status 4" in out.stdout and "thermal status 4" in out.stdout
+
+
+def _header_text():
+    return open(os.path.join(ROOT, "include", "maille_gpu.h")).read()
+
+
+def test_rust_bindings_mirror_the_header():
+    """crates/maille-gpu-sys cannot be compiled here (no Rust toolchain): check its declarations
+    against include/maille_gpu.h as text. Every header function is declared with as many
+    parameters, and every problem/result struct lists the header's fields in the header's order."""
+    import re
+    hdr = re.sub(r"/\*.*?\*/", "", _header_text(), flags=re.S)
+    rs = open(os.path.join(ROOT, "crates", "maille-gpu-sys", "src", "lib.rs")).read()
+    rs = re.sub(r"//[^\n]*", "", rs)
+
+    def nparams(args):
+        args = args.strip().rstrip(",")  # rustfmt leaves a trailing comma on multi-line lists
+        return 0 if args in ("", "void") else args.count(",") + 1
+
+    hfun = {m.group(1): nparams(m.group(2)) for m in re.finditer(r"\b(maille_gpu_\w+)\s*\(([^)]*)\)\s*;", hdr)}
+    block = rs[rs.index('extern "C" {'):]
+    block = block[:block.index("\n}\n")]
+    rfun = {m.group(1): nparams(m.group(2)) for m in re.finditer(r"pub fn (maille_gpu_\w+)\s*\(([^)]*)\)", block)}
+    assert len(hfun) >= 30
+    assert hfun == rfun, set(hfun.items()) ^ set(rfun.items())
+
+    for m in re.finditer(r"typedef struct \{(.*?)\}\s*(\w+);", hdr, flags=re.S):
+        body, name = m.group(1), m.group(2)
+        fields = []
+        for decl in re.findall(r"[^;]+;", body):
+            parts = [d.strip() for d in decl.strip().rstrip(";").split(",")]
+            fields.append(parts[0].split()[-1].lstrip("*"))  # "const double* coords" -> coords
+            fields += [d.lstrip("*") for d in parts[1:]]       # "double ms_setup, ms_upload"
+        r = re.search(r"pub struct " + name + r" \{(.*?)\n\}", rs, flags=re.S)
+        assert r, name
+        assert re.findall(r"pub (\w+):", r.group(1)) == fields, name

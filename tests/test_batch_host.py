@@ -153,3 +153,42 @@ def test_sharding_is_consistent_across_ranks(tmp_path):
     assert views[0] == views[1]
     a, b = views[0]
     assert not set(a) & set(b) and sorted(a + b) == list(range(40))
+
+
+def _gather_worker(rank, world, port, out_dir):
+    """Fake per-rank results (no device): instance k's displacement is filled with k, so the
+    gathered batch shows where every instance landed."""
+    import pickle
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    costs = [float(c) for c in np.arange(1, 12)]
+    mine = batch.partition_lpt(costs, world)[rank]
+    part = batch.BatchField([np.full((3 * (k + 1), 2), float(k)) for k in mine],
+                            np.array([[k, k + 1] for k in mine], np.int32).reshape(-1, 2),
+                            np.array([[k * 1e-13, 0.0] for k in mine]).reshape(-1, 2),
+                            np.zeros(len(mine), np.int32))
+    whole = batch.gather_sharded(mine, part, len(costs), 2)
+    with open(os.path.join(out_dir, f"g{rank}.pkl"), "wb") as fh:
+        pickle.dump(whole, fh)
+    dist.destroy_process_group()
+
+
+def test_sharded_results_gather_on_rank_zero(tmp_path):
+    """The gather after a sharded solve puts every instance back in batch order on rank 0 and
+    returns None on the other ranks (world size 2, gloo)."""
+    import pickle
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    mp.spawn(_gather_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True)
+    whole = pickle.load(open(tmp_path / "g0.pkl", "rb"))
+    assert pickle.load(open(tmp_path / "g1.pkl", "rb")) is None
+    assert len(whole.displacements) == 11
+    for k in range(11):
+        assert whole.displacements[k].shape == (3 * (k + 1), 2) and (whole.displacements[k] == k).all()
+        assert list(whole.iterations[k]) == [k, k + 1]
+    assert whole.info["ranks"] == 2

@@ -224,3 +224,41 @@ def test_full_batched_workload(gpu, oracle_lib):
     for k in small + big:
         for j in range(8):
             assert rel(g.displacements[k][:, j], f.displacements[k][:, j]) < 1e-8
+
+
+def _sharded_worker(rank, world, port, out_dir):
+    """One rank of a sharded batch on device 0: its LPT share solved by its own BatchSolver (no
+    collective while solving), then the results gathered on rank 0 over gloo."""
+    import pickle
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    probs, loads = mg.batched_tet4(count=16, lo=3, hi=8, load_cases=4)
+    mine, part = batch.solve_sharded(probs, loads, rank, world, device=0, tol=1e-13)
+    whole = batch.gather_sharded(mine, part, len(probs), 4)
+    with open(os.path.join(out_dir, f"s{rank}.pkl"), "wb") as fh:
+        pickle.dump((mine, whole), fh)
+    dist.destroy_process_group()
+
+
+def test_sharded_batch_gathers_to_the_unsharded_result(gpu, tmp_path):
+    """Two ranks (two processes sharing device 0; their kernels never wait on one another) solve
+    disjoint LPT shares of a 16-instance batch; the gathered result equals the unsharded
+    BatchSolver's instance by instance."""
+    import pickle
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    mp.spawn(_sharded_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True)
+    (mine0, whole), (mine1, none) = [pickle.load(open(tmp_path / f"s{r}.pkl", "rb")) for r in range(2)]
+    assert none is None and mine0 and mine1 and not set(mine0) & set(mine1)
+    probs, loads = mg.batched_tet4(count=16, lo=3, hi=8, load_cases=4)
+    with batch.BatchSolver(probs, loads, tol=1e-13) as b:
+        ref = b.solve()
+    assert (whole.status == 0).all()
+    for k in range(16):
+        assert rel(whole.displacements[k], ref.displacements[k]) < 1e-10, k
+        assert whole.rel_residual[k].max() <= 1e-13

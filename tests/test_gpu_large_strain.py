@@ -121,3 +121,61 @@ def test_full_size_block_matches_the_oracle_summary(gpu):
     el = np.array(g["elements"])
     assert rel(gm[el], np.array(g["dJdmu"])) < 1e-6
     assert abs(gm.sum() - g["dJdmu_sum"]) < 1e-6 * abs(g["dJdmu_sum"])
+
+
+def test_newton_cuts_match_the_oracle(gpu, oracle_lib):
+    """A Newton limit too small for the whole increment forces advance's halvings
+    (model.rs:820-870): the GPU takes the same cuts as the oracle, with the same Newton counts
+    and end state."""
+    p, mu, tip = mg.large_strain_block(cells=(8, 2, 2))
+    for inc, nmax in ((2, 3), (10, 2)):
+        r = oracle_lib.large_strain_run(p, increments=inc, newton_max=nmax)
+        assert r["status"] == 0 and r["cuts"].sum() > 0
+        with mb.LargeStrainSolver(p, increments=inc, newton_max=nmax) as s:
+            h = s.run()
+        assert np.array_equal(h.cuts, r["cuts"]), (h.cuts, r["cuts"])
+        assert np.array_equal(h.newton, r["newton"])
+        assert h.newton_total == r["newton_total"]
+        assert rel(h.displacements, r["u_hist"]) < 1e-9
+        assert rel(h.reactions[-1], r["reactions"][-1]) < 1e-7
+
+
+def test_exhausted_cuts_report_not_converged(gpu, oracle_lib):
+    p, mu, tip = mg.large_strain_block(cells=(8, 2, 2))
+    r = oracle_lib.large_strain_run(p, increments=2, newton_max=2)
+    assert r["status"] == 2 and r["stop_cuts"] == 5
+    with mb.LargeStrainSolver(p, increments=2, newton_max=2) as s:
+        with pytest.raises(mb.MailleError) as e:
+            s.run()
+    assert e.value.kind == "IterativeNotConverged" or "converge" in str(e.value)
+    assert e.value.history.cuts[0] == 5
+
+
+def test_inner_pcg_cap_fails_without_a_cut(gpu, oracle_lib):
+    """An inner PCG at its cap is IterativeNotConverged, passed up with no halving, as in the
+    reference (model.rs:839-842) and the oracle."""
+    p, mu, tip = mg.large_strain_block(cells=(8, 2, 2))
+    r = oracle_lib.large_strain_run(p, increments=10, pcg_max=3)
+    assert r["status"] == 2 and r["stop_cuts"] == 0
+    with mb.LargeStrainSolver(p, increments=10, max_iter=3) as s:
+        with pytest.raises(mb.MailleError) as e:
+            s.run()
+    assert e.value.kind == "IterativeNotConverged"
+    assert e.value.history.cuts[0] == 0
+    assert e.value.history.newton_total == r["newton_total"] == 1
+    assert e.value.history.pcg_total == r["pcg_total"] == 3
+
+
+def test_cancel_flag_stops_the_run(gpu, oracle_lib):
+    p, mu, tip = mg.large_strain_block(cells=(8, 2, 2))
+    with mb.LargeStrainSolver(p, increments=4) as s:
+        s.cancel(True)
+        with pytest.raises(mb.MailleError) as e:
+            s.run()
+        assert e.value.kind == "Cancelled"
+        assert e.value.history.newton_total == 0 and not e.value.history.cuts.any()
+        s.cancel(False)
+        h = s.run()
+    r = oracle_lib.large_strain_run(p, increments=4)
+    assert np.array_equal(h.newton, r["newton"])
+    assert rel(h.reactions[-1], r["reactions"][-1]) < 1e-7

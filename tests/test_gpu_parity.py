@@ -200,6 +200,28 @@ def test_unconstrained_structure_is_reported(gpu):
     assert e.value.kind in ("Singular", "IterativeNotConverged")
 
 
+@pytest.mark.parametrize("precision", [MAILLE_FP64, MAILLE_MIXED])
+def test_shift_ladder_matches_the_oracle(gpu, oracle_lib, precision):
+    # Pcg::new (iterative.rs:14, 201-207): on a nearly incompressible Tet10 block, IC(0) fails the
+    # pivot test (iterative.rs:160-163) at shifts 0, 1e-3 and 1e-2 under RCM and succeeds at 0.1;
+    # the GPU (node RCM, block IC(0)) retries the same ladder and stops at the same shift
+    p = cases.nearly_incompressible((2, 2, 2), True, 0.49)
+    ref = oracle_lib.model_solve(p, solver=2, tol=1e-14)
+    assert ref["status"] == 0 and ref["shift"] == 0.1
+    f = solve(p, tol=1e-14, precision=precision, ordering=MAILLE_ORDER_RCM)
+    assert f.info["shift"] == ref["shift"]
+    assert rel(f.displacements, ref["u"]) < 1e-10
+    assert rel(f.von_mises, ref["von_mises"]) < 1e-10
+    # Tet4 4^3 at nu = 0.4999 needs 0.1 under every ordering, the multicolour default included
+    q = cases.nearly_incompressible((4, 4, 4), False, 0.4999)
+    refq = oracle_lib.model_solve(q, solver=2, tol=1e-14)
+    assert refq["shift"] == 0.1
+    for ordering in (MAILLE_ORDER_RCM, MAILLE_ORDER_MULTICOLOR):
+        g = solve(q, tol=1e-14, precision=precision, ordering=ordering)
+        assert g.info["shift"] == refq["shift"], (ordering, g.info["shift"])
+        assert rel(g.displacements, refq["u"]) < 1e-10
+
+
 def test_iteration_cap_reports_not_converged(gpu):
     with pytest.raises(mb.MailleError) as e:
         solve(mg.plain_tet4(8), max_iter=3)
@@ -217,6 +239,28 @@ def test_cancel_flag_stops_the_solve(gpu):
     h.cancel(False)
     assert h.solve().info["iterations"] > 0
     h.close()
+
+
+def test_device_buffer_solve_equals_the_host_solve(gpu):
+    # maille_gpu_solve_device: loads and displacements in device memory the caller owns; the same
+    # PCG as maille_gpu_solve, so the same displacements bit for bit
+    import torch
+    from maille_b200 import _lib
+    p = mg.plain_tet4(8)
+    with mb.SolverHandle(model_of(p)) as h:
+        ref = h.solve()
+        f2 = np.zeros(3 * p.n_nodes)
+        f2[3 * np.nonzero(np.abs(p.coords[:, 2] - 1) < 1e-12)[0]] = 0.01
+        ref2 = h.solve(f2)
+        dev = torch.device("cuda", 0)
+        t_f = torch.from_numpy(f2).to(dev)
+        t_u = torch.zeros(3 * p.n_nodes, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        assert h._L.maille_gpu_solve_device(h._h, None, t_u.data_ptr()) == 0, _lib.last_error()
+        assert np.array_equal(t_u.cpu().numpy(), ref.displacements)
+        assert h._L.maille_gpu_solve_device(h._h, t_f.data_ptr(), t_u.data_ptr()) == 0, _lib.last_error()
+        assert np.array_equal(t_u.cpu().numpy(), ref2.displacements)
+        assert h._L.maille_gpu_solve_device(h._h, None, None) == _lib.MAILLE_INVALID_INPUT
 
 
 def test_handle_solves_several_right_hand_sides(gpu):

@@ -212,3 +212,27 @@ def test_steady_known_answers_of_the_reference_through_the_gpu(gpu):
     m = math.sqrt(hf * 2.0 * (H + T) / (K * H * T))
     exact = 20.0 + 80.0 * np.cosh(m * (length - nodes[:, 0])) / math.cosh(m * length)
     assert np.max(np.abs(inc.temperatures - exact)) / 80.0 < 0.002
+
+
+def test_cancel_flag_stops_the_step(gpu, oracle_lib):
+    """The observer's Flow::Stop role (solve_step_with, model.rs:628, 1203-1218): a raised flag
+    stops the step before its first increment with MAILLE_CANCELLED; cleared, the same step runs
+    to the oracle's history."""
+    p = mg.thermal_cube(4, False, increments=3, time_period=0.03)
+    ref = oracle_lib.thermal_transient(p, solver=2)
+    th.cancel(True, device=0)
+    try:
+        s, out = th.solve_problem(p, f=ref["f"])
+    finally:
+        th.cancel(False, device=0)
+    assert s == 5, (s, _lib.last_error())
+    assert "Cancelled before increment 1" in _lib.last_error()
+    assert not out["iterations"].any()
+    s, out = th.solve_problem(p, f=ref["f"])
+    assert s == 0, _lib.last_error()
+    _check(out, ref)
+
+
+def test_cancel_rejects_a_device_out_of_range(gpu):
+    with pytest.raises(th.MailleError):
+        th.cancel(True, device=64)

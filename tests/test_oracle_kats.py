@@ -345,6 +345,21 @@ def test_iterative_static_solution_matches_the_direct_one(oracle_lib):
     assert gap(i["gauss"][..., 3], d["gauss"][..., 3]) < 1e-7
 
 
+@pytest.mark.parametrize("quadratic,cells,nu", [(True, 2, 0.49), (False, 4, 0.4999)])
+def test_shift_ladder_rescues_a_failed_factorisation(oracle_lib, quadratic, cells, nu):
+    # Pcg::new (iterative.rs:201-207): IC(0) of a nearly incompressible block meets a pivot
+    # <= 1e-12 a_ii (iterative.rs:160-163) at shifts 0, 1e-3 and 1e-2 and succeeds at 0.1; the
+    # shifted preconditioner still converges to the direct solution (tests/iterative.rs:68-83)
+    p = cases.nearly_incompressible((cells,) * 3, quadratic, nu)
+    d = oracle_lib.model_solve(p, solver=1)
+    i = oracle_lib.model_solve(p, solver=2, tol=1e-14)
+    assert i["status"] == 0 and i["shift"] == 0.1
+    assert np.abs(i["u"] - d["u"]).max() < 1e-8 * np.abs(d["u"]).max()
+    # the same matrix at nu = 0.3 factors without a shift
+    q = cases.nearly_incompressible((cells,) * 3, quadratic, 0.3)
+    assert oracle_lib.model_solve(q, solver=2)["shift"] == 0.0
+
+
 def test_iterative_solver_reports_an_unconstrained_structure(oracle_lib):
     # tests/iterative.rs:199-224
     r = oracle_lib.model_solve(cases.unconstrained(), solver=2)

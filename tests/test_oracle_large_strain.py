@@ -130,3 +130,28 @@ def test_adjoint_reaction_gradient_matches_central_differences(oracle_lib):
         mm[e] -= h
         fd = (J(mp) - J(mm)) / (2 * h)
         assert abs(fd - gm[e]) <= 1e-6 * abs(gm[e]), (e, fd, gm[e])
+
+
+def test_newton_failures_halve_the_increment(oracle_lib):
+    """advance (model.rs:820-870): a Newton that needs more than newton_max corrections is
+    retried on two halves of the interval, up to five halvings deep (MAX_CUTS, model.rs:1224)."""
+    p, mu, tip = mg.large_strain_block(cells=(8, 2, 2))
+    full = oracle_lib.large_strain_run(p, increments=2)
+    assert full["status"] == 0 and not full["cuts"].any()
+    cut = oracle_lib.large_strain_run(p, increments=2, newton_max=3)
+    assert cut["status"] == 0 and (cut["cuts"] == 1).all()
+    # the same end state at the Newton tolerance
+    assert np.linalg.norm(cut["u_hist"][-1] - full["u_hist"][-1]) < 1e-7 * np.linalg.norm(full["u_hist"][-1])
+    # every halving exhausted: NotConverged after MAX_CUTS = 5 cuts of the first increment
+    out = oracle_lib.large_strain_run(p, increments=2, newton_max=2)
+    assert out["status"] == 2 and out["stop_increment"] == 1 and out["stop_cuts"] == 5
+
+
+def test_inner_pcg_cap_ends_the_run_without_a_cut(oracle_lib):
+    """An inner solve at its iteration cap is IterativeNotConverged (error.rs:226-229), which
+    advance passes up unchanged: no halving (model.rs:839-842 cuts on NotConverged, Singular and
+    PlasticCollapse only)."""
+    p, mu, tip = mg.large_strain_block(cells=(8, 2, 2))
+    out = oracle_lib.large_strain_run(p, increments=10, pcg_max=3)
+    assert out["status"] == 2 and out["stop_increment"] == 1 and out["stop_cuts"] == 0
+    assert out["pcg_total"] == 3 and out["newton_total"] == 1
