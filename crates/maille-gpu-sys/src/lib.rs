@@ -72,7 +72,7 @@ pub struct MailleElasticResult {
     pub ms_post: f64,
     pub ms_download: f64,
     pub ms_element: f64,
-    pub ms_analysis_wait: f64,
+    pub ms_ordering: f64,
     pub ms_symbolic: f64,
     pub ms_buffers: f64,
 }
@@ -101,7 +101,7 @@ impl Default for MailleElasticResult {
             ms_post: 0.0,
             ms_download: 0.0,
             ms_element: 0.0,
-            ms_analysis_wait: 0.0,
+            ms_ordering: 0.0,
             ms_symbolic: 0.0,
             ms_buffers: 0.0,
         }

@@ -101,8 +101,9 @@ typedef struct {
     int64_t block_rows;         /* free nodes in the 3x3-block system */
     int64_t blocks;             /* 3x3 blocks of the full symmetric pattern */
     int32_t levels;             /* levels of the IC(0) sweeps */
-    double ms_setup;            /* host ordering (node graph, RCM / colouring), on a host thread that
-                                   runs while the device takes the inputs (create) */
+    double ms_setup;            /* host analysis on a thread that runs while the device takes the
+                                   inputs (create): node incidence and boundary lists, and with
+                                   MAILLE_HOST_ORDERING=1 the ordering too */
     double ms_upload;           /* host -> device copies of the inputs (create) */
     double ms_assembly;         /* scatter-reduce assembly of the element matrices (create,
                                    refactor) */
@@ -112,8 +113,9 @@ typedef struct {
     double ms_download;         /* device -> host copies */
     /* the rest of create, in order on the device stream (each 0 after solve-only calls): */
     double ms_element;          /* element integration (Ke of every element) */
-    double ms_analysis_wait;    /* host wall time create waited for the ordering thread after
-                                   the element integration was enqueued */
+    double ms_ordering;         /* wall time from the element integration to a known ordering:
+                                   the device ordering (node graph, RCM, greedy colouring) and
+                                   the join of the host thread */
     double ms_symbolic;         /* device pattern and scatter map (radix sorts), the host plan of
                                    the sliced layouts and their slot fills */
     double ms_buffers;          /* numeric buffers and the remaining index uploads */
@@ -432,7 +434,7 @@ typedef struct {
     int64_t free_nodes;
     int64_t nonzeros;         /* entries of the full symmetric pattern of the free nodes */
     int32_t levels;           /* levels of the IC(0) sweeps */
-    double ms_setup;          /* host ordering */
+    double ms_setup;          /* host node incidence (and the ordering with MAILLE_HOST_ORDERING=1) */
     double ms_upload;         /* host -> device copies and device analysis */
     double ms_assembly;       /* element matrices + assembly of the left and right matrices */
     double ms_factor;         /* IC(0) incl. shift retries */

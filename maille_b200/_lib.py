@@ -45,7 +45,7 @@ class ElasticResult(ctypes.Structure):
         ("ms_assembly", ctypes.c_double), ("ms_factor", ctypes.c_double),
         ("ms_solve", ctypes.c_double), ("ms_post", ctypes.c_double),
         ("ms_download", ctypes.c_double), ("ms_element", ctypes.c_double),
-        ("ms_analysis_wait", ctypes.c_double), ("ms_symbolic", ctypes.c_double),
+        ("ms_ordering", ctypes.c_double), ("ms_symbolic", ctypes.c_double),
         ("ms_buffers", ctypes.c_double),
     ]
 

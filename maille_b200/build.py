@@ -13,9 +13,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = [os.path.join(HERE, "csrc", f) for f in ("setup.cpp", "kernels.cu", "sparse.cu", "persist.cu", "solver.cu", "noalloc.cu",
-                                                        "batch_kernels.cu", "batch.cu", "large_strain.cu", "analysis.cu", "memory.cu", "thermal.cu")]
+                                                        "batch_kernels.cu", "batch.cu", "large_strain.cu", "analysis.cu", "memory.cu", "thermal.cu", "ordering.cu")]
 HDR = [os.path.join(HERE, "csrc", f) for f in ("common.hpp", "kernels.cuh", "sparse.cuh", "reduce.cuh",
-                                                         "cuda_host.hpp", "batch.cuh", "handle.hpp", "analysis.cuh", "tet.cuh")] + [
+                                                         "cuda_host.hpp", "batch.cuh", "handle.hpp", "analysis.cuh", "tet.cuh", "ordering.cuh")] + [
     os.path.join(HERE, "..", "include", "maille_gpu.h")]
 LIB = os.path.join(HERE, "libmaille_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

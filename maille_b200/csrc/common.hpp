@@ -139,6 +139,18 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
              const uint8_t* fixed, int ordering, Symbolic& s, Error& err, bool pattern = true,
              bool boundary_lists = true);
 
+// The part of analyse that does not depend on the ordering: the input checks, the node incidence,
+// the kept nodes (a node with a free DOF: kept in caller order, kept_of[v] its kept index or -1),
+// the free DOF count and, with boundary_lists, belem and bnodes.
+bool analyse_topology(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn, const uint8_t* fixed,
+                      Symbolic& s, std::vector<int32_t>& kept, std::vector<int32_t>& kept_of, Error& err,
+                      bool boundary_lists);
+
+// The ordering fields of s (nb, perm, inv, fixmask, levels, level_ptr) from an ordering computed
+// elsewhere: order[new row] = kept index with rows grouped by level, level[kept index].
+void apply_ordering(const std::vector<int32_t>& kept, const std::vector<int32_t>& order,
+                    const std::vector<int32_t>& level, const uint8_t* fixed, Symbolic& s);
+
 // Face pressure loads f_a -= p * integral(N_a n dS) added into f (assembly.rs:650-674 with the
 // tet branch of face_rule, assembly.rs:556-585). Host-side: part of the host program's assemble.
 bool face_pressure_loads(int64_t n_nodes, const double* coords, int npe, int64_t n_elems,

@@ -46,7 +46,7 @@ void parallel_for(int64_t n, F&& fn) {
 
 struct NodeGraph {
     std::vector<int64_t> off;   // [n + 1]
-    std::vector<int32_t> adj;   // neighbours, self excluded, element-encounter order
+    std::vector<int32_t> adj;   // neighbours, self excluded, by ascending kept index
     int64_t degree(int32_t v) const { return off[v + 1] - off[v]; }
     // asks the cache for vertex v's neighbour list ahead of its use: the searches below visit
     // vertices far from memory order, so each list would otherwise cost a DRAM miss
@@ -271,9 +271,9 @@ void boundary(Symbolic& s, int64_t n_nodes, int npe, int64_t n_elems, const int6
 
 }  // namespace
 
-bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
-             const uint8_t* fixed, int ordering, Symbolic& s, Error& err, bool pattern, bool boundary_lists) {
-    const double t0 = now_ms();
+bool analyse_topology(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn, const uint8_t* fixed,
+                      Symbolic& s, std::vector<int32_t>& kept, std::vector<int32_t>& kept_of, Error& err,
+                      bool boundary_lists) {
     if (npe != 4 && npe != 10) {
         err = {MAILLE_INVALID_INPUT, "nodes_per_elem must be 4 or 10"};
         return false;
@@ -292,20 +292,11 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
                                              " refers to unknown node " + std::to_string(conn[k])};
             return false;
         }
-    const bool stage_timing = std::getenv("MAILLE_SETUP_TIMING") != nullptr;
-    double t_stage = now_ms();
-    auto stage = [&](const char* name) {
-        if (!stage_timing) return;
-        const double t = now_ms();
-        std::fprintf(stderr, "maille setup %-12s %8.1f ms\n", name, t - t_stage);
-        t_stage = t;
-    };
     s = Symbolic{};
     s.n_nodes = n_nodes;
     s.n_elems = n_elems;
     s.npe = npe;
     const int32_t N = (int32_t)n_nodes;
-
     // node -> (element, local) incidence, sorted by element
     s.inc_ptr.assign(N + 1, 0);
     for (int64_t k = 0; k < n_elems * npe; ++k) s.inc_ptr[conn[k] + 1]++;
@@ -315,10 +306,9 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
         std::vector<int64_t> cur(s.inc_ptr.begin(), s.inc_ptr.end() - 1);
         for (int64_t k = 0; k < n_elems * npe; ++k) s.inc[cur[conn[k]]++] = (int32_t)k;
     }
-
-    stage("incidence");
-    // kept nodes (at least one free DOF) in original order; graph on them
-    std::vector<int32_t> kept_of(N, -1), kept;
+    // kept nodes (at least one free DOF) in original order
+    kept_of.assign(N, -1);
+    kept.clear();
     for (int32_t v = 0; v < N; ++v) {
         const bool all = fixed && fixed[3 * v] && fixed[3 * v + 1] && fixed[3 * v + 2];
         if (!all) {
@@ -327,16 +317,60 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
         }
     }
     for (int64_t g = 0; g < 3 * n_nodes; ++g) s.free_dofs += (fixed && fixed[g]) ? 0 : 1;
-    const int32_t nk = (int32_t)kept.size();
-    if (nk == 0) {
+    if (kept.empty()) {
         err = {MAILLE_INVALID_INPUT, "every DOF is fixed"};
         return false;
     }
+    if (boundary_lists) boundary(s, n_nodes, npe, n_elems, conn, fixed);
+    return true;
+}
+
+void apply_ordering(const std::vector<int32_t>& kept, const std::vector<int32_t>& order,
+                    const std::vector<int32_t>& level, const uint8_t* fixed, Symbolic& s) {
+    const int32_t nk = (int32_t)kept.size();
+    int32_t nl = 0;
+    for (int32_t k = 0; k < nk; ++k) nl = std::max(nl, level[k] + 1);
+    s.levels = nl;
+    s.level_ptr.assign(s.levels + 1, 0);
+    for (int32_t k = 0; k < nk; ++k) s.level_ptr[level[k] + 1]++;
+    for (int32_t l = 0; l < s.levels; ++l) s.level_ptr[l + 1] += s.level_ptr[l];
+    s.nb = nk;
+    s.perm.resize(nk);
+    s.inv.assign(s.n_nodes, -1);
+    s.fixmask.assign(nk, 0);
+    for (int32_t r = 0; r < nk; ++r) {
+        const int32_t v = kept[order[r]];
+        s.perm[r] = v;
+        s.inv[v] = r;
+        uint8_t m = 0;
+        for (int c = 0; c < 3; ++c)
+            if (fixed && fixed[3 * v + c]) m |= (uint8_t)(1u << c);
+        s.fixmask[r] = m;
+    }
+}
+
+bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
+             const uint8_t* fixed, int ordering, Symbolic& s, Error& err, bool pattern, bool boundary_lists) {
+    const double t0 = now_ms();
+    const bool stage_timing = std::getenv("MAILLE_SETUP_TIMING") != nullptr;
+    double t_stage = now_ms();
+    auto stage = [&](const char* name) {
+        if (!stage_timing) return;
+        const double t = now_ms();
+        std::fprintf(stderr, "maille setup %-12s %8.1f ms\n", name, t - t_stage);
+        t_stage = t;
+    };
+    std::vector<int32_t> kept_of, kept;
+    if (!analyse_topology(n_nodes, npe, n_elems, conn, fixed, s, kept, kept_of, err, boundary_lists && !pattern))
+        return false;
+    stage("topology");
+    const int32_t nk = (int32_t)kept.size();
     NodeGraph g;
     g.off.assign(nk + 1, 0);
     {
-        // neighbours of each kept node in element-encounter order, deduplicated with a per-thread
-        // mark array: a counting pass, then a filling pass
+        // neighbours of each kept node by ascending kept index (the order the device analysis
+        // produces by sorting keys): a counting pass, then a filling pass that sorts each list;
+        // duplicates are dropped with a per-thread mark array
         auto visit = [&](int32_t k, std::vector<int32_t>& mark, auto&& fn) {
             const int32_t v = kept[k];
             mark[k] = k;
@@ -366,6 +400,7 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
             for (int64_t k = k0; k < k1; ++k) {
                 int64_t q = g.off[k];
                 visit((int32_t)k, mark, [&](int32_t w) { g.adj[q++] = w; });
+                std::sort(g.adj.begin() + g.off[k], g.adj.begin() + g.off[k + 1]);
             }
         });
     }
@@ -373,71 +408,41 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
     stage("graph");
     // ordering over kept nodes: order[new] = kept index
     std::vector<int32_t> order = ordering == MAILLE_ORDER_MULTICOLOR_BFS ? reverse_bfs(g) : rcm(g);
-    std::vector<int32_t> colour;
+    std::vector<int32_t> level;
     if (ordering != MAILLE_ORDER_RCM) {
-        colour = greedy_colour(g, order);
-        // rows by colour, visit order inside a colour (a stable counting sort)
+        level = greedy_colour(g, order);
+        // rows by colour, visit order inside a colour (a stable counting sort). A row's lower
+        // neighbours are exactly its neighbours of smaller colours, and greedy colouring gives a
+        // node colour c only when its earlier-visited neighbours hold every colour below c, so the
+        // level of each row is its colour.
         int32_t nc = 0;
-        for (int32_t k = 0; k < nk; ++k) nc = std::max(nc, colour[k] + 1);
+        for (int32_t k = 0; k < nk; ++k) nc = std::max(nc, level[k] + 1);
         std::vector<int64_t> pos((size_t)nc + 1, 0);
-        for (int32_t k = 0; k < nk; ++k) pos[colour[k] + 1]++;
+        for (int32_t k = 0; k < nk; ++k) pos[level[k] + 1]++;
         for (int32_t c = 0; c < nc; ++c) pos[c + 1] += pos[c];
         std::vector<int32_t> by_colour(nk);
-        for (int32_t v : order) by_colour[pos[colour[v]]++] = v;
+        for (int32_t v : order) by_colour[pos[level[v]]++] = v;
         order.swap(by_colour);
-    }
-    stage("ordering");
-    if (!colour.empty()) {
-        // Multicolour order: a row's lower neighbours are exactly its neighbours of smaller
-        // colours, and greedy colouring gives a node colour c only when its earlier-visited
-        // neighbours hold every colour below c, so the level of each row is its colour and the
-        // rows are already grouped by level.
-        int32_t nc = 0;
-        for (int32_t k = 0; k < nk; ++k) nc = std::max(nc, colour[k] + 1);
-        s.levels = nc;
-        s.level_ptr.assign(s.levels + 1, 0);
-        for (int32_t k = 0; k < nk; ++k) s.level_ptr[colour[k] + 1]++;
-        for (int32_t l = 0; l < s.levels; ++l) s.level_ptr[l + 1] += s.level_ptr[l];
     } else {
         // levels of the lower-triangular dependency graph in that order, then group rows by
         // level (a topological renumbering leaves the IC(0) factor unchanged)
-        std::vector<int32_t> rank(nk), level(nk, 0);
+        std::vector<int32_t> rank(nk);
+        level.assign(nk, 0);
         for (int32_t r = 0; r < nk; ++r) rank[order[r]] = r;
-        int32_t maxl = 0;
         for (int32_t r = 0; r < nk; ++r) {
             const int32_t k = order[r];
             int32_t l = 0;
             for (int64_t p = g.off[k]; p < g.off[k + 1]; ++p)
                 if (rank[g.adj[p]] < r) l = std::max(l, level[g.adj[p]] + 1);
             level[k] = l;
-            maxl = std::max(maxl, l);
         }
-        s.levels = maxl + 1;
         std::stable_sort(order.begin(), order.end(),
                          [&](int32_t a, int32_t b) { return level[a] < level[b]; });
-        s.level_ptr.assign(s.levels + 1, 0);
-        for (int32_t k = 0; k < nk; ++k) s.level_ptr[level[k] + 1]++;
-        for (int32_t l = 0; l < s.levels; ++l) s.level_ptr[l + 1] += s.level_ptr[l];
     }
-    s.nb = nk;
-    s.perm.resize(nk);
-    s.inv.assign(N, -1);
-    s.fixmask.assign(nk, 0);
-    for (int32_t r = 0; r < nk; ++r) {
-        const int32_t v = kept[order[r]];
-        s.perm[r] = v;
-        s.inv[v] = r;
-        uint8_t m = 0;
-        for (int c = 0; c < 3; ++c)
-            if (fixed && fixed[3 * v + c]) m |= (uint8_t)(1u << c);
-        s.fixmask[r] = m;
-    }
-
+    stage("ordering");
+    apply_ordering(kept, order, level, fixed, s);
     stage("levels");
     if (!pattern) {
-        g = NodeGraph{};
-        if (boundary_lists) boundary(s, n_nodes, npe, n_elems, conn, fixed);
-        stage("boundary");
         s.ms = now_ms() - t0;
         return true;
     }

@@ -29,6 +29,7 @@
 #include "cuda_host.hpp"
 #include "handle.hpp"
 #include "kernels.cuh"
+#include "ordering.cuh"
 #include "sparse.cuh"
 
 using namespace maille;
@@ -336,15 +337,26 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
                                                    " refers to unknown node " + std::to_string(p->conn[k])});
     if (std::all_of(h->h_fixed.begin(), h->h_fixed.end(), [](uint8_t f) { return f != 0; }))
         return fail({MAILLE_INVALID_INPUT, "every DOF is fixed"});
-    // host: ordering, levels and boundary lists, on a thread of its own while the device takes
-    // the inputs and integrates the element matrices (neither depends on the ordering); the
-    // pattern and scatter map are built on the device afterwards (analysis.cu)
+    if (p->n_nodes >= (int64_t(1) << 30) || p->n_elems * node_pairs(p->nodes_per_elem) >= (int64_t(1) << 31))
+        return fail({MAILLE_INVALID_INPUT, "mesh too large for 32-bit node and element-pair indices"});
+    // The ordering runs on the device (ordering.cu) once the inputs are there; the host keeps the
+    // part that does not depend on it (node incidence, boundary lists) on a thread of its own
+    // meanwhile. MAILLE_HOST_ORDERING=1 orders on that host thread instead (the same permutation:
+    // the same algorithms on the same graph). The pattern and scatter map follow on the device
+    // (analysis.cu).
+    const bool host_ordering = env_int("MAILLE_HOST_ORDERING", 0) != 0;
+    const int ordering = p->ordering == MAILLE_ORDER_AUTO ? MAILLE_ORDER_MULTICOLOR : p->ordering;
+    std::vector<int32_t> kept, kept_of;
     const double t_setup0 = now_ms();
     double t_setup1 = t_setup0;
     bool analysed = false;
     std::thread analysis([&] {
-        analysed = analyse(p->n_nodes, p->nodes_per_elem, p->n_elems, p->conn, h->h_fixed.data(),
-                           p->ordering, h->sym, err, /*pattern=*/false);
+        if (host_ordering)
+            analysed = analyse(p->n_nodes, p->nodes_per_elem, p->n_elems, p->conn, h->h_fixed.data(), ordering,
+                               h->sym, err, /*pattern=*/false);
+        else
+            analysed = analyse_topology(p->n_nodes, p->nodes_per_elem, p->n_elems, p->conn, h->h_fixed.data(),
+                                        h->sym, kept, kept_of, err, /*boundary_lists=*/true);
         t_setup1 = now_ms();
     });
     struct Joiner {
@@ -397,9 +409,32 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         }
         CK(cudaEventRecord(h->ev[9], st));  // element matrices integrated
         const double t_wait0 = now_ms();
-        analysis.join();
+        if (host_ordering) {
+            analysis.join();
+            if (!analysed) return fail(err);
+        } else {
+            // kept nodes: at least one free DOF (the same rule as analyse_topology)
+            std::vector<int32_t> h_kept_of(p->n_nodes, -1), h_kept;
+            for (int64_t v = 0; v < p->n_nodes; ++v)
+                if (!(h->h_fixed[3 * v] && h->h_fixed[3 * v + 1] && h->h_fixed[3 * v + 2])) {
+                    h_kept_of[v] = (int32_t)h_kept.size();
+                    h_kept.push_back((int32_t)v);
+                }
+            int32_t* d_kept_of = dupload(h_kept_of.data(), h_kept_of.size(), st);
+            std::vector<int32_t> order, level;
+            try {
+                gpu_ordering(h->npe, h->n_elems, h->conn, d_kept_of, (int32_t)h_kept.size(), ordering, st, order,
+                             level);
+            } catch (...) {
+                dfree(d_kept_of);
+                throw;
+            }
+            dfree(d_kept_of);
+            analysis.join();
+            if (!analysed) return fail(err);
+            apply_ordering(h_kept, order, level, h->h_fixed.data(), h->sym);
+        }
         const double t_wait1 = now_ms();
-        if (!analysed) return fail(err);
         CK(cudaEventRecord(h->ev[10], st));  // symbolic: the ordering is known
         if (h->sym.levels >= kMaxLevels) return fail({MAILLE_INVALID_INPUT, "too many IC(0) levels"});
         // symbolic
@@ -511,7 +546,7 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
             res->ms_setup = t_setup1 - t_setup0;
             res->ms_upload = elapsed(h->ev[0], h->ev[8]);
             res->ms_element = elapsed(h->ev[8], h->ev[9]);
-            res->ms_analysis_wait = t_wait1 - t_wait0;
+            res->ms_ordering = t_wait1 - t_wait0;
             res->ms_symbolic = elapsed(h->ev[10], h->ev[11]);
             res->ms_buffers = elapsed(h->ev[11], h->ev[1]);
             res->ms_assembly = elapsed(h->ev[1], h->ev[2]);

@@ -42,6 +42,7 @@
 #include "common.hpp"
 #include "cuda_host.hpp"
 #include "kernels.cuh"
+#include "ordering.cuh"
 #include "reduce.cuh"
 #include "sparse.cuh"
 #include "tet.cuh"
@@ -1033,12 +1034,21 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
     bool analysed = false;
     const double t_setup0 = now_ms();
     double t_setup1 = t_setup0;
+    // AUTO: MULTICOLOR_BFS (on Tet10 40^3: 17 levels against 18 and 12 % fewer iterations than
+    // MULTICOLOR, the step 21 % shorter). The ordering runs on the device (ordering.cu) once the
+    // connectivity is there, the node incidence on this thread meanwhile; MAILLE_HOST_ORDERING=1
+    // orders on the thread instead (the same permutation).
+    const int ordering = p->ordering == MAILLE_ORDER_AUTO ? MAILLE_ORDER_MULTICOLOR_BFS : p->ordering;
+    const char* host_env = std::getenv("MAILLE_HOST_ORDERING");
+    const bool host_ordering = host_env && std::atoi(host_env) != 0;
+    std::vector<int32_t> kept, kept_of;
     std::thread analysis([&] {
-        // AUTO: MULTICOLOR_BFS (on Tet10 40^3: 17 levels against 18 and 12 % fewer iterations
-        // than MULTICOLOR, the step 21 % shorter)
-        const int ordering = p->ordering == MAILLE_ORDER_AUTO ? MAILLE_ORDER_MULTICOLOR_BFS : p->ordering;
-        analysed = analyse(n, npe, ne, p->conn, fixed3.data(), ordering, sym, err, /*pattern=*/false,
-                           /*boundary_lists=*/false);
+        if (host_ordering)
+            analysed = analyse(n, npe, ne, p->conn, fixed3.data(), ordering, sym, err, /*pattern=*/false,
+                               /*boundary_lists=*/false);
+        else
+            analysed = analyse_topology(n, npe, ne, p->conn, fixed3.data(), sym, kept, kept_of, err,
+                                        /*boundary_lists=*/false);
         t_setup1 = now_ms();
     });
     struct Joiner {
@@ -1126,8 +1136,23 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
             CK(cudaGetLastError());
         }
         CK(cudaEventRecord(ev[2], st));
-        analysis.join();
-        if (!analysed) return th_fail(err.status, err.message);
+        if (host_ordering) {
+            analysis.join();
+            if (!analysed) return th_fail(err.status, err.message);
+        } else {
+            std::vector<int32_t> h_kept_of(n, -1), h_kept;
+            for (int64_t v = 0; v < n; ++v)
+                if (!p->fixed[v]) {
+                    h_kept_of[v] = (int32_t)h_kept.size();
+                    h_kept.push_back((int32_t)v);
+                }
+            int32_t* d_kept_of = mem.take(dupload(h_kept_of.data(), h_kept_of.size(), st));
+            std::vector<int32_t> order, level;
+            gpu_ordering(npe, ne, conn, d_kept_of, (int32_t)h_kept.size(), ordering, st, order, level);
+            analysis.join();
+            if (!analysed) return th_fail(err.status, err.message);
+            apply_ordering(h_kept, order, level, fixed3.data(), sym);
+        }
         if (sym.levels >= kMaxLevels) return th_fail(MAILLE_INVALID_INPUT, "too many IC(0) levels");
         const int32_t nb = sym.nb;
         int32_t* perm = mem.take(dupload(sym.perm.data(), sym.perm.size(), st));

@@ -201,3 +201,19 @@ def nearly_incompressible(cells, quadratic: bool, nu: float, size=(1.0, 1.0, 1.0
     loads = np.zeros(3 * n)
     loads[3 * int(np.argmax(nodes[:, 2])) + 2] = -1.0
     return problem(nodes, conn, nu=nu, fixed=fixed, loads=loads, name=f"incompressible_{nu}")
+
+
+def two_blocks(cells=3, quadratic=False) -> Problem:
+    """Two separate clamped cubes in one model (two connected components of the node graph), a
+    pressure of 10 on the top of each: the orderings treat one component after the other."""
+    p = mg.clamped_cube((cells,) * 3, quadratic, E)
+    q = mg.clamped_cube((cells + 1, cells, cells), quadratic, 2 * E, size=(1.5, 1.0, 1.0))
+    n = p.coords.shape[0]
+    coords = np.concatenate([p.coords, q.coords + np.array([3.0, 0.0, 0.0])])
+    conn = np.concatenate([p.conn, q.conn + n])
+    return Problem(coords=coords, conn=conn, young=np.concatenate([p.young, q.young]),
+                   poisson=np.concatenate([p.poisson, q.poisson]), fixed=np.concatenate([p.fixed, q.fixed]),
+                   imposed=np.zeros(3 * coords.shape[0]), loads=np.zeros(3 * coords.shape[0]),
+                   p_elem=np.concatenate([p.p_elem, q.p_elem + p.conn.shape[0]]),
+                   p_face=np.concatenate([p.p_face, q.p_face]),
+                   p_value=np.concatenate([p.p_value, q.p_value]), name="two_blocks")

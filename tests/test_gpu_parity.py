@@ -141,6 +141,24 @@ def test_plain_tet4_config_tolerance_1e10_with_the_reference_ordering(gpu, oracl
     assert rel(f.von_mises, ref["von_mises"]) < 1e-10
 
 
+@pytest.mark.parametrize("ordering", [MAILLE_ORDER_MULTICOLOR, MAILLE_ORDER_RCM, MAILLE_ORDER_MULTICOLOR_BFS])
+def test_device_ordering_equals_the_host_ordering(gpu, monkeypatch, ordering):
+    # the ordering computed on the device (node graph, RCM / breadth-first search, greedy colouring
+    # or levels, ordering.cu) and by the host analysis (setup.cpp, MAILLE_HOST_ORDERING=1) are the
+    # same algorithms on the same graph: the same permutation, hence the same levels, iterations
+    # and displacements bit for bit; two_blocks has two connected components
+    p5 = mg.mixed_tet10(5)
+    p5.fixed[3 * 40 + 1] = 1  # a node with one fixed DOF stays in the system
+    for p in (mg.plain_tet4(8), p5, cases.two_blocks(3), cases.two_blocks(2, quadratic=True)):
+        monkeypatch.setenv("MAILLE_HOST_ORDERING", "1")
+        a = solve(p, ordering=ordering)
+        monkeypatch.delenv("MAILLE_HOST_ORDERING")
+        b = solve(p, ordering=ordering)
+        assert a.info["levels"] == b.info["levels"], (p.name, a.info["levels"], b.info["levels"])
+        assert a.info["iterations"] == b.info["iterations"], p.name
+        assert np.array_equal(a.displacements, b.displacements), p.name
+
+
 def test_rcm_ordering_takes_the_reference_iteration_count(gpu, oracle_lib):
     # node RCM + block IC(0) equals the reference's scalar RCM + scalar IC(0) on these meshes
     for p in (mg.plain_tet4(20), mg.mixed_tet10(12)):

@@ -236,3 +236,20 @@ def test_cancel_flag_stops_the_step(gpu, oracle_lib):
 def test_cancel_rejects_a_device_out_of_range(gpu):
     with pytest.raises(th.MailleError):
         th.cancel(True, device=64)
+
+
+@pytest.mark.parametrize("ordering", [_lib.MAILLE_ORDER_MULTICOLOR_BFS, _lib.MAILLE_ORDER_MULTICOLOR,
+                                      _lib.MAILLE_ORDER_RCM])
+def test_device_ordering_equals_the_host_ordering(gpu, monkeypatch, ordering):
+    """The thermal step orders its free nodes on the device by default; the host analysis
+    (MAILLE_HOST_ORDERING=1) runs the same algorithms on the same graph: the same levels,
+    iterations and temperatures bit for bit."""
+    p = mg.thermal_cube(5, True, increments=2, time_period=0.02)
+    monkeypatch.setenv("MAILLE_HOST_ORDERING", "1")
+    s1, a = th.solve_problem(p, fluxes=False, ordering=ordering)
+    monkeypatch.delenv("MAILLE_HOST_ORDERING")
+    s2, b = th.solve_problem(p, fluxes=False, ordering=ordering)
+    assert s1 == 0 and s2 == 0, _lib.last_error()
+    assert a["info"]["levels"] == b["info"]["levels"]
+    assert np.array_equal(a["iterations"], b["iterations"])
+    assert np.array_equal(a["temps"], b["temps"])
