@@ -108,6 +108,25 @@ impl Default for MailleElasticResult {
     }
 }
 
+// All-zero is a valid value of every field (null pointers, zero counts).
+impl Default for MailleThermalResult {
+    fn default() -> Self {
+        unsafe { std::mem::zeroed() }
+    }
+}
+
+impl Default for MailleLargeStrainResult {
+    fn default() -> Self {
+        unsafe { std::mem::zeroed() }
+    }
+}
+
+impl Default for MailleBatchResult {
+    fn default() -> Self {
+        unsafe { std::mem::zeroed() }
+    }
+}
+
 #[repr(C)]
 pub struct MailleGpuHandle {
     _private: [u8; 0],

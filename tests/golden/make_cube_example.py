@@ -4,7 +4,7 @@
 reference checks it against the analytic field ux = 0.01 x, uy = -0.25 * 0.01 y,
 uz = -0.25 * 0.01 z (crates/maille-cli/tests/examples.rs:669-681).
 
-Run here (it reads the reference tree): python tests/golden/make_cube_example.py /root/reference
+Run where the reference tree is checked out: python tests/golden/make_cube_example.py <reference root>
 """
 import json
 import os
@@ -93,4 +93,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_cube_example.py <root of the reference project>")
+    main(sys.argv[1])
