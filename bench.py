@@ -57,6 +57,8 @@ def parse():
                     help="profiling mode: time one form only (no reference solve, e2e or CPU); "
                          "prints a short line, not the benchmark line")
     ap.add_argument("--thermal-cells", type=int, default=40, help="cube side of the thermal section")
+    ap.add_argument("--ordering", choices=sorted(ORDERINGS), default="auto",
+                    help="ordering of the elastic solves (MailleOrdering)")
     return ap.parse_args()
 
 
@@ -127,10 +129,15 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(rows), "samples_under_load": len(sm)}
 
 
+ORDERINGS = {"auto": 0, "multicolor": 1, "rcm": 2, "multicolor_bfs": 3, "multicolor_iterated": 4}
+ORDERING = 0  # --ordering of the elastic solves (MailleOrdering)
+
+
 def solve_model(mb, p, precision, tol, device):
     m = mb.Model.from_arrays(p.coords, p.conn, p.young, p.poisson, p.fixed, p.imposed, p.loads,
                              (p.p_elem, p.p_face, p.p_value))
     m.with_solver(mb.SolverKind.ITERATIVE).with_tolerance(tol).with_precision(precision)
+    m.ordering = ORDERING
     return m
 
 
@@ -697,8 +704,10 @@ def run_only(args):
     h = mb.SolverHandle(solve_model(mb, p, prec, args.tol, 0), device=0)
     ms, info, launches = time_handle(torch, h, args.steps, args.warmup, L)
     h.close()
-    print(json.dumps({"only": args.only, "workload": f"tet10_{args.cells}^3", "ms_per_step": ms,
-                      "iterations": info["iterations"], "updates": info["outer_iterations"],
+    print(json.dumps({"only": args.only, "workload": f"tet10_{args.cells}^3", "ordering": args.ordering,
+                      "ms_per_step": ms, "iterations": info["iterations"], "updates": info["outer_iterations"],
+                      "levels": info["levels"], "ms_solve": info["ms_solve"],
+                      "ms_per_iteration": info["ms_solve"] / max(1, info["iterations"]),
                       "launches_per_step": launches}))
 
 
@@ -772,7 +781,7 @@ def run_ours(args):
     coords, conn, young, poisson = pin(p.coords), pin(p.conn.astype(np.int64)), pin(p.young), pin(p.poisson)
     fixed, imposed, floads = pin(p.fixed), pin(p.imposed), pin(f)
     prob, keep = problem_struct(coords, conn, young, poisson, fixed, imposed, floads, args.tol,
-                                10000, MAILLE_MIXED, 0, local)
+                                10000, MAILLE_MIXED, ORDERING, local)
     ng = 4
     outs = dict(u=pin(np.zeros(3 * p.n_nodes)), r=pin(np.zeros(3 * p.n_nodes)),
                 g=pin(np.zeros(p.n_elems * ng * 9)), vm=pin(np.zeros(p.n_elems * ng)))
@@ -840,7 +849,7 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic",
         "config": {"workload": f"tet10_{args.cells}^3_lognormal_mixed", "free_dofs": free,
                    "tol": args.tol, "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (matrices > 1 GB)", "ordering": "multicolor",
+                   "l2": "inputs larger than L2 (matrices > 1 GB)", "ordering": args.ordering,
                    "levels": info_m["levels"], "blocks": info_m["blocks"]},
         "accuracy": {"rel_err_vs_fp64": err_mixed, "target": 1e-8, "ok": err_mixed <= 1e-8},
         "mixed": {"iterations": info_m["iterations"], "outer": info_m["outer_iterations"],
@@ -872,7 +881,9 @@ def run_ours(args):
 
 
 def main():
+    global ORDERING
     args = parse()
+    ORDERING = ORDERINGS[args.ordering]
     if args.impl == "reference":
         run_reference(args)
     elif args.only:

@@ -25,6 +25,7 @@ pub const MAILLE_ORDER_AUTO: i32 = 0;
 pub const MAILLE_ORDER_MULTICOLOR: i32 = 1;
 pub const MAILLE_ORDER_RCM: i32 = 2;
 pub const MAILLE_ORDER_MULTICOLOR_BFS: i32 = 3;
+pub const MAILLE_ORDER_MULTICOLOR_ITERATED: i32 = 4;
 
 pub const MAILLE_BATCH_MAX_RHS: i32 = 8;
 pub const MAILLE_NOALLOC_MAX_BLOCK_ROWS: i64 = 1 << 26;

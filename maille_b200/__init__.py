@@ -7,7 +7,8 @@ this package is the host-side mirror of the reference's solve interface.
 from .model import (Bc, Dof, Field, ITERATIVE_FROM, Load, MailleError, Material, Mesh, Model,  # noqa: F401
                     Pressure, SolverHandle, SolverKind, face_pressure_loads)
 from ._lib import (MAILLE_FP64, MAILLE_MIXED, MAILLE_ORDER_AUTO, MAILLE_ORDER_MULTICOLOR,  # noqa: F401
-                   MAILLE_ORDER_MULTICOLOR_BFS, MAILLE_ORDER_RCM)
+                   MAILLE_ORDER_MULTICOLOR_BFS, MAILLE_ORDER_RCM,
+                   MAILLE_ORDER_MULTICOLOR_ITERATED)
 
 __version__ = "0.1.0"
 from .batch import BatchField, BatchSolver, partition_lpt, solve_sharded  # noqa: F401,E402

@@ -18,6 +18,7 @@ MAILLE_OK, MAILLE_SINGULAR, MAILLE_NOT_CONVERGED, MAILLE_INVALID_INPUT, MAILLE_C
 MAILLE_FP64, MAILLE_MIXED = 0, 1
 MAILLE_NOALLOC_MAX_BLOCK_ROWS = 1 << 26
 MAILLE_ORDER_AUTO, MAILLE_ORDER_MULTICOLOR, MAILLE_ORDER_RCM, MAILLE_ORDER_MULTICOLOR_BFS = 0, 1, 2, 3
+MAILLE_ORDER_MULTICOLOR_ITERATED = 4
 
 _d = ctypes.POINTER(ctypes.c_double)
 _i64 = ctypes.POINTER(ctypes.c_int64)

@@ -358,6 +358,20 @@ __global__ void k_order_keys(int32_t nk, const int32_t* __restrict__ value, cons
     }
 }
 
+// visit keys of an iterated-greedy pass: classes from the last to the first, RCM position inside
+__global__ void k_class_keys(int32_t nk, int32_t top, const int32_t* __restrict__ value,
+                             const int32_t* __restrict__ rpos, uint64_t* __restrict__ keys, int32_t* __restrict__ ids) {
+    GRID_STRIDE(v, (int64_t)nk) {
+        keys[v] = ((uint64_t)(uint32_t)(top - value[v]) << 32) | (uint64_t)(uint32_t)rpos[v];
+        ids[v] = (int32_t)v;
+    }
+}
+
+// rpos of a visit order given as an array of nodes
+__global__ void k_inverse(int32_t nk, const int32_t* __restrict__ visit, int32_t* __restrict__ rpos) {
+    GRID_STRIDE(q, (int64_t)nk) rpos[visit[q]] = (int32_t)q;
+}
+
 __global__ void k_fill_i32(int64_t n, int32_t v, int32_t* __restrict__ a) {
     GRID_STRIDE(i, n) a[i] = v;
 }
@@ -510,25 +524,44 @@ void gpu_ordering(int npe, int64_t n_elems, const int32_t* conn, const int32_t* 
     k_reverse<<<grid_of(nk), kT, 0, st>>>(nk, queue.p, visit.p, rpos.p);
     k_fill_i32<<<grid_of(nk), kT, 0, st>>>(nk, -1, value.p);
     CK(cudaMemsetAsync(fail.p, 0, sizeof(int32_t), st));
-    {
-        const int g = coop_grid((const void*)k_greedy, kT);
+    const int greedy_grid = coop_grid((const void*)k_greedy, kT);
+    auto colour = [&](const int32_t* vis, const int32_t* rp, int mode) {
         int32_t nk_ = nk;
         const int64_t* o = off.p;
         const int32_t* ad = adj;
-        const int32_t* vi = visit.p;
-        const int32_t* rp = rpos.p;
         int32_t* va = value.p;
-        int mode = ordering == MAILLE_ORDER_RCM ? 1 : 0;
         int32_t* fl = fail.p;
-        void* args[] = {&nk_, &o, &ad, &vi, &rp, &va, &mode, &fl};
+        void* args[] = {&nk_, &o, &ad, &vis, &rp, &va, &mode, &fl};
         counted();
-        CK(cudaLaunchCooperativeKernel((const void*)k_greedy, dim3(g), dim3(kT), args, 0, st));
+        CK(cudaLaunchCooperativeKernel((const void*)k_greedy, dim3(greedy_grid), dim3(kT), args, 0, st));
+    };
+    colour(visit.p, rpos.p, ordering == MAILLE_ORDER_RCM ? 1 : 0);
+    Buf<uint64_t> k0(nk), k1(nk);
+    Buf<int32_t> i0(nk), i1(nk);
+    if (ordering == MAILLE_ORDER_MULTICOLOR_ITERATED) {
+        // iterated greedy: recolour visiting the classes from the last to the first (RCM order
+        // inside a class), twice; the node dependencies now span at most the class count
+        Buf<int32_t> rpos2(nk);
+        for (int pass = 0; pass < 2; ++pass) {
+            std::vector<int32_t> hv(nk);
+            CK(cudaMemcpyAsync(hv.data(), value.p, (size_t)nk * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            const int32_t top = *std::max_element(hv.begin(), hv.end());
+            counted();
+            k_class_keys<<<grid_of(nk), kT, 0, st>>>(nk, top, value.p, rpos.p, k0.p, i0.p);
+            size_t b2 = 0;
+            CK(cub::DeviceRadixSort::SortPairs(nullptr, b2, k0.p, k1.p, i0.p, i1.p, nk, 0, 64, st));
+            temp.reserve(b2);
+            CK(cub::DeviceRadixSort::SortPairs(temp.p, b2, k0.p, k1.p, i0.p, i1.p, nk, 0, 64, st));
+            counted(3);
+            k_inverse<<<grid_of(nk), kT, 0, st>>>(nk, i1.p, rpos2.p);
+            k_fill_i32<<<grid_of(nk), kT, 0, st>>>(nk, -1, value.p);
+            colour(i1.p, rpos2.p, 0);
+        }
     }
     int32_t h_fail = 0;
     CK(cudaMemcpyAsync(&h_fail, fail.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    // rows by (colour or level, visit position)
-    Buf<uint64_t> k0(nk), k1(nk);
-    Buf<int32_t> i0(nk), i1(nk);
+    // rows by (colour or level, RCM visit position)
     counted();
     k_order_keys<<<grid_of(nk), kT, 0, st>>>(nk, value.p, rpos.p, k0.p, i0.p);
     size_t bytes = 0;

@@ -57,7 +57,8 @@ struct NodeGraph {
     }
     void prefetch_offset(int32_t v) const { __builtin_prefetch(off.data() + v); }
 };
-constexpr int64_t kAhead = 16;  // vertices ahead of the one being visited (lists; offsets 2x)
+constexpr int64_t kAhead = 16;
+constexpr int kIteratedPasses = 2;  // MULTICOLOR_ITERATED: two passes restore the classes' direction  // vertices ahead of the one being visited (lists; offsets 2x)
 
 // Vertex sets as bit sets: 64 KB for half a million vertices, so the random tests of a
 // breadth-first search stay in the core's cache.
@@ -249,6 +250,26 @@ std::vector<int32_t> greedy_colour(const NodeGraph& g, const std::vector<int32_t
     return colour;
 }
 
+// Iterated greedy (Culberson): recolours every node greedily, visiting the colour classes from
+// the last to the first and, inside a class, in the order of `order`; a pass never adds a colour
+// (the first node of each class finds every colour of the classes visited before it free or
+// takes at most the class count). Returns the colours after `passes` passes.
+std::vector<int32_t> iterated_greedy(const NodeGraph& g, const std::vector<int32_t>& order,
+                                     std::vector<int32_t> colour, int passes) {
+    const int32_t n = (int32_t)order.size();
+    std::vector<int32_t> pos(n);
+    for (int32_t i = 0; i < n; ++i) pos[order[i]] = i;
+    std::vector<int32_t> visit(n);
+    for (int k = 0; k < passes; ++k) {
+        std::iota(visit.begin(), visit.end(), 0);
+        std::sort(visit.begin(), visit.end(), [&](int32_t a, int32_t b) {
+            return colour[a] != colour[b] ? colour[a] > colour[b] : pos[a] < pos[b];
+        });
+        colour = greedy_colour(g, visit);
+    }
+    return colour;
+}
+
 // elements touching a fixed DOF, and the nodes with a fixed DOF they contain
 void boundary(Symbolic& s, int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
               const uint8_t* fixed) {
@@ -411,6 +432,7 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
     std::vector<int32_t> level;
     if (ordering != MAILLE_ORDER_RCM) {
         level = greedy_colour(g, order);
+        if (ordering == MAILLE_ORDER_MULTICOLOR_ITERATED) level = iterated_greedy(g, order, level, kIteratedPasses);
         // rows by colour, visit order inside a colour (a stable counting sort). A row's lower
         // neighbours are exactly its neighbours of smaller colours, and greedy colouring gives a
         // node colour c only when its earlier-visited neighbours hold every colour below c, so the

@@ -195,7 +195,7 @@ bool check_problem(const MailleElasticProblem* p, Error& err) {
         err = {MAILLE_INVALID_INPUT, "unknown precision"};
         return false;
     }
-    if (p->ordering < MAILLE_ORDER_AUTO || p->ordering > MAILLE_ORDER_MULTICOLOR_BFS) {
+    if (p->ordering < MAILLE_ORDER_AUTO || p->ordering > MAILLE_ORDER_MULTICOLOR_ITERATED) {
         err = {MAILLE_INVALID_INPUT, "unknown ordering"};
         return false;
     }

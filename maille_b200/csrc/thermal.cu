@@ -987,7 +987,7 @@ int32_t check_thermal(const MailleThermalProblem* p, std::string& why) {
     if (!(p->time_step > 0.0) || !std::isfinite(p->time_step)) return bad("time_step must be finite and > 0");
     if (!(p->theta >= 0.5 && p->theta <= 1.0)) return bad("theta must lie in [0.5, 1] (ThetaOutOfRange)");
     if (p->increments <= 0) return bad("increments must be > 0 (NoIncrements)");
-    if (p->ordering < MAILLE_ORDER_AUTO || p->ordering > MAILLE_ORDER_MULTICOLOR_BFS) return bad("unknown ordering");
+    if (p->ordering < MAILLE_ORDER_AUTO || p->ordering > MAILLE_ORDER_MULTICOLOR_ITERATED) return bad("unknown ordering");
     if (p->n_convection < 0 || (p->n_convection > 0 && (!p->conv_elem || !p->conv_face || !p->conv_film)))
         return bad("null convection arrays");
     const int64_t n = p->n_nodes;
@@ -1427,7 +1427,7 @@ int32_t maille_gpu_thermal_transient(const MailleThermalProblem* problem, Maille
 }
 
 int32_t maille_gpu_thermal_cancel(int32_t device, int32_t flag) {
-    set_last_error("");
+    // the last error stays: a caller reads the message of the step it just cancelled afterwards
     if (device < 0 || device >= kMaxCancelDevices) return th_fail(MAILLE_INVALID_INPUT, "device out of range");
     try {
         *(volatile int32_t*)(cancel_flags() + device) = flag ? 1 : 0;

@@ -104,7 +104,7 @@ def test_invalid_inputs_are_rejected_before_any_device_work(lib):
     assert status(fixed=np.ones_like(p0.fixed)) == _lib.MAILLE_INVALID_INPUT  # nothing free
     assert lib.maille_gpu_elastic_solve(None, None) == _lib.MAILLE_INVALID_INPUT
     p, keep = problem_struct(**good)
-    p.ordering = 4
+    p.ordering = 5
     assert _solve_status(lib, p) == _lib.MAILLE_INVALID_INPUT and "ordering" in _lib.last_error()
     # wrong element family
     p, keep = problem_struct(**good)

@@ -11,7 +11,8 @@ import cases
 import maille_b200 as mb
 from maille_b200 import meshgen as mg
 from maille_b200._lib import (MAILLE_FP64, MAILLE_MIXED, MAILLE_ORDER_MULTICOLOR,
-                              MAILLE_ORDER_MULTICOLOR_BFS, MAILLE_ORDER_RCM)
+                              MAILLE_ORDER_MULTICOLOR_BFS, MAILLE_ORDER_MULTICOLOR_ITERATED,
+                              MAILLE_ORDER_RCM)
 
 pytestmark = pytest.mark.gpu
 
@@ -141,7 +142,8 @@ def test_plain_tet4_config_tolerance_1e10_with_the_reference_ordering(gpu, oracl
     assert rel(f.von_mises, ref["von_mises"]) < 1e-10
 
 
-@pytest.mark.parametrize("ordering", [MAILLE_ORDER_MULTICOLOR, MAILLE_ORDER_RCM, MAILLE_ORDER_MULTICOLOR_BFS])
+@pytest.mark.parametrize("ordering", [MAILLE_ORDER_MULTICOLOR, MAILLE_ORDER_RCM, MAILLE_ORDER_MULTICOLOR_BFS,
+                                      MAILLE_ORDER_MULTICOLOR_ITERATED])
 def test_device_ordering_equals_the_host_ordering(gpu, monkeypatch, ordering):
     # the ordering computed on the device (node graph, RCM / breadth-first search, greedy colouring
     # or levels, ordering.cu) and by the host analysis (setup.cpp, MAILLE_HOST_ORDERING=1) are the
@@ -223,21 +225,25 @@ def test_shift_ladder_matches_the_oracle(gpu, oracle_lib, precision):
     # Pcg::new (iterative.rs:14, 201-207): on a nearly incompressible Tet10 block, IC(0) fails the
     # pivot test (iterative.rs:160-163) at shifts 0, 1e-3 and 1e-2 under RCM and succeeds at 0.1;
     # the GPU (node RCM, block IC(0)) retries the same ladder and stops at the same shift
+    # FP64 at 1e-14 within 1e-10 of the oracle; the mixed form (FP32 inner solves) to its own
+    # contract, 1e-8 relative displacement error, at 1e-10: on these ill-conditioned matrices its
+    # attainable residual stays above 1e-14
+    tol, err = (1e-14, 1e-10) if precision == MAILLE_FP64 else (1e-10, 1e-8)
     p = cases.nearly_incompressible((2, 2, 2), True, 0.49)
     ref = oracle_lib.model_solve(p, solver=2, tol=1e-14)
     assert ref["status"] == 0 and ref["shift"] == 0.1
-    f = solve(p, tol=1e-14, precision=precision, ordering=MAILLE_ORDER_RCM)
+    f = solve(p, tol=tol, precision=precision, ordering=MAILLE_ORDER_RCM)
     assert f.info["shift"] == ref["shift"]
-    assert rel(f.displacements, ref["u"]) < 1e-10
-    assert rel(f.von_mises, ref["von_mises"]) < 1e-10
+    assert rel(f.displacements, ref["u"]) < err
+    assert rel(f.von_mises, ref["von_mises"]) < err
     # Tet4 4^3 at nu = 0.4999 needs 0.1 under every ordering, the multicolour default included
     q = cases.nearly_incompressible((4, 4, 4), False, 0.4999)
     refq = oracle_lib.model_solve(q, solver=2, tol=1e-14)
     assert refq["shift"] == 0.1
     for ordering in (MAILLE_ORDER_RCM, MAILLE_ORDER_MULTICOLOR):
-        g = solve(q, tol=1e-14, precision=precision, ordering=ordering)
+        g = solve(q, tol=tol, precision=precision, ordering=ordering)
         assert g.info["shift"] == refq["shift"], (ordering, g.info["shift"])
-        assert rel(g.displacements, refq["u"]) < 1e-10
+        assert rel(g.displacements, refq["u"]) < err
 
 
 def test_iteration_cap_reports_not_converged(gpu):

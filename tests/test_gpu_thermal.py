@@ -239,7 +239,7 @@ def test_cancel_rejects_a_device_out_of_range(gpu):
 
 
 @pytest.mark.parametrize("ordering", [_lib.MAILLE_ORDER_MULTICOLOR_BFS, _lib.MAILLE_ORDER_MULTICOLOR,
-                                      _lib.MAILLE_ORDER_RCM])
+                                      _lib.MAILLE_ORDER_RCM, _lib.MAILLE_ORDER_MULTICOLOR_ITERATED])
 def test_device_ordering_equals_the_host_ordering(gpu, monkeypatch, ordering):
     """The thermal step orders its free nodes on the device by default; the host analysis
     (MAILLE_HOST_ORDERING=1) runs the same algorithms on the same graph: the same levels,
