@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--no-thermal", action="store_true", help="skip the transient thermal section")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--adjoint-cells", type=int, default=48)
-    ap.add_argument("--only", choices=["mixed", "plain", "thermal", "batched", "large_strain"], default=None,
+    ap.add_argument("--only", choices=["mixed", "plain", "thermal", "thermal_mixed", "batched", "large_strain"],
+                    default=None,
                     help="profiling mode: time one form only (no reference solve, e2e or CPU); "
                          "prints a short line, not the benchmark line")
     ap.add_argument("--thermal-cells", type=int, default=40, help="cube side of the thermal section")
@@ -435,16 +436,19 @@ def large_strain_section(mb, mg, steps, device):
     return out
 
 
-def thermal_section(mg, steps, device, hbm, cells=40):
+def thermal_section(mg, steps, device, hbm, cells=40, ordering=0):
     """Transient heat conduction on the Tet10 unit cube 40^3 (531 441 nodes, 524 880 free): 10
     backward-Euler increments of (C/dt + K) T_{n+1} = C/dt T_n + F, each solved by IC(0)-PCG from
-    zero to 1e-12 (Model::solve_step). One step = the whole transient through the C ABI from host
-    buffers (element matrices, assembly, IC(0), the increments, the history copied back); the
+    zero to 1e-12 (Model::solve_step), in FP64 and in the mixed form (FP32 matrices and vectors,
+    FP64 reliable updates). One step = the whole transient through the C ABI from host buffers
+    (ordering, element matrices, assembly, IC(0), the increments, the history copied back); the
     device time of the increments comes from the library's CUDA events. Roofline of the
-    persistent scalar PCG: algorithmic bytes per iteration = the left matrix (values + columns)
-    once for the SpMV and its strict triangles once per sweep, plus about 16 vector passes."""
+    persistent scalar PCG: algorithmic bytes per iteration = the left matrix (values + int32
+    columns) once for the SpMV and its strict triangles once per sweep, plus 16 vector passes
+    (values of the storage precision)."""
     import torch
     from maille_b200 import thermal as th
+    from maille_b200._lib import MAILLE_FP64, MAILLE_MIXED
     p = mg.thermal_cube(cells, True, increments=10, time_period=0.1)
     f = p.loads + th.thermal_loads(p.coords, p.conn, list(zip(p.s_elem, p.s_value)),
                                    list(zip(p.c_elem, p.c_face, p.c_film, p.c_sink)))
@@ -456,38 +460,49 @@ def thermal_section(mg, steps, device, hbm, cells=40):
     res = dict(temps=pin(np.zeros((p.increments + 1, p.n_nodes))),
                reactions=pin(np.zeros((p.increments + 1, p.n_nodes))), fluxes=None,
                iterations=np.zeros(p.increments, np.int32))
-    s, out = th.solve_problem(p, f=f, fluxes=False, device=device, out=res)  # warm-up
-    if s != 0:
-        return {"workload": p.name, "error": s}
-    walls, dev = [], []
-    for _ in range(max(1, steps)):
-        t0 = time.perf_counter()
-        s, out = th.solve_problem(p, f=f, fluxes=False, device=device, out=res)
-        walls.append((time.perf_counter() - t0) * 1e3)
-        dev.append(out["info"]["ms_steps"])
-    info = out["info"]
-    nnz, nb, its = info["nonzeros"], info["free_nodes"], info["iterations_total"]
-    bytes_it = 12 * nnz + 12 * (nnz - nb) + 16 * 8 * nb
-    ms_it = statistics.median(dev) / its
-    wall = statistics.median(walls)
-    res = {"workload": p.name + "_10inc", "free_nodes": nb, "nonzeros": nnz, "levels": info["levels"],
-           "increments": p.increments, "iterations_total": its, "iterations": out["iterations"].tolist(),
-           "e2e_ms": wall, "e2e_value": nb * p.increments / (wall / 1e3), "unit": "DOF*increments/s",
-           "ms_increments_device": statistics.median(dev), "ms_setup": info["ms_setup"],
-           "ms_upload": info["ms_upload"], "ms_assembly": info["ms_assembly"], "ms_factor": info["ms_factor"],
-           "ms_download": info["ms_download"],
-           "roofline": {"bound": "hbm", "kernel": "k_heat_pcg (persistent FP64 scalar IC(0)-PCG)",
-                        "bytes_per_iteration": bytes_it, "ms_per_iteration": ms_it,
-                        "achieved": bytes_it / (ms_it * 1e6), "peak": hbm,
-                        "frac": bytes_it / (ms_it * 1e6) / hbm}}
     path = os.path.join(ROOT, "tests", "golden", "thermal_40_oracle_summary.json")
-    if cells == 40 and os.path.exists(path):
-        g = json.load(open(path))
-        sample = out["temps"][-1][::g["t_final_stride"]]
-        res["max_abs_err_vs_oracle_final_T"] = float(np.max(np.abs(sample - np.array(g["t_final_sample"]))))
-        res["oracle_iterations_total"] = g["total_iterations"]
-        res["oracle_cpu_note"] = "the CPU oracle's time for this workload is in the reference arm's line"
-    return res
+    golden = json.load(open(path)) if cells == 40 and os.path.exists(path) else None
+    forms = {}
+    for name, prec in (("fp64", MAILLE_FP64), ("mixed", MAILLE_MIXED)):
+        kw = dict(f=f, fluxes=False, device=device, out=res, precision=prec, ordering=ordering)
+        s, out = th.solve_problem(p, **kw)  # warm-up
+        if s != 0:
+            forms[name] = {"error": s}
+            continue
+        walls, dev = [], []
+        for _ in range(max(1, steps)):
+            t0 = time.perf_counter()
+            s, out = th.solve_problem(p, **kw)
+            walls.append((time.perf_counter() - t0) * 1e3)
+            dev.append(out["info"]["ms_steps"])
+        info = out["info"]
+        nnz, nb, its = info["nonzeros"], info["free_nodes"], info["iterations_total"]
+        vb = 8 if prec == MAILLE_FP64 else 4
+        bytes_it = (vb + 4) * nnz + (vb + 4) * (nnz - nb) + 16 * vb * nb
+        ms_it = statistics.median(dev) / its
+        wall = statistics.median(walls)
+        r = {"iterations_total": its, "iterations": out["iterations"].tolist(), "levels": info["levels"],
+             "e2e_ms": wall, "e2e_value": nb * p.increments / (wall / 1e3), "unit": "DOF*increments/s",
+             "ms_increments_device": statistics.median(dev), "ms_setup": info["ms_setup"],
+             "ms_upload": info["ms_upload"], "ms_assembly": info["ms_assembly"], "ms_factor": info["ms_factor"],
+             "ms_download": info["ms_download"], "max_rel_residual": info["max_rel_residual"],
+             "roofline": {"bound": "hbm", "kernel": f"k_heat_pcg<{'double' if vb == 8 else 'float'}> "
+                                                   "(persistent scalar IC(0)-PCG)",
+                          "bytes_per_iteration": bytes_it, "ms_per_iteration": ms_it,
+                          "achieved": bytes_it / (ms_it * 1e6), "peak": hbm,
+                          "frac": bytes_it / (ms_it * 1e6) / hbm}}
+        if golden:
+            sample = out["temps"][-1][::golden["t_final_stride"]]
+            r["max_abs_err_vs_oracle_final_T"] = float(np.max(np.abs(sample - np.array(golden["t_final_sample"]))))
+        forms[name] = r
+    out = {"workload": p.name + "_10inc", "free_nodes": info["free_nodes"], "nonzeros": info["nonzeros"],
+           "increments": p.increments, **forms}
+    if golden:
+        out["oracle_iterations_total"] = golden["total_iterations"]
+        out["oracle_cpu_note"] = "the CPU oracle's time for this workload is in the reference arm's line"
+    if "fp64" in forms and "mixed" in forms and "e2e_ms" in forms["mixed"]:
+        out["speedup_mixed_vs_fp64_device"] = forms["fp64"]["ms_increments_device"] / forms["mixed"]["ms_increments_device"]
+    return out
 
 
 def spmv_roofline(torch, h, L, precision, blocks, nb, reps=50):
@@ -677,18 +692,20 @@ def run_only(args):
         print(json.dumps({"only": "large_strain", "newton_total": int(h.newton_total),
                           "pcg_total": int(h.pcg_total), "ms_total": h.ms_total}))
         return
-    if args.only == "thermal":
+    if args.only in ("thermal", "thermal_mixed"):
         from maille_b200 import meshgen as mg, thermal as th
         p = mg.thermal_cube(args.thermal_cells, True, increments=10, time_period=0.1)
         f = p.loads + th.thermal_loads(p.coords, p.conn, list(zip(p.s_elem, p.s_value)),
                                        list(zip(p.c_elem, p.c_face, p.c_film, p.c_sink)))
+        prec = 1 if args.only == "thermal_mixed" else 0
         for _ in range(args.warmup + args.steps):
-            s, out = th.solve_problem(p, f=f, fluxes=False)
+            s, out = th.solve_problem(p, f=f, fluxes=False, precision=prec, ordering=ORDERING)
             if s != 0:
                 raise SystemExit(f"thermal transient failed with status {s}")
-        print(json.dumps({"only": "thermal", "workload": p.name + "_10inc",
-                          "iterations": out["info"]["iterations_total"],
-                          "ms_increments_device": out["info"]["ms_steps"]}))
+        print(json.dumps({"only": args.only, "workload": p.name + "_10inc", "ordering": args.ordering,
+                          "iterations": out["info"]["iterations_total"], "levels": out["info"]["levels"],
+                          "ms_increments_device": out["info"]["ms_steps"],
+                          "ms_per_iteration": out["info"]["ms_steps"] / out["info"]["iterations_total"]}))
         return
     import torch
     import maille_b200 as mb

@@ -248,6 +248,7 @@ pub struct MailleThermalProblem {
     pub max_iter: i32,
     pub ordering: i32,
     pub device: i32,
+    pub precision: i32,
 }
 
 #[repr(C)]

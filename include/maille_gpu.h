@@ -422,6 +422,10 @@ typedef struct {
     int32_t max_iter;             /* per increment; <= 0 selects 10000 */
     int32_t ordering;             /* MailleOrdering of the free nodes */
     int32_t device;
+    int32_t precision;            /* MaillePrecision: MAILLE_FP64 (0), or MAILLE_MIXED: FP32 matrices
+                                     and vectors in the PCG with FP64 reliable updates (x accumulated
+                                     in FP64, true residual b - A x against the FP64 matrix, the
+                                     stopping test on it) */
 } MailleThermalProblem;
 
 typedef struct {

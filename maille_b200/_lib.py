@@ -103,7 +103,7 @@ class ThermalProblem(ctypes.Structure):
         ("conv_elem", _i64), ("conv_face", _i32), ("conv_film", _d), ("initial", _d),
         ("time_step", ctypes.c_double), ("theta", ctypes.c_double), ("increments", ctypes.c_int32),
         ("rel_tol", ctypes.c_double), ("max_iter", ctypes.c_int32), ("ordering", ctypes.c_int32),
-        ("device", ctypes.c_int32),
+        ("device", ctypes.c_int32), ("precision", ctypes.c_int32),
     ]
 
 

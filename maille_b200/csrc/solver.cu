@@ -531,6 +531,10 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         // 4 reduction slots for every block of the persistent grid and of the norm kernels
         // (grids capped at 8 and 4 blocks per SM)
         h->persist_grid = std::min(h->persist_grid, 8 * device_sms());
+        // MAILLE_PERSIST_BLOCKS_PER_SM: fewer co-resident blocks than the occupancy allows (a
+        // tuning and measurement knob: the sweeps' time against the warps in flight)
+        if (const int bps = env_int("MAILLE_PERSIST_BLOCKS_PER_SM", 0); bps > 0)
+            h->persist_grid = std::min(h->persist_grid, bps * device_sms());
         h->partials = dalloc<double>((size_t)4 * 8 * device_sms());
         if (env_int("MAILLE_PHASE_TIMING", 0)) {
             h->timing = dalloc<unsigned long long>(8);

@@ -33,6 +33,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -385,6 +386,10 @@ __global__ void k_gather_slots(int64_t n, const int32_t* __restrict__ src, const
         out[t] = s >= 0 ? M[s] : 0.0;
     }
 }
+__global__ void k_to_float(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        b[t] = (float)a[t];
+}
 __global__ void k_gather_diag(int32_t nb, const int64_t* __restrict__ diag, const double* __restrict__ M,
                               double* __restrict__ D) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (int64_t)gridDim.x * blockDim.x)
@@ -483,14 +488,19 @@ __global__ void __launch_bounds__(kT) k_heat_rhs(SellDev R, const double* __rest
     }
 }
 
-// Arguments of the persistent PCG kernel of one increment.
+// Arguments of the persistent PCG kernel of one increment. T is the storage type of the
+// iteration's matrices and vectors: double in the plain form, float in the mixed form, whose
+// solution accumulates in x64 (FP64) through reliable updates against the FP64 matrix A64v.
+template <typename T>
 struct HeatPcg {
+    using Rec = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
     int32_t nb;
     SellDev A, Lo, Up;
     const int32_t* bwd_slice;        // [Up.nslices] slices of Up in backward sweep order
-    const double *Av, *Lv, *Uv, *D, *b;
-    double *x, *r, *p, *ap;          // [nb + 1]
-    double2 *yrec, *zrec;            // [nb + 1] sweep records (value, tag); entry nb always ready
+    const T *Av, *Lv, *Uv, *D;
+    const double* b;                 // FP64 right-hand side
+    T *x, *r, *p, *ap;               // [nb + 1]; the plain form's x is the solution
+    Rec *yrec, *zrec;                // [nb + 1] sweep records (value, tag); entry nb always ready
     double* partials;                // [4 * grid]
     int32_t* timeout;                // set when a record wait ran out
     unsigned long long epoch0;       // the launch's sweeps tag their records epoch0 + 1, + 2, ...
@@ -502,6 +512,11 @@ struct HeatPcg {
     int32_t* iterations;
     double* rel;
     unsigned long long* timing;      // optional [4] ns per phase (block 0): spmv, update, sweeps, p
+    // mixed form only
+    const double* A64v;              // A's FP64 values in the same sliced layout
+    double* x64;                     // [nb + 1] the FP64 solution
+    double* r64;                     // [nb + 1] the true residual b - A x64
+    double delta;                    // reliable update when ||r|| fell below delta x its last true value
 };
 
 __device__ __forceinline__ unsigned long long heat_clock() {
@@ -511,6 +526,9 @@ __device__ __forceinline__ unsigned long long heat_clock() {
 }
 
 constexpr unsigned int kSpinLimit = 1u << 22;  // re-reads of a record before a wait gives up
+// mixed form: a reliable update whenever the FP32 residual fell below this fraction of the last
+// true one (the elastic mixed form's threshold)
+constexpr double kHeatDelta = 0.3;
 
 __device__ __forceinline__ void heat_publish(double v, double* partials, int slot, double* sh) {
     const double t = block_sum(v, sh);
@@ -523,11 +541,17 @@ __device__ __forceinline__ double heat_total(const double* partials, int slot) {
     return warp_sum(t);
 }
 
-// A sweep record: the row's value and the epoch of the sweep that wrote it, in one 16-byte
-// access (the tag never arrives without its value).
+// A sweep record: the row's value and the epoch of the sweep that wrote it, in one access (16
+// bytes in FP64, the tag a 64-bit word; 8 bytes in FP32, the tag the low 32 bits of the epoch), so
+// the tag never arrives without its value.
 __device__ __forceinline__ double2 ld_rec(const double2* q) {
     double2 v;
     asm volatile("ld.relaxed.gpu.global.v2.f64 {%0,%1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(q) : "memory");
+    return v;
+}
+__device__ __forceinline__ float2 ld_rec(const float2* q) {
+    float2 v;
+    asm volatile("ld.relaxed.gpu.global.v2.f32 {%0,%1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(q) : "memory");
     return v;
 }
 __device__ __forceinline__ void st_rec(double2* q, double v, unsigned long long tag) {
@@ -535,14 +559,23 @@ __device__ __forceinline__ void st_rec(double2* q, double v, unsigned long long 
                  "d"(__longlong_as_double((long long)tag))
                  : "memory");
 }
+__device__ __forceinline__ void st_rec(float2* q, float v, unsigned long long tag) {
+    asm volatile("st.relaxed.gpu.global.v2.f32 [%0], {%1,%2};" ::"l"(q), "f"(v),
+                 "f"(__uint_as_float((unsigned int)tag))
+                 : "memory");
+}
 __device__ __forceinline__ bool rec_ready(double2 v, unsigned long long epoch) {
     return (unsigned long long)__double_as_longlong(v.y) >= epoch;
+}
+__device__ __forceinline__ bool rec_ready(float2 v, unsigned long long epoch) {
+    return __float_as_uint(v.y) >= (unsigned int)epoch;
 }
 
 // Waits (bounded) until the four records v (read once already from rec at the columns c) carry
 // `epoch`, re-reading the stale ones; false when the wait gave up (its own limit, or another
 // warp's timeout flag).
-__device__ __forceinline__ bool await4(const double2* rec, int4 c, unsigned long long epoch, double2 v[4],
+template <typename R>
+__device__ __forceinline__ bool await4(const R* rec, int4 c, unsigned long long epoch, R v[4],
                                        const int32_t* timeout) {
     for (unsigned int k = 0; k < kSpinLimit; ++k) {
         const bool r0 = rec_ready(v[0], epoch), r1 = rec_ready(v[1], epoch), r2 = rec_ready(v[2], epoch),
@@ -556,8 +589,8 @@ __device__ __forceinline__ bool await4(const double2* rec, int4 c, unsigned long
     }
     return false;
 }
-__device__ __forceinline__ bool await1(const double2* rec, unsigned long long epoch, double2& v,
-                                       const int32_t* timeout) {
+template <typename R>
+__device__ __forceinline__ bool await1(const R* rec, unsigned long long epoch, R& v, const int32_t* timeout) {
     v = ld_rec(rec);
     for (unsigned int k = 0; k < kSpinLimit; ++k) {
         if (rec_ready(v, epoch)) return true;
@@ -567,42 +600,91 @@ __device__ __forceinline__ bool await1(const double2* rec, unsigned long long ep
     return false;
 }
 
+// 4 consecutive slot values of a lane (16-byte aligned)
+__device__ __forceinline__ void lane4(const double* p, double v[4]) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p + 2));
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void lane4(const float* p, float v[4]) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+
 // Lane share of sum over a slice row's slots of vals * rec[col].value once every record carries
 // `epoch`, reduced over the row's lanes. The columns and values of step g + 1 are requested
 // before the records of step g are awaited, so a step costs about one round trip.
-__device__ __forceinline__ double slice_row_dot_rec(const SellDev& S, const double* __restrict__ vals, int64_t g0,
-                                                    int64_t g1, const double2* rec, unsigned long long epoch,
-                                                    int lane, const int32_t* timeout, bool& ok) {
-    double acc = 0.0;
+template <typename T, typename R>
+__device__ __forceinline__ T slice_row_dot_rec(const SellDev& S, const T* __restrict__ vals, int64_t g0, int64_t g1,
+                                               const R* rec, unsigned long long epoch, int lane,
+                                               const int32_t* timeout, bool& ok) {
+    T acc = 0;
     int4 cn = make_int4(0, 0, 0, 0);
-    double2 an = make_double2(0.0, 0.0), bn = an;
+    T vn[4] = {0, 0, 0, 0};
     if (g0 < g1) {
         const int64_t base = g0 * kStepSlots + 4 * lane;
         cn = __ldg(reinterpret_cast<const int4*>(S.col + base));
-        an = __ldg(reinterpret_cast<const double2*>(vals + base));
-        bn = __ldg(reinterpret_cast<const double2*>(vals + base + 2));
+        lane4(vals + base, vn);
     }
     for (int64_t g = g0; g < g1; ++g) {
         const int4 c = cn;
-        const double2 v01 = an, v23 = bn;
+        const T v0 = vn[0], v1 = vn[1], v2 = vn[2], v3 = vn[3];
         if (g + 1 < g1) {
             const int64_t base = (g + 1) * kStepSlots + 4 * lane;
             cn = __ldg(reinterpret_cast<const int4*>(S.col + base));
-            an = __ldg(reinterpret_cast<const double2*>(vals + base));
-            bn = __ldg(reinterpret_cast<const double2*>(vals + base + 2));
+            lane4(vals + base, vn);
         }
-        double2 v[4];
+        R v[4];
         v[0] = ld_rec(rec + c.x);
         v[1] = ld_rec(rec + c.y);
         v[2] = ld_rec(rec + c.z);
         v[3] = ld_rec(rec + c.w);
         if (!await4(rec, c, epoch, v, timeout)) ok = false;
-        acc += v01.x * v[0].x;
-        acc += v01.y * v[1].x;
-        acc += v23.x * v[2].x;
-        acc += v23.y * v[3].x;
+        acc += v0 * (T)v[0].x;
+        acc += v1 * (T)v[1].x;
+        acc += v2 * (T)v[2].x;
+        acc += v3 * (T)v[3].x;
     }
     __syncwarp();
+    for (int o = S.lpr >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    return acc;
+}
+
+// Lane share of a sliced SpMV row (vals * x[col]) in the precision of x, reduced over the row's
+// lanes; kChunk steps' columns and values are requested before their gathers.
+template <int kChunk, typename M, typename X>
+__device__ __forceinline__ X slice_row_dot_t(const SellDev& S, const M* __restrict__ vals, int32_t sl, const X* x,
+                                             int lane) {
+    X acc = 0;
+    const int64_t g0 = S.off[sl], g1 = S.off[sl + 1];
+    for (int64_t g = g0; g < g1; g += kChunk) {
+        int4 c[kChunk];
+        M v[kChunk][4];
+#pragma unroll
+        for (int j = 0; j < kChunk; ++j)
+            if (g + j < g1) {
+                const int64_t base = (g + j) * kStepSlots + 4 * lane;
+                c[j] = __ldg(reinterpret_cast<const int4*>(S.col + base));
+                lane4(vals + base, v[j]);
+            }
+        X xv[kChunk][4];
+#pragma unroll
+        for (int j = 0; j < kChunk; ++j)
+            if (g + j < g1) {
+                xv[j][0] = __ldcg(x + c[j].x);
+                xv[j][1] = __ldcg(x + c[j].y);
+                xv[j][2] = __ldcg(x + c[j].z);
+                xv[j][3] = __ldcg(x + c[j].w);
+            }
+#pragma unroll
+        for (int j = 0; j < kChunk; ++j)
+            if (g + j < g1) {
+                acc += (X)v[j][0] * xv[j][0];
+                acc += (X)v[j][1] * xv[j][1];
+                acc += (X)v[j][2] * xv[j][2];
+                acc += (X)v[j][3] * xv[j][3];
+            }
+    }
     for (int o = S.lpr >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     return acc;
 }
@@ -616,7 +698,8 @@ __device__ __forceinline__ double slice_row_dot_rec(const SellDev& S, const doub
 // slice can always proceed. The next slice's metadata is fetched while this one is swept (going
 // further, with the next slice's columns and values too, measured slower: more registers on the
 // critical path). Returns this thread's share of r . z.
-__device__ __forceinline__ double heat_sweeps(const HeatPcg& a, unsigned long long epoch) {
+template <typename T>
+__device__ __forceinline__ double heat_sweeps(const HeatPcg<T>& a, unsigned long long epoch) {
     const int lane = threadIdx.x & 31;
     const int32_t w0 = (int32_t)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int32_t nw = (int32_t)(((int64_t)gridDim.x * blockDim.x) >> 5);
@@ -626,11 +709,11 @@ __device__ __forceinline__ double heat_sweeps(const HeatPcg& a, unsigned long lo
     // the slice's place in L or U, its step range and this lane's row
     auto meta = [&](int32_t k, int32_t& sl, int64_t& g0, int64_t& g1, int32_t& row) {
         const bool fwd = k < nl;
-        const SellDev& T = fwd ? a.Lo : a.Up;
+        const SellDev& S = fwd ? a.Lo : a.Up;
         sl = fwd ? k : __ldg(a.bwd_slice + (k - nl));
-        g0 = __ldg(T.off + sl);
-        g1 = __ldg(T.off + sl + 1);
-        row = __ldg(T.rowid + (int64_t)sl * (32 / T.lpr) + lane / T.lpr);
+        g0 = __ldg(S.off + sl);
+        g1 = __ldg(S.off + sl + 1);
+        row = __ldg(S.rowid + (int64_t)sl * (32 / S.lpr) + lane / S.lpr);
     };
     int32_t sl_n = 0, row_n = -1;
     int64_t g0_n = 0, g1_n = 0;
@@ -640,22 +723,22 @@ __device__ __forceinline__ double heat_sweeps(const HeatPcg& a, unsigned long lo
         const int64_t g0 = g0_n, g1 = g1_n;
         if (k + nw < nt) meta(k + nw, sl_n, g0_n, g1_n, row_n);
         const bool fwd = k < nl;
-        const SellDev& T = fwd ? a.Lo : a.Up;
-        const bool owner = (lane % T.lpr) == 0 && row >= 0;
+        const SellDev& S = fwd ? a.Lo : a.Up;
+        const bool owner = (lane % S.lpr) == 0 && row >= 0;
         // the row's own operands, requested before the wait
-        const double d = owner ? __ldg(a.D + row) : 1.0;
-        const double ri = owner ? __ldcg(a.r + row) : 0.0;
-        const double acc = slice_row_dot_rec(T, fwd ? a.Lv : a.Uv, g0, g1, fwd ? a.yrec : a.zrec, epoch, lane,
-                                             a.timeout, ok);
+        const T d = owner ? __ldg(a.D + row) : (T)1;
+        const T ri = owner ? __ldcg(a.r + row) : (T)0;
+        const T acc = slice_row_dot_rec<T>(S, fwd ? a.Lv : a.Uv, g0, g1, fwd ? a.yrec : a.zrec, epoch, lane,
+                                           a.timeout, ok);
         if (owner) {
             if (fwd) {
                 st_rec(a.yrec + row, (ri - acc) / d, epoch);
             } else {
-                double2 y;
+                typename HeatPcg<T>::Rec y;
                 if (!await1(a.yrec + row, epoch, y, a.timeout)) ok = false;
-                const double z = (y.x - acc) / d;
+                const T z = (y.x - acc) / d;
                 st_rec(a.zrec + row, z, epoch);
-                rz += ri * z;
+                rz += (double)ri * (double)z;
             }
         }
     }
@@ -675,12 +758,29 @@ __global__ void k_heat_gate(const volatile int32_t* cancel, const int32_t* prev_
     *status = g;
 }
 
+// two consecutive entries of a vector (16-byte FP64 / 8-byte FP32 access) and back
+__device__ __forceinline__ double2 ld2(const double* p) { return __ldcg(reinterpret_cast<const double2*>(p)); }
+__device__ __forceinline__ double2 ld2(const float* p) {
+    const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
+    return make_double2(v.x, v.y);
+}
+__device__ __forceinline__ void st2(double* p, double a, double b) {
+    *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+__device__ __forceinline__ void st2(float* p, double a, double b) {
+    *reinterpret_cast<float2*>(p) = make_float2((float)a, (float)b);
+}
+
 // IC(0)-PCG of one increment from x = 0 (Pcg::solve, iterative.rs:210-248) in one cooperative
 // launch: SpMV, the x / r update, the dataflow preconditioner and the p update, each closed by a
 // grid barrier (four per iteration). (Fusing the two updates into the SpMV and the sweeps saves
 // two barriers but puts more loads on the sweeps' critical path; measured slower.) Every
 // reduction is per-block partials in fixed slots summed in slot order by every block.
-__global__ void __launch_bounds__(kT, 2) k_heat_pcg(HeatPcg a) {
+// MIXED: FP32 matrices and vectors with FP64 scalars and reductions; whenever the FP32 residual
+// fell by delta since the last true one (and at the end), x64 += x, x = 0 and r64 = b - A64 x64 in
+// FP64, r = r64 (the reliable update of the elastic mixed form); the stopping test is on r64.
+template <typename T, bool MIXED>
+__global__ void __launch_bounds__(kT, 2) k_heat_pcg(HeatPcg<T> a) {
     __shared__ double sh[kT / 32];
     cg::grid_group grid = cg::this_grid();
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
@@ -706,13 +806,18 @@ __global__ void __launch_bounds__(kT, 2) k_heat_pcg(HeatPcg a) {
     double loc = 0.0;
     for (int64_t i = tid; i < a.nb; i += nth) {
         const double bi = a.b[i];
-        a.x[i] = 0.0;
-        a.r[i] = bi;
+        a.x[i] = (T)0;
+        a.r[i] = (T)bi;
+        if constexpr (MIXED) {
+            a.x64[i] = 0.0;
+            a.r64[i] = bi;
+        }
         loc += bi * bi;
     }
     heat_publish(loc, a.partials, 3, sh);
     grid.sync();
     const double bnorm = sqrt(heat_total(a.partials, 3));
+    double maxr = bnorm;  // mixed: the last true residual norm
     int32_t status = 0, it = 0;
     double rel = 0.0;
     if (bnorm > 0.0) {
@@ -720,7 +825,7 @@ __global__ void __launch_bounds__(kT, 2) k_heat_pcg(HeatPcg a) {
         heat_publish(loc, a.partials, 2, sh);
         grid.sync();
         double rz = heat_total(a.partials, 2);
-        for (int64_t i = tid; i < a.nb; i += nth) a.p[i] = __ldcg(&a.zrec[i].x);
+        for (int64_t i = tid; i < a.nb; i += nth) a.p[i] = (T)__ldcg(&a.zrec[i].x);
         grid.sync();
         for (;;) {
             if (__ldcg(a.timeout)) {
@@ -733,11 +838,11 @@ __global__ void __launch_bounds__(kT, 2) k_heat_pcg(HeatPcg a) {
                 const int32_t w0 = (int32_t)(tid >> 5), nw = (int32_t)(nth >> 5);
                 loc = 0.0;
                 for (int32_t sl = w0; sl < a.A.nslices; sl += nw) {
-                    const double acc = slice_row_dot<2>(a.A, a.Av, sl, a.p, lane);
+                    const T acc = slice_row_dot_t<2>(a.A, a.Av, sl, (const T*)a.p, lane);
                     const int32_t row = a.A.rowid[(int64_t)sl * S + r];
                     if (q == 0 && row >= 0) {
                         a.ap[row] = acc;
-                        loc += __ldcg(a.p + row) * acc;
+                        loc += (double)__ldcg(a.p + row) * (double)acc;
                     }
                 }
             }
@@ -752,36 +857,71 @@ __global__ void __launch_bounds__(kT, 2) k_heat_pcg(HeatPcg a) {
             }
             const double alpha = rz / pap;
             loc = 0.0;
-            // two entries per thread and pass (16-byte accesses; the vectors hold nb + 1 >= 2 entries
-            // and start 256-byte aligned); an odd last entry is taken alone
+            // two entries per thread and pass (16-byte FP64 / 8-byte FP32 accesses; the vectors
+            // hold nb + 1 >= 2 entries and start 256-byte aligned); an odd last entry alone
             for (int64_t i2 = tid; 2 * i2 < a.nb; i2 += nth) {
                 const int64_t i = 2 * i2;
                 if (i + 1 < a.nb) {
-                    const double2 xv = __ldcg(reinterpret_cast<const double2*>(a.x + i));
-                    const double2 pv = __ldcg(reinterpret_cast<const double2*>(a.p + i));
-                    const double2 rv = __ldcg(reinterpret_cast<const double2*>(a.r + i));
-                    const double2 av = __ldcg(reinterpret_cast<const double2*>(a.ap + i));
-                    const double r0 = rv.x - alpha * av.x, r1 = rv.y - alpha * av.y;
-                    *reinterpret_cast<double2*>(a.x + i) = make_double2(xv.x + alpha * pv.x, xv.y + alpha * pv.y);
-                    *reinterpret_cast<double2*>(a.r + i) = make_double2(r0, r1);
-                    loc += r0 * r0;
-                    loc += r1 * r1;
+                    const double2 xv = ld2(a.x + i), pv = ld2(a.p + i), rv = ld2(a.r + i), av = ld2(a.ap + i);
+                    const T r0 = (T)(rv.x - alpha * av.x), r1 = (T)(rv.y - alpha * av.y);
+                    st2(a.x + i, xv.x + alpha * pv.x, xv.y + alpha * pv.y);
+                    st2(a.r + i, r0, r1);
+                    loc += (double)r0 * (double)r0;
+                    loc += (double)r1 * (double)r1;
                 } else {
-                    a.x[i] = __ldcg(a.x + i) + alpha * __ldcg(a.p + i);
-                    const double ri = __ldcg(a.r + i) - alpha * __ldcg(a.ap + i);
+                    a.x[i] = (T)((double)__ldcg(a.x + i) + alpha * (double)__ldcg(a.p + i));
+                    const T ri = (T)((double)__ldcg(a.r + i) - alpha * (double)__ldcg(a.ap + i));
                     a.r[i] = ri;
-                    loc += ri * ri;
+                    loc += (double)ri * (double)ri;
                 }
             }
             heat_publish(loc, a.partials, 1, sh);
             grid.sync();
             mark(1);
-            const double rn = sqrt(heat_total(a.partials, 1));
-            rel = rn / bnorm;
-            if (rn <= a.tol * bnorm) break;
-            if (it >= a.max_iter) {
-                status = 2;
-                break;
+            double rn = sqrt(heat_total(a.partials, 1));
+            if constexpr (MIXED) {
+                if (rn <= a.tol * bnorm || rn < a.delta * maxr || it >= a.max_iter) {
+                    // reliable update: fold x into x64, the true residual against the FP64 matrix
+                    for (int64_t i = tid; i < a.nb; i += nth) {
+                        a.x64[i] += (double)__ldcg(a.x + i);
+                        a.x[i] = (T)0;
+                    }
+                    grid.sync();
+                    {
+                        const int lane = threadIdx.x & 31, S = 32 / a.A.lpr, r = lane / a.A.lpr,
+                                  q = lane % a.A.lpr;
+                        const int32_t w0 = (int32_t)(tid >> 5), nw = (int32_t)(nth >> 5);
+                        loc = 0.0;
+                        for (int32_t sl = w0; sl < a.A.nslices; sl += nw) {
+                            const double acc = slice_row_dot_t<2>(a.A, a.A64v, sl, (const double*)a.x64, lane);
+                            const int32_t row = a.A.rowid[(int64_t)sl * S + r];
+                            if (q == 0 && row >= 0) {
+                                const double rv = a.b[row] - acc;
+                                a.r64[row] = rv;
+                                loc += rv * rv;
+                            }
+                        }
+                    }
+                    heat_publish(loc, a.partials, 1, sh);
+                    grid.sync();
+                    rn = sqrt(heat_total(a.partials, 1));
+                    maxr = rn;
+                    rel = rn / bnorm;
+                    if (rn <= a.tol * bnorm) break;
+                    if (it >= a.max_iter) {
+                        status = 2;
+                        break;
+                    }
+                    for (int64_t i = tid; i < a.nb; i += nth) a.r[i] = (T)__ldcg(a.r64 + i);
+                    grid.sync();
+                }
+            } else {
+                rel = rn / bnorm;
+                if (rn <= a.tol * bnorm) break;
+                if (it >= a.max_iter) {
+                    status = 2;
+                    break;
+                }
             }
             loc = heat_sweeps(a, ++epoch);
             heat_publish(loc, a.partials, 2, sh);
@@ -797,11 +937,11 @@ __global__ void __launch_bounds__(kT, 2) k_heat_pcg(HeatPcg a) {
             for (int64_t i2 = tid; 2 * i2 < a.nb; i2 += nth) {
                 const int64_t i = 2 * i2;
                 if (i + 1 < a.nb) {
-                    const double z0 = __ldcg(&a.zrec[i].x), z1 = __ldcg(&a.zrec[i + 1].x);
-                    const double2 pv = __ldcg(reinterpret_cast<const double2*>(a.p + i));
-                    *reinterpret_cast<double2*>(a.p + i) = make_double2(z0 + beta * pv.x, z1 + beta * pv.y);
+                    const double z0 = (double)__ldcg(&a.zrec[i].x), z1 = (double)__ldcg(&a.zrec[i + 1].x);
+                    const double2 pv = ld2(a.p + i);
+                    st2(a.p + i, z0 + beta * pv.x, z1 + beta * pv.y);
                 } else {
-                    a.p[i] = __ldcg(&a.zrec[i].x) + beta * __ldcg(a.p + i);
+                    a.p[i] = (T)((double)__ldcg(&a.zrec[i].x) + beta * (double)__ldcg(a.p + i));
                 }
             }
             grid.sync();
@@ -988,6 +1128,13 @@ int32_t check_thermal(const MailleThermalProblem* p, std::string& why) {
     if (!(p->theta >= 0.5 && p->theta <= 1.0)) return bad("theta must lie in [0.5, 1] (ThetaOutOfRange)");
     if (p->increments <= 0) return bad("increments must be > 0 (NoIncrements)");
     if (p->ordering < MAILLE_ORDER_AUTO || p->ordering > MAILLE_ORDER_MULTICOLOR_ITERATED) return bad("unknown ordering");
+    if (p->precision != MAILLE_FP64 && p->precision != MAILLE_MIXED) return bad("unknown precision");
+    if (p->precision == MAILLE_MIXED) {
+        // FP32 sweep records carry 32-bit tags: every sweep of the step needs its own
+        const int64_t span = (int64_t)(p->max_iter > 0 ? p->max_iter : kDefaultMaxIter) + 2;
+        if ((int64_t)p->increments * span >= (int64_t)UINT32_MAX - 1)
+            return bad("too many increments x iterations for the mixed form's 32-bit sweep tags");
+    }
     if (p->n_convection < 0 || (p->n_convection > 0 && (!p->conv_elem || !p->conv_face || !p->conv_film)))
         return bad("null convection arrays");
     const int64_t n = p->n_nodes;
@@ -1247,9 +1394,14 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
         for (double* q : {x, r, pp, ap, b}) CK(cudaMemsetAsync(q, 0, nv * sizeof(double), st));
         // sweep records (value, tag): tags start at 0, below every epoch; the dummy node's tag is
         // the largest, so padding slots never wait
-        double2* yrec = mem.take(dalloc<double2>(nv));
-        double2* zrec = mem.take(dalloc<double2>(nv));
-        {
+        const bool mixed = p->precision == MAILLE_MIXED;
+        double2* yrec = nullptr;
+        double2* zrec = nullptr;
+        float2* yrec32 = nullptr;
+        float2* zrec32 = nullptr;
+        if (!mixed) {
+            yrec = mem.take(dalloc<double2>(nv));
+            zrec = mem.take(dalloc<double2>(nv));
             static thread_local double2 h_dummy;
             const long long all_ones = -1LL;
             h_dummy.x = 0.0;
@@ -1258,6 +1410,40 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
                 CK(cudaMemsetAsync(q, 0, nv * sizeof(double2), st));
                 CK(cudaMemcpyAsync(q + nb, &h_dummy, sizeof(double2), cudaMemcpyHostToDevice, st));
             }
+        } else {
+            yrec32 = mem.take(dalloc<float2>(nv));
+            zrec32 = mem.take(dalloc<float2>(nv));
+            static thread_local float2 h_dummy32;
+            const unsigned int ones = 0xFFFFFFFFu;
+            h_dummy32.x = 0.0f;
+            std::memcpy(&h_dummy32.y, &ones, sizeof(float));
+            for (float2* q : {yrec32, zrec32}) {
+                CK(cudaMemsetAsync(q, 0, nv * sizeof(float2), st));
+                CK(cudaMemcpyAsync(q + nb, &h_dummy32, sizeof(float2), cudaMemcpyHostToDevice, st));
+            }
+        }
+        // mixed form: FP32 copies of the operands and the FP32 work vectors (x64 = x, r64 the
+        // true residual)
+        float *Av32 = nullptr, *Lv32 = nullptr, *Uv32 = nullptr, *D32 = nullptr, *x32 = nullptr, *r32 = nullptr,
+              *p32 = nullptr, *ap32 = nullptr;
+        double* r64 = nullptr;
+        if (mixed) {
+            Av32 = mem.take(dalloc<float>((size_t)slots(sk)));
+            Lv32 = mem.take(dalloc<float>((size_t)slots(sl)));
+            Uv32 = mem.take(dalloc<float>((size_t)slots(su)));
+            D32 = mem.take(dalloc<float>((size_t)nb + 1));
+            for (int k = 0; k < 4; ++k) counted();
+            k_to_float<<<grid_of(slots(sk)), kT, 0, st>>>(slots(sk), Av, Av32);
+            k_to_float<<<grid_of(slots(sl)), kT, 0, st>>>(slots(sl), Lv, Lv32);
+            k_to_float<<<grid_of(slots(su)), kT, 0, st>>>(slots(su), Uv, Uv32);
+            k_to_float<<<grid_of(nv), kT, 0, st>>>(nv, D, D32);
+            CK(cudaGetLastError());
+            for (float** q : {&x32, &r32, &p32, &ap32}) {
+                *q = mem.take(dalloc<float>(nv));
+                CK(cudaMemsetAsync(*q, 0, nv * sizeof(float), st));
+            }
+            r64 = mem.take(dalloc<double>(nv));
+            CK(cudaMemsetAsync(r64, 0, nv * sizeof(double), st));
         }
         // U's slices in backward sweep order (levels descending)
         std::vector<int32_t> bwd;
@@ -1293,9 +1479,9 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
         // two blocks of 256 threads per SM (128 registers a thread): 3 or 4 blocks (80 or 64
         // registers) spill and make every grid barrier dearer, measured slower in every phase
         int per_sm = 0, sms = 0, dev = p->device;
-        void* pcg_fn = (void*)k_heat_pcg;
+        void* pcg_fn = mixed ? (void*)k_heat_pcg<float, true> : (void*)k_heat_pcg<double, false>;
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_heat_pcg, kT, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_fn, kT, 0));
         const int grid = sms * std::min(per_sm, 2);
         if (grid <= 0) return th_fail(MAILLE_CUDA_ERROR, "the PCG kernel does not fit on the device");
         double* partials = mem.take(dalloc<double>((size_t)4 * grid));
@@ -1315,12 +1501,24 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
             k_heat_rhs<<<grid_of((int64_t)sk.h.nslices() * 32), kT, 0, st>>>(sk.dev(), Rv, x, g, b);
             counted();
             k_heat_gate<<<1, 1, 0, st>>>(d_cancel, s > 1 ? d_status + (s - 2) : nullptr, d_status + (s - 1));
-            HeatPcg a{nb, sk.dev(), sl.dev(), su.dev(), bwd_slice, Av, Lv, Uv, D, b, x, r, pp, ap, yrec, zrec,
-                      partials, timeout, (unsigned long long)s << 32, tol, max_iter, d_status + (s - 1),
-                      d_iters + (s - 1), d_rel + (s - 1), timing};
-            void* args[] = {&a};
             counted();
-            CK(cudaLaunchCooperativeKernel(pcg_fn, dim3(grid), dim3(kT), args, 0, st));
+            if (!mixed) {
+                HeatPcg<double> a{nb, sk.dev(), sl.dev(), su.dev(), bwd_slice, Av, Lv, Uv, D, b, x, r, pp, ap,
+                                  yrec, zrec, partials, timeout, (unsigned long long)s << 32, tol, max_iter,
+                                  d_status + (s - 1), d_iters + (s - 1), d_rel + (s - 1), timing,
+                                  nullptr, nullptr, nullptr, 0.0};
+                void* args[] = {&a};
+                CK(cudaLaunchCooperativeKernel(pcg_fn, dim3(grid), dim3(kT), args, 0, st));
+            } else {
+                // 32-bit tags: increment s starts after the sweeps every earlier increment can take
+                const unsigned long long epoch0 = (unsigned long long)(s - 1) * ((unsigned long long)max_iter + 2);
+                HeatPcg<float> a{nb, sk.dev(), sl.dev(), su.dev(), bwd_slice, Av32, Lv32, Uv32, D32, b, x32, r32,
+                                 p32, ap32, yrec32, zrec32, partials, timeout, epoch0, tol, max_iter,
+                                 d_status + (s - 1), d_iters + (s - 1), d_rel + (s - 1), timing,
+                                 Av, x, r64, kHeatDelta};
+                void* args[] = {&a};
+                CK(cudaLaunchCooperativeKernel(pcg_fn, dim3(grid), dim3(kT), args, 0, st));
+            }
             counted();
             k_heat_scatter<<<grid_of(n), kT, 0, st>>>(n, inv, fixed, imp, x, temps + (size_t)s * n);
             if (!fixed_nodes.empty()) {

@@ -97,7 +97,7 @@ def thermal_loads(coords, conn, sources=(), convection=()) -> np.ndarray:
 
 def thermal_problem_struct(coords, conn, conductivity, rho_c, fixed, imposed, f, initial, time_step,
                            theta, increments, conv_elem=None, conv_face=None, conv_film=None,
-                           tol=1e-12, max_iter=10000, ordering=MAILLE_ORDER_AUTO, device=0):
+                           tol=1e-12, max_iter=10000, ordering=MAILLE_ORDER_AUTO, device=0, precision=0):
     """ThermalProblem over numpy arrays (kept alive in the returned dict)."""
     conn_a = np.asarray(conn)
     keep = dict(coords=np.ascontiguousarray(coords, np.float64).ravel(),
@@ -118,12 +118,12 @@ def thermal_problem_struct(coords, conn, conductivity, rho_c, fixed, imposed, f,
         f=ptr(keep["f"], _lib._d), n_convection=keep["ce"].size, conv_elem=ptr(keep["ce"], _lib._i64),
         conv_face=ptr(keep["cf"], _lib._i32), conv_film=ptr(keep["ch"], _lib._d),
         initial=ptr(keep["initial"], _lib._d), time_step=time_step, theta=theta, increments=increments,
-        rel_tol=tol, max_iter=max_iter, ordering=ordering, device=device)
+        rel_tol=tol, max_iter=max_iter, ordering=ordering, device=device, precision=precision)
     return p, keep
 
 
 def solve_problem(prob, f=None, tol=1e-12, max_iter=10000, fluxes=True, device=0,
-                  ordering=MAILLE_ORDER_AUTO, out=None):
+                  ordering=MAILLE_ORDER_AUTO, out=None, precision=0):
     """The transient step of a meshgen.ThermalProblem on the GPU. `f` is the assembled heat-load
     vector (None: nodal loads plus the problem's sources and convection through
     thermal_loads). `out` may hold preallocated result arrays (temps, reactions, fluxes,
@@ -140,7 +140,8 @@ def solve_problem(prob, f=None, tol=1e-12, max_iter=10000, fluxes=True, device=0
             list(zip(prob.c_elem, prob.c_face, prob.c_film, prob.c_sink)))
     p, keep = thermal_problem_struct(prob.coords, prob.conn, prob.conductivity, prob.rho_c, prob.fixed,
                                      prob.imposed, f, prob.initial, prob.time_step, prob.theta, steps,
-                                     prob.c_elem, prob.c_face, prob.c_film, tol, max_iter, ordering, device)
+                                     prob.c_elem, prob.c_face, prob.c_film, tol, max_iter, ordering, device,
+                                     precision)
     if out is None:
         out = dict(temps=np.zeros((steps + 1, n)), reactions=np.zeros((steps + 1, n)),
                    fluxes=np.zeros((steps + 1, ne, ng, 6)) if fluxes else None,

@@ -113,7 +113,7 @@ int main(int argc, char** argv) {
         }
     const int32_t steps = 5;
     MailleThermalProblem tp = {nn, coords, 4, ne, conn, k, rc, fixed, imposed, NULL, 0, NULL, NULL, NULL, t0,
-                               0.02, 1.0, steps, 1e-12, 10000, MAILLE_ORDER_AUTO, 0};
+                               0.02, 1.0, steps, 1e-12, 10000, MAILLE_ORDER_AUTO, 0, MAILLE_FP64};
     double* temps = calloc((size_t)(steps + 1) * nn, sizeof(double));
     double* react = calloc((size_t)(steps + 1) * nn, sizeof(double));
     MailleThermalResult tr = {0};

@@ -258,6 +258,8 @@ def test_thermal_inputs_are_rejected_before_any_device_work(lib):
         return lib.maille_gpu_thermal_transient(ctypes.byref(p), ctypes.byref(r))
 
     assert status(theta=0.4) == _lib.MAILLE_INVALID_INPUT and "theta" in _lib.last_error()
+    assert status(precision=7) == _lib.MAILLE_INVALID_INPUT and "precision" in _lib.last_error()
+    assert status(precision=1, increments=600000) == _lib.MAILLE_INVALID_INPUT and "32-bit" in _lib.last_error()
     assert status(theta=float("nan")) == _lib.MAILLE_INVALID_INPUT
     assert status(increments=0) == _lib.MAILLE_INVALID_INPUT
     assert status(time_step=0.0) == _lib.MAILLE_INVALID_INPUT

@@ -124,16 +124,17 @@ def test_iteration_cap_reports_not_converged(gpu):
     assert "increment 1" in _lib.last_error()
 
 
-def test_full_size_transient_matches_the_oracle_summary(gpu):
+@pytest.mark.parametrize("precision", [_lib.MAILLE_FP64, _lib.MAILLE_MIXED])
+def test_full_size_transient_matches_the_oracle_summary(gpu, precision):
     # the 40^3 Tet10 workload (7.7 M lower slots, more than one thread each in any capped grid):
     # iterations per increment, reaction sums and sampled final temperatures against the
-    # oracle's run (tests/golden/make_thermal_40_summary.py)
+    # oracle's run (tests/golden/make_thermal_40_summary.py), in both precisions
     import json
     import os
     g = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
                                     "thermal_40_oracle_summary.json")))
     p = mg.thermal_cube(40, True, increments=g["increments"], time_period=g["time_period"])
-    s, out = th.solve_problem(p, fluxes=False)
+    s, out = th.solve_problem(p, fluxes=False, precision=precision)
     assert s == 0, _lib.last_error()
     assert out["info"]["free_nodes"] == g["free_nodes"]
     sample = out["temps"][-1][::g["t_final_stride"]]
@@ -252,4 +253,30 @@ def test_device_ordering_equals_the_host_ordering(gpu, monkeypatch, ordering):
     assert s1 == 0 and s2 == 0, _lib.last_error()
     assert a["info"]["levels"] == b["info"]["levels"]
     assert np.array_equal(a["iterations"], b["iterations"])
+    assert np.array_equal(a["temps"], b["temps"])
+
+
+@pytest.mark.parametrize("quadratic,cells", [(False, 8), (True, 4)])
+def test_mixed_precision_transient_matches_the_oracle(gpu, oracle_lib, quadratic, cells):
+    """The mixed form (FP32 matrices and vectors, FP64 reliable updates, the stopping test on the
+    FP64 true residual) against the oracle's FP64 history, at the FP64 tolerances of this file."""
+    p = mg.thermal_cube(cells, quadratic, increments=4, time_period=0.04)
+    ref = oracle_lib.thermal_transient(p, solver=2)
+    s, out = th.solve_problem(p, f=ref["f"], precision=_lib.MAILLE_MIXED)
+    assert s == 0, _lib.last_error()
+    _check(out, ref)
+    assert out["info"]["max_rel_residual"] <= 1e-12
+    s64, out64 = th.solve_problem(p, f=ref["f"])
+    assert s64 == 0
+    # the same problem in FP64 within the solver tolerance
+    assert _rel(out["temps"], out64["temps"]) < 1e-10
+
+
+def test_mixed_precision_iteration_cap_and_repeatability(gpu):
+    p = mg.thermal_cube(6, False, increments=2, time_period=0.02)
+    s, out = th.solve_problem(p, max_iter=3, precision=_lib.MAILLE_MIXED)
+    assert s == _lib.MAILLE_NOT_CONVERGED and "IterativeNotConverged at increment 1" in _lib.last_error()
+    s1, a = th.solve_problem(p, precision=_lib.MAILLE_MIXED)
+    s2, b = th.solve_problem(p, precision=_lib.MAILLE_MIXED)
+    assert s1 == 0 and s2 == 0
     assert np.array_equal(a["temps"], b["temps"])
