@@ -22,6 +22,8 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
+#include <cstdio>
+#include <cstdlib>
 
 #include <cooperative_groups.h>
 #include <cub/cub.cuh>
@@ -275,20 +277,34 @@ __global__ void __launch_bounds__(kT) k_bfs(BfsArgs a) {
     }
 }
 
+__device__ __forceinline__ int32_t ld_val(const int32_t* p) {
+    int32_t v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_val(int32_t* p, int32_t v) {
+    asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Greedy colouring (mode 0) or dependency levels (mode 1) of the nodes in visit order: visit[q]
-// is the node at visit position q, rpos its inverse. A warp takes positions w, w + W, ...; for the
-// node at position q it waits for the values of its neighbours of smaller visit position and sets
-// the smallest colour none of them holds (mode 0) or one more than their largest level (mode 1).
-// Values start at -1. *fail is set when a wait ran out or a colour reached 1024.
+// is the node at visit position q, rpos its inverse. Warps claim visit positions in increasing
+// order from a counter (*next, 0 at launch); for the node at position q a warp waits for the
+// values of its neighbours of smaller visit position and sets the smallest colour none of them
+// holds (mode 0) or one more than their largest level (mode 1). The smallest unfinished position
+// was claimed by a warp that waits only on smaller, finished positions, so the launch always
+// progresses (every warp is co-resident); a warp stuck behind a slow node does not hold up the
+// positions after it, as a fixed schedule would. Values start at -1. *fail is set when a wait
+// ran out or a colour reached 1024.
 __global__ void __launch_bounds__(kT) k_greedy(int32_t nk, const int64_t* __restrict__ off,
                                                const int32_t* __restrict__ adj, const int32_t* __restrict__ visit,
                                                const int32_t* __restrict__ rpos, int32_t* value, int mode,
-                                               int32_t* fail) {
+                                               int32_t* fail, int32_t* next) {
     const int lane = threadIdx.x & 31;
-    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    volatile int32_t* val = value;
-    for (int64_t q = gw; q < nk; q += nwarps) {
+    for (;;) {
+        int32_t qq = 0;
+        if (lane == 0) qq = atomicAdd(next, 1);
+        const int64_t q = __shfl_sync(0xffffffffu, qq, 0);
+        if (q >= nk) break;
         const int32_t v = visit[q];
         unsigned int words = 0;  // lane j: colours 32 j .. 32 j + 31 held by earlier neighbours
         int32_t top = -1;         // mode 1: largest level of an earlier neighbour
@@ -299,10 +315,15 @@ __global__ void __launch_bounds__(kT) k_greedy(int32_t nk, const int64_t* __rest
             if (p < off[v + 1]) {
                 const int32_t u = adj[p];
                 if (rpos[u] < q) {
-                    unsigned int k = 0;
-                    c = val[u];
+                    // a pending neighbour is polled with a growing pause: thousands of warps wait
+                    // on the same few nodes of the frontier, and back-to-back polls of those lines
+                    // slow down the stores they wait for
+                    unsigned int k = 0, pause = 32;
+                    c = ld_val(value + u);
                     while (c < 0 && k < kSpin) {
-                        c = val[u];
+                        __nanosleep(pause);
+                        pause = pause < 256 ? 2 * pause : 256;
+                        c = ld_val(value + u);
                         ++k;
                     }
                     if (c < 0) bad = true;
@@ -334,7 +355,7 @@ __global__ void __launch_bounds__(kT) k_greedy(int32_t nk, const int64_t* __rest
         }
         if (lane == 0) {
             if (bad) atomicExch(fail, 1);
-            val[v] = bad ? 0 : result;  // a failed node still unblocks the later ones; discarded
+            st_val(value + v, bad ? 0 : result);  // a failed node still unblocks the later ones
         }
         __syncwarp();
     }
@@ -411,6 +432,16 @@ int coop_grid(const void* fn, int threads) {
 void gpu_ordering(int npe, int64_t n_elems, const int32_t* conn, const int32_t* kept_of, int32_t nk,
                   int ordering, cudaStream_t st, std::vector<int32_t>& order, std::vector<int32_t>& level) {
     if (nk <= 0) throw CudaFailure{"no kept node to order"};
+    // MAILLE_SETUP_TIMING: wall time of each step (stream synchronised)
+    const bool timing = std::getenv("MAILLE_SETUP_TIMING") != nullptr;
+    double t_mark = now_ms();
+    auto tmark = [&](const char* name, int extra = -1) {
+        if (!timing) return;
+        cudaStreamSynchronize(st);
+        const double t = now_ms();
+        std::fprintf(stderr, "maille ordering %-16s %8.2f ms %d\n", name, t - t_mark, extra);
+        t_mark = t;
+    };
     // the kept-node graph, neighbours by ascending index
     const int64_t nkeys = n_elems * npe * (npe - 1);
     if (nkeys >= INT_MAX || nkeys <= 0) throw CudaFailure{"mesh size outside the device ordering's range"};
@@ -452,6 +483,7 @@ void gpu_ordering(int npe, int64_t n_elems, const int32_t* conn, const int32_t* 
         int32_t* p;
         ~AdjFree() { dfree(p); }
     } adj_free{adj};
+    tmark("graph", (int)m);
 
     Buf<int32_t> mark(nk), queue(nk), cnt(nk), out(4);
     Buf<unsigned long long> par(nk), best(1);
@@ -475,6 +507,7 @@ void gpu_ordering(int npe, int64_t n_elems, const int32_t* conn, const int32_t* 
         levels = h[0];
         qend = h[1];
         last_begin = h[2];
+        tmark(ordering_search ? "ordering search" : "peripheral search", levels);
     };
     auto argmin = [&](auto launch) -> int64_t {
         static const unsigned long long none = ~0ull;
@@ -524,18 +557,25 @@ void gpu_ordering(int npe, int64_t n_elems, const int32_t* conn, const int32_t* 
     k_reverse<<<grid_of(nk), kT, 0, st>>>(nk, queue.p, visit.p, rpos.p);
     k_fill_i32<<<grid_of(nk), kT, 0, st>>>(nk, -1, value.p);
     CK(cudaMemsetAsync(fail.p, 0, sizeof(int32_t), st));
-    const int greedy_grid = coop_grid((const void*)k_greedy, kT);
+    // one block of 8 warps per SM: a round of warps spans a few levels of the colouring's
+    // dependency graph (about 300 nodes a level on the Tet10 cube), and fewer waiting warps keep
+    // the polls off the frontier's cache lines
+    const int greedy_grid = std::min(coop_grid((const void*)k_greedy, kT), device_sms());
+    Buf<int32_t> claim(1);
     auto colour = [&](const int32_t* vis, const int32_t* rp, int mode) {
         int32_t nk_ = nk;
         const int64_t* o = off.p;
         const int32_t* ad = adj;
         int32_t* va = value.p;
         int32_t* fl = fail.p;
-        void* args[] = {&nk_, &o, &ad, &vis, &rp, &va, &mode, &fl};
+        int32_t* nx = claim.p;
+        CK(cudaMemsetAsync(claim.p, 0, sizeof(int32_t), st));
+        void* args[] = {&nk_, &o, &ad, &vis, &rp, &va, &mode, &fl, &nx};
         counted();
         CK(cudaLaunchCooperativeKernel((const void*)k_greedy, dim3(greedy_grid), dim3(kT), args, 0, st));
     };
     colour(visit.p, rpos.p, ordering == MAILLE_ORDER_RCM ? 1 : 0);
+    tmark("greedy", greedy_grid);
     Buf<uint64_t> k0(nk), k1(nk);
     Buf<int32_t> i0(nk), i1(nk);
     if (ordering == MAILLE_ORDER_MULTICOLOR_ITERATED) {
@@ -574,6 +614,7 @@ void gpu_ordering(int npe, int64_t n_elems, const int32_t* conn, const int32_t* 
     CK(cudaMemcpyAsync(order.data(), i1.p, (size_t)nk * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(level.data(), value.p, (size_t)nk * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    tmark("sort and copies", bfs_grid);
     if (h_fail) throw CudaFailure{"device ordering: a colouring wait ran out or a node needs 1024 colours or more"};
 }
 

@@ -531,10 +531,15 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         // 4 reduction slots for every block of the persistent grid and of the norm kernels
         // (grids capped at 8 and 4 blocks per SM)
         h->persist_grid = std::min(h->persist_grid, 8 * device_sms());
-        // MAILLE_PERSIST_BLOCKS_PER_SM: fewer co-resident blocks than the occupancy allows (a
-        // tuning and measurement knob: the sweeps' time against the warps in flight)
-        if (const int bps = env_int("MAILLE_PERSIST_BLOCKS_PER_SM", 0); bps > 0)
-            h->persist_grid = std::min(h->persist_grid, bps * device_sms());
+        // small systems: a grid sized to the work (one block of 8 warps per 8 slices of K, at
+        // least half the SMs), so that each of the iteration's grid barriers spans fewer blocks
+        // (the large-strain block, 587 slices: 74 blocks, 8 % faster than 296)
+        h->persist_grid = std::min<int64_t>(
+            h->persist_grid, std::max<int64_t>(device_sms() / 2, (h->sk.h.nslices() + 7) / 8));
+        // MAILLE_PERSIST_GRID: fewer co-resident blocks than the occupancy allows (a tuning and
+        // measurement knob: the phases' time against the warps in flight and the barrier cost)
+        if (const int blocks = env_int("MAILLE_PERSIST_GRID", 0); blocks > 0)
+            h->persist_grid = std::min(h->persist_grid, blocks);
         h->partials = dalloc<double>((size_t)4 * 8 * device_sms());
         if (env_int("MAILLE_PHASE_TIMING", 0)) {
             h->timing = dalloc<unsigned long long>(8);
