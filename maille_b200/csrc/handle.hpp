@@ -37,6 +37,14 @@ struct SellBuf {
         fill_sell(SELL_FULL, h.lpr, h.nslices(), h.steps(), rowid, off, pt.row_ptr, pt.col, pt.diag,
                   nb, col, src, st);
     }
+    // hands the device buffers to `out` (freed together by the caller) and forgets them
+    void gather(std::vector<void*>& out) {
+        for (void* p : {(void*)rowid, (void*)off, (void*)col, (void*)src}) out.push_back(p);
+        rowid = nullptr;
+        off = nullptr;
+        col = nullptr;
+        src = nullptr;
+    }
     void release() {
         for (void* p : {(void*)rowid, (void*)off, (void*)col, (void*)src}) dfree(p);
         rowid = nullptr;
@@ -73,6 +81,15 @@ struct PsellBuf {
                    nb, col, src, st);
         CK(cudaStreamSynchronize(st));
         dfree(rstart);
+    }
+    void gather(std::vector<void*>& out) {
+        for (void* p : {(void*)off, (void*)col, (void*)src, (void*)head, (void*)row0, (void*)rows}) out.push_back(p);
+        off = nullptr;
+        col = nullptr;
+        src = nullptr;
+        head = nullptr;
+        row0 = nullptr;
+        rows = nullptr;
     }
     void release() {
         for (void* p : {(void*)off, (void*)col, (void*)src, (void*)head, (void*)row0, (void*)rows}) dfree(p);

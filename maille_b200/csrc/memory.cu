@@ -70,6 +70,17 @@ void device_free(void* p) {
     cudaStreamSynchronize(d.stream);
 }
 
+void device_free_all(const std::vector<void*>& ps) {
+    bool any = false;
+    for (void* p : ps) any = any || p != nullptr;
+    if (!any) return;
+    DevicePool& d = pool_of_current_device();
+    cudaDeviceSynchronize();
+    for (void* p : ps)
+        if (p) cudaFreeAsync(p, d.stream);
+    cudaStreamSynchronize(d.stream);
+}
+
 int device_sms() {
     constexpr int kMaxDevices = 64;
     static std::atomic<int> cached[kMaxDevices];

@@ -579,12 +579,16 @@ void build_sell(const Symbolic& s, SellKind kind, int lpr, SellHost& out) {
     const int S = 32 / lpr, per_step = 4 * lpr;
     out.level_slices.push_back(0);
     std::vector<int32_t> rows;
+    std::vector<int64_t> count;
     for (int32_t l = 0; l < s.levels; ++l) {
-        rows.clear();
-        for (int32_t i = s.level_ptr[l]; i < s.level_ptr[l + 1]; ++i) rows.push_back(i);
-        std::stable_sort(rows.begin(), rows.end(), [&](int32_t a, int32_t b) {
-            return end(a) - start(a) > end(b) - start(b);
-        });
+        // the level's rows by decreasing length, stable (a counting sort: lengths are small)
+        int64_t maxlen = 0;
+        for (int32_t i = s.level_ptr[l]; i < s.level_ptr[l + 1]; ++i) maxlen = std::max<int64_t>(maxlen, end(i) - start(i));
+        count.assign((size_t)maxlen + 2, 0);
+        for (int32_t i = s.level_ptr[l]; i < s.level_ptr[l + 1]; ++i) count[(size_t)(maxlen - (end(i) - start(i))) + 1]++;
+        for (size_t k = 1; k < count.size(); ++k) count[k] += count[k - 1];
+        rows.resize((size_t)(s.level_ptr[l + 1] - s.level_ptr[l]));
+        for (int32_t i = s.level_ptr[l]; i < s.level_ptr[l + 1]; ++i) rows[count[(size_t)(maxlen - (end(i) - start(i)))]++] = i;
         for (size_t c0 = 0; c0 < rows.size(); c0 += S) {
             const size_t c1 = std::min(rows.size(), c0 + S);
             int64_t maxlen = 0;

@@ -57,10 +57,12 @@ MailleGpuHandle::~MailleGpuHandle() {
                     elem_slot, ke, K, F, Ks64, Ls64, Us64, D64, Ks32, Ls32, Us32, D32, b64, x64,
                     r64, z64, p64, ap64, x32, r32, z32, p32, ap32, u_full, y_full, ye, gauss, vm,
                     react, lambda_full, grad, node_stress, node_vm, scal, partials, timing, claim, dsum, dticket, dfail};
-    for (void* p : bufs) dfree(p);
-    sk.release();
-    pl.release();
-    pu.release();
+    // one device synchronisation for all of them (a free per buffer waited for the device each time)
+    std::vector<void*> all(std::begin(bufs), std::end(bufs));
+    sk.gather(all);
+    pl.gather(all);
+    pu.gather(all);
+    device_free_all(all);
     if (h_scal) cudaFreeHost(h_scal);
     if (h_sum) cudaFreeHost(h_sum);
     for (auto& e : ev)
