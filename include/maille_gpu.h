@@ -50,8 +50,8 @@ typedef enum {
 
 /* Ordering of the free nodes for the level-scheduled IC(0). */
 typedef enum {
-    MAILLE_ORDER_AUTO = 0,           /* the path's measured best: MULTICOLOR for the elastic
-                                        solves, MULTICOLOR_BFS for the thermal step */
+    MAILLE_ORDER_AUTO = 0,           /* the path's measured best: MULTICOLOR_ITERATED for the
+                                        elastic solves, MULTICOLOR_BFS for the thermal step */
     MAILLE_ORDER_MULTICOLOR = 1,     /* greedy colouring of the node graph visited in RCM order:
                                         one level per colour, a few dozen levels */
     MAILLE_ORDER_RCM = 2,            /* reverse Cuthill-McKee on the node graph (the reference's

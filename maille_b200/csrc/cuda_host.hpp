@@ -42,7 +42,8 @@ inline double now_ms() {
 // stream when it returns; a free waits for the device to be idle, like cudaFree.
 void* device_alloc(size_t bytes);
 void device_free(void* p);
-// Frees every non-null pointer of `ps` after a single wait for the device to be idle.
+// Frees every non-null pointer of `ps` on the pool's stream and waits for it; the caller has
+// synchronised every stream that used them (a handle's destructor: its own stream).
 void device_free_all(const std::vector<void*>& ps);
 // Returns the pool's unused memory of `device` to the device (0, or -1 on a CUDA error).
 int32_t trim_device_memory(int device);

@@ -75,7 +75,6 @@ void device_free_all(const std::vector<void*>& ps) {
     for (void* p : ps) any = any || p != nullptr;
     if (!any) return;
     DevicePool& d = pool_of_current_device();
-    cudaDeviceSynchronize();
     for (void* p : ps)
         if (p) cudaFreeAsync(p, d.stream);
     cudaStreamSynchronize(d.stream);
