@@ -362,21 +362,25 @@ __device__ __forceinline__ void stage_step(const T* vals, int64_t g, Stage<T>& s
     bulk_stage(st.buf, vals + g * 9 * kStepSlots, kBytes, st.bar);
 }
 
+// The first read of this lane's 4 records of a step (columns c4; padding slots need none).
+template <typename T>
+__device__ __forceinline__ void issue_records(int4 c4, const T* z, int32_t pad, typename RecOf<T>::type q[4]) {
+    const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) q[j] = cc[j] == pad ? pad_record<T>() : ld_record(z, cc[j]);
+}
+
 // One step of a packed slice for this lane's 4 slots: P[j] = V_j z[col_j], every column first
 // awaited for sweep `epoch`; false when a wait hit the spin limit. The step's values are already on
-// their way into the warp's buffer (a bulk copy started when the buffer last became free) and the
-// lane's columns were fetched ahead, so the records are requested at once and their L2 round trip
-// is the step's only wait. Once every lane has read the buffer, lane 0 starts the copy of step
-// `next` (the next step of this slice or the first of the warp's next slice; < 0: none).
+// their way into the warp's buffer (a bulk copy started when the buffer last became free), the
+// lane's columns were fetched ahead and its records q requested by issue_records, so their L2
+// round trip is the step's only wait. Once every lane has read the buffer, lane 0 starts the copy
+// of step `next` (the next step of this slice or the first of the warp's next slice; < 0: none).
 template <typename T>
 __device__ __forceinline__ bool slot_products(const T* __restrict__ vals, int4 c4, const T* z,
                                               unsigned int epoch, int lane, Stage<T>& st,
-                                              int64_t next, int32_t pad, T P[4][3]) {
-    using R = typename RecOf<T>::type;
+                                              int64_t next, typename RecOf<T>::type q[4], T P[4][3]) {
     const int32_t cc[4] = {c4.x, c4.y, c4.z, c4.w};
-    R q[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) q[j] = cc[j] == pad ? pad_record<T>() : ld_record(z, cc[j]);
     bool ok = await_records<T>(z, cc, epoch, q, kSpinLimit);
     ok = mbar_wait(st.bar, st.phase) && ok;
     st.phase ^= 1u;
@@ -527,7 +531,10 @@ __device__ __forceinline__ int4 lane_cols(const PsellDev& A, int64_t g, int lane
 // The warp's slice loop is software-pipelined so that a slice's critical path is the L2 round
 // trip of its records: the bookkeeping of the slice after next, the columns and owned rows of the
 // next slice, the next slice's right-hand sides and diagonal blocks, and (once the buffer frees)
-// the next step's values are all requested while the current slice runs.
+// the next step's values are all requested while the current slice runs, and the slice's own row
+// inputs (right-hand sides, diagonal blocks, the update's operands) are requested right after its
+// records, so they travel during the records' round trip instead of being carried in registers
+// from the previous slice (whose register copy waited for them at the loop's end).
 // In a one-step slice (at most 32 rows) lane k owns row k. Each lane forms the products of its 4
 // slots and sums them per row inside the lane; a segmented scan over the warp (fixed order)
 // carries the partial sums across lanes, and the owner of each row fetches the row's total from
@@ -548,8 +555,7 @@ __device__ __forceinline__ double sweep(const PsellDev& A, unsigned int epoch, c
     int4 c0 = lane_cols(A, m0.g0, lane);
     int32_t row0 = lane < m0.r1 - m0.r0 ? __ldg(A.rows + m0.r0 + lane) : -1;
     if (lane == 0) stage_step(vals, m0.g0, st);
-    RowIn<T, FWD, FUSED> in0{};
-    if (row0 >= 0) in0.load(row0, D, nb, r, z, upd);
+    using R = typename RecOf<T>::type;
     for (; k < n; k += nw) {
         const bool more = k + nw < n;
         const SliceMeta m2 = slice_meta(A, k + 2 * nw);
@@ -561,12 +567,16 @@ __device__ __forceinline__ double sweep(const PsellDev& A, unsigned int epoch, c
         }
         const int64_t next_slice = more ? m1.g0 : -1;
         T a0 = 0, a1 = 0, a2 = 0;
+        RowIn<T, FWD, FUSED> in{};
         if (m0.g1 - m0.g0 == 1) {
+            R q[4];
+            issue_records<T>(c0, z, A.pad, q);
+            if (row0 >= 0) in.load(row0, D, nb, r, z, upd);
             const int32_t nrows = m0.r1 - m0.r0;
             const uint32_t mine = head_bits(m0.head, lane);
             const int last = lane + 1 < nrows ? nth_set(m0.head, lane + 1) - 1 : 127;
             T P[4][3];
-            ok = slot_products(vals, c0, z, epoch, lane, st, next_slice, A.pad, P) && ok;
+            ok = slot_products(vals, c0, z, epoch, lane, st, next_slice, q, P) && ok;
             // in-lane running sums, restarted at each row start; the lane's carry-out is the sum
             // of its slots after its last row start (all 4 when none starts here)
             T s0 = 0, s1 = 0, s2 = 0;
@@ -609,24 +619,23 @@ __device__ __forceinline__ double sweep(const PsellDev& A, unsigned int epoch, c
                 if (j == js) { a0 = v0; a1 = v1; a2 = v2; }
             }
         } else {
+            if (row0 >= 0) in.load(row0, D, nb, r, z, upd);
             for (int64_t g = m0.g0; g < m0.g1; ++g) {
                 const int4 cg4 = g == m0.g0 ? c0 : lane_cols(A, g, lane);
+                R q[4];
+                issue_records<T>(cg4, z, A.pad, q);
                 T P[4][3];
-                ok = slot_products(vals, cg4, z, epoch, lane, st, g + 1 < m0.g1 ? g + 1 : next_slice, A.pad, P) && ok;
+                ok = slot_products(vals, cg4, z, epoch, lane, st, g + 1 < m0.g1 ? g + 1 : next_slice, q, P) && ok;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) { a0 += P[j][0]; a1 += P[j][1]; a2 += P[j][2]; }
             }
             lanes_sum<T, 32>(a0, a1, a2);
         }
-        if (row0 >= 0) loc += in0.finish(row0, a0, a1, a2, r, z, epoch, upd);
-        // the next slice's right-hand sides and diagonal blocks (its rows arrived meanwhile)
-        RowIn<T, FWD, FUSED> in1{};
-        if (row1 >= 0) in1.load(row1, D, nb, r, z, upd);
+        if (row0 >= 0) loc += in.finish(row0, a0, a1, a2, r, z, epoch, upd);
         m0 = m1;
         m1 = m2;
         c0 = c1;
         row0 = row1;
-        in0 = in1;
     }
     return loc;
 }
