@@ -185,7 +185,7 @@ struct MailleGpuBatch {
                         flags, timing};
         for (void* q : bufs) dfree(q);
         for (void* q : state_bufs) dfree(q);
-        if (h_cancel) cudaFreeHost(h_cancel);
+        pinned_slot_free(h_cancel);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (st) cudaStreamDestroy(st);
@@ -732,8 +732,7 @@ int32_t create_batch(const MailleBatchProblem* p, MailleGpuBatch** out) {
         b->tickets = dalloc<unsigned int>(3 * (size_t)b->n_inst);
         CK(cudaMemsetAsync(b->tickets, 0, 3 * (size_t)b->n_inst * sizeof(unsigned int), st));
         b->flags = dalloc<unsigned int>(((size_t)s.nb + 1) * 8);
-        CK(cudaHostAlloc(&b->h_cancel, sizeof(int32_t), cudaHostAllocMapped));
-        *b->h_cancel = 0;
+        b->h_cancel = static_cast<int32_t*>(pinned_slot_alloc(sizeof(int32_t)));
         CK(cudaHostGetDevicePointer((void**)&b->d_cancel, b->h_cancel, 0));
         if (env_int("MAILLE_PHASE_TIMING", 0)) {
             b->timing = dalloc<unsigned long long>(8);

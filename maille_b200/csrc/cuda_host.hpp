@@ -47,6 +47,10 @@ void device_free(void* p);
 void device_free_all(const std::vector<void*>& ps);
 // Returns the pool's unused memory of `device` to the device (0, or -1 on a CUDA error).
 int32_t trim_device_memory(int device);
+// A zeroed pinned host slot of at most 256 bytes, mapped and portable (its device address equals
+// its host address); slots are reused, never returned to the driver.
+void* pinned_slot_alloc(size_t bytes);
+void pinned_slot_free(void* p);
 // Streaming multiprocessors of the current device (cudaDevAttrMultiProcessorCount, cached per
 // device): grid caps are multiples of it.
 int device_sms();

@@ -296,7 +296,7 @@ struct MailleGpuLargeStrain {
                           wv, gmu, glam, partials, norms})
             dfree(p);
         dfree(ticket);
-        if (h_norms) cudaFreeHost(h_norms);
+        pinned_slot_free(h_norms);
         if (h) maille_gpu_destroy(h);
     }
 };
@@ -600,7 +600,7 @@ int32_t ls_create(const MailleLargeStrainProblem* p, MailleGpuLargeStrain** out)
         s->norms = maille::dalloc<double>(4);
         s->ticket = maille::dalloc<unsigned int>(2);
         CK(cudaMemsetAsync(s->ticket, 0, 2 * sizeof(unsigned int), st));
-        CK(cudaMallocHost(&s->h_norms, 4 * sizeof(double)));
+        s->h_norms = static_cast<double*>(pinned_slot_alloc(4 * sizeof(double)));
         status = ls_set_materials(s.get(), nullptr, nullptr);
         if (status != MAILLE_OK) return status;
     } catch (const CudaFailure& e) {

@@ -15,6 +15,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -78,6 +79,40 @@ void device_free_all(const std::vector<void*>& ps) {
     for (void* p : ps)
         if (p) cudaFreeAsync(p, d.stream);
     cudaStreamSynchronize(d.stream);
+}
+
+namespace {
+
+// Small pinned host slots (a handle's scalar read-back, a cancel flag). Each cudaFreeHost waits for
+// every device, and a handle's destruction took tens of milliseconds in two of them; the slots are
+// carved from mapped, portable chunks that stay allocated for the process, so a slot's device
+// address is its host address on every device (unified addressing).
+constexpr size_t kPinnedSlot = 256;
+constexpr size_t kPinnedChunk = 64 * 1024;
+std::mutex g_pinned_mutex;
+std::vector<void*> g_pinned_free;
+
+}  // namespace
+
+void* pinned_slot_alloc(size_t bytes) {
+    if (bytes > kPinnedSlot) throw CudaFailure{"pinned_slot_alloc: more than 256 bytes asked"};
+    std::lock_guard<std::mutex> lock(g_pinned_mutex);
+    if (g_pinned_free.empty()) {
+        void* chunk = nullptr;
+        CK(cudaHostAlloc(&chunk, kPinnedChunk, cudaHostAllocMapped | cudaHostAllocPortable));
+        for (size_t off = kPinnedChunk; off >= kPinnedSlot; off -= kPinnedSlot)
+            g_pinned_free.push_back(static_cast<char*>(chunk) + off - kPinnedSlot);
+    }
+    void* p = g_pinned_free.back();
+    g_pinned_free.pop_back();
+    std::memset(p, 0, kPinnedSlot);
+    return p;
+}
+
+void pinned_slot_free(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mutex);
+    g_pinned_free.push_back(p);
 }
 
 int device_sms() {

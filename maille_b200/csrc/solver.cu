@@ -66,8 +66,8 @@ MailleGpuHandle::~MailleGpuHandle() {
     pu.gather(all);
     device_free_all(all);
     const double t1 = now_ms();
-    if (h_scal) cudaFreeHost(h_scal);
-    if (h_sum) cudaFreeHost(h_sum);
+    pinned_slot_free(h_scal);
+    pinned_slot_free(h_sum);
     const double t2 = now_ms();
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
@@ -528,8 +528,8 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         h->ye = dalloc<double>(std::max<size_t>(1, s.belem.size()) * 3 * h->npe);
         h->scal = dalloc<PcgScalars>(1);
         CK(cudaMemsetAsync(h->scal, 0, sizeof(PcgScalars), st));
-        CK(cudaMallocHost(&h->h_scal, sizeof(PcgScalars)));
-        CK(cudaMallocHost(&h->h_sum, 4 * sizeof(double)));
+        h->h_scal = static_cast<PcgScalars*>(pinned_slot_alloc(sizeof(PcgScalars)));
+        h->h_sum = static_cast<double*>(pinned_slot_alloc(4 * sizeof(double)));
         h->dsum = dalloc<double>(4);
         h->dticket = dalloc<unsigned int>(1);
         CK(cudaMemsetAsync(h->dticket, 0, sizeof(unsigned int), st));
