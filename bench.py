@@ -808,11 +808,14 @@ def run_ours(args):
     assert L.maille_gpu_elastic_solve(ctypes.byref(prob), ctypes.byref(res)) == 0
     if world > 1:
         torch.distributed.barrier()
+    walls = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
+        t1 = time.perf_counter()
         s = L.maille_gpu_elastic_solve(ctypes.byref(prob), ctypes.byref(res))
         if s != 0:
             raise RuntimeError(L.maille_gpu_last_error().decode())
+        walls.append((time.perf_counter() - t1) * 1000.0)
     e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
     if world > 1:
         t = torch.tensor([e2e_ms], device="cuda")
@@ -821,7 +824,7 @@ def run_ours(args):
     h2d = sum(a.nbytes for a in (coords, conn, young, poisson, fixed, imposed, floads))
     d2h = sum(a.nbytes for a in outs.values())
     e2e = {"value": world * free / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+           "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "step_walls_ms": walls,
            "phases_ms": {k: getattr(res, k) for k in ("ms_setup", "ms_upload", "ms_element",
                                                       "ms_ordering", "ms_symbolic", "ms_buffers",
                                                       "ms_assembly", "ms_factor", "ms_solve", "ms_post",
