@@ -118,8 +118,8 @@ typedef struct {
     /* the rest of create, in order on the device stream (each 0 after solve-only calls): */
     double ms_element;          /* element integration (Ke of every element) */
     double ms_ordering;         /* wall time from the element integration to a known ordering:
-                                   the device ordering (node graph, RCM, greedy colouring) and
-                                   the join of the host thread */
+                                   the device node incidence, the device ordering (node graph,
+                                   RCM, greedy colouring) and the join of the host thread */
     double ms_symbolic;         /* device pattern and scatter map (radix sorts), the host plan of
                                    the sliced layouts and their slot fills */
     double ms_buffers;          /* numeric buffers and the remaining index uploads */

@@ -139,12 +139,14 @@ bool analyse(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn,
              const uint8_t* fixed, int ordering, Symbolic& s, Error& err, bool pattern = true,
              bool boundary_lists = true);
 
-// The part of analyse that does not depend on the ordering: the input checks, the node incidence,
-// the kept nodes (a node with a free DOF: kept in caller order, kept_of[v] its kept index or -1),
-// the free DOF count and, with boundary_lists, belem and bnodes.
+// The part of analyse that does not depend on the ordering: the input checks, the node incidence
+// (with incidence = false only its run starts inc_ptr: the device builds inc, ordering.cuh
+// gpu_incidence), the kept nodes (a
+// node with a free DOF: kept in caller order, kept_of[v] its kept index or -1), the free DOF count
+// and, with boundary_lists, belem and bnodes.
 bool analyse_topology(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn, const uint8_t* fixed,
                       Symbolic& s, std::vector<int32_t>& kept, std::vector<int32_t>& kept_of, Error& err,
-                      bool boundary_lists);
+                      bool boundary_lists, bool incidence = true);
 
 // The ordering fields of s (nb, perm, inv, fixmask, levels, level_ptr) from an ordering computed
 // elsewhere: order[new row] = kept index with rows grouped by level, level[kept index].

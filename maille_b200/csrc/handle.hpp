@@ -114,7 +114,7 @@ struct MailleGpuHandle {
     int32_t max_iter = kDefaultMaxIter;
     double delta = 0.3;  // reliable update when the FP32 residual fell by this factor
     std::vector<uint8_t> h_fixed;
-    std::vector<double> h_f, h_f0, h_imposed;
+    std::vector<double> h_f, h_f0;
     bool any_imposed = false;
     // device: inputs (caller numbering)
     double *coords = nullptr, *young = nullptr, *poisson = nullptr, *imposed = nullptr, *f = nullptr,

@@ -474,6 +474,24 @@ struct Temp {
     ~Temp() { dfree(p); }
 };
 
+__global__ void k_narrow(int64_t n, const int64_t* __restrict__ in, int32_t* __restrict__ out) {
+    GRID_STRIDE(k, n) out[k] = (int32_t)in[k];
+}
+
+__global__ void k_iota(int64_t n, int32_t* __restrict__ out) {
+    GRID_STRIDE(k, n) out[k] = (int32_t)k;
+}
+
+// ptr[v] = first position of key v in the sorted keys (n_nodes + 1 entries)
+__global__ void k_run_starts(int64_t n_nodes, const uint32_t* __restrict__ keys, int64_t n,
+                             int64_t* __restrict__ ptr) {
+    GRID_STRIDE(v, n_nodes + 1) ptr[v] = lower_bound_dev<uint32_t>(keys, n, (uint32_t)v);
+}
+
+__global__ void k_zero_free(int64_t n, const uint8_t* __restrict__ fixed, double* __restrict__ v) {
+    GRID_STRIDE(k, n) if (!fixed[k]) v[k] = 0.0;
+}
+
 // blocks of a cooperative launch of fn: every block co-resident
 int coop_grid(const void* fn, int threads) {
     int per_sm = 0;
@@ -673,6 +691,44 @@ void gpu_ordering(int npe, int64_t n_elems, const int32_t* conn, const int32_t* 
     CK(cudaStreamSynchronize(st));
     tmark("sort and copies", bfs_grid);
     if (h_fail) throw CudaFailure{"device ordering: a colouring wait ran out or a node needs 1024 colours or more"};
+}
+
+
+void gpu_narrow(const int64_t* in, int64_t n, int32_t* out, cudaStream_t st) {
+    if (n <= 0) return;
+    counted();
+    k_narrow<<<grid_of(n), kT, 0, st>>>(n, in, out);
+    CK(cudaGetLastError());
+}
+
+void gpu_zero_free(int64_t n, const uint8_t* fixed, double* v, cudaStream_t st) {
+    if (n <= 0) return;
+    counted();
+    k_zero_free<<<grid_of(n), kT, 0, st>>>(n, fixed, v);
+    CK(cudaGetLastError());
+}
+
+void gpu_incidence(const int32_t* conn, int64_t n, int64_t n_nodes, cudaStream_t st, int64_t* inc_ptr,
+                   int32_t* inc) {
+    if (n <= 0 || n >= (int64_t(1) << 31)) throw CudaFailure{"gpu_incidence: entry count out of range"};
+    Buf<int32_t> iota(n);
+    Buf<uint32_t> keys(n);
+    counted();
+    k_iota<<<grid_of(n), kT, 0, st>>>(n, iota.p);
+    int bits = 1;
+    while ((int64_t(1) << bits) <= n_nodes) ++bits;
+    // node ids are non-negative, so their unsigned order is theirs; the sort is stable, so the
+    // positions of one node stay ascending
+    const uint32_t* k_in = reinterpret_cast<const uint32_t*>(conn);
+    size_t bytes = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, k_in, keys.p, iota.p, inc, (int)n, 0, bits, st));
+    Temp temp;
+    temp.reserve(bytes);
+    CK(cub::DeviceRadixSort::SortPairs(temp.p, bytes, k_in, keys.p, iota.p, inc, (int)n, 0, bits, st));
+    counted(3);
+    k_run_starts<<<grid_of(n_nodes + 1), kT, 0, st>>>(n_nodes, keys.p, n, inc_ptr);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));  // the temporaries are freed on return
 }
 
 }  // namespace maille

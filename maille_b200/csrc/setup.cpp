@@ -294,7 +294,7 @@ void boundary(Symbolic& s, int64_t n_nodes, int npe, int64_t n_elems, const int6
 
 bool analyse_topology(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* conn, const uint8_t* fixed,
                       Symbolic& s, std::vector<int32_t>& kept, std::vector<int32_t>& kept_of, Error& err,
-                      bool boundary_lists) {
+                      bool boundary_lists, bool incidence) {
     if (npe != 4 && npe != 10) {
         err = {MAILLE_INVALID_INPUT, "nodes_per_elem must be 4 or 10"};
         return false;
@@ -318,12 +318,13 @@ bool analyse_topology(int64_t n_nodes, int npe, int64_t n_elems, const int64_t* 
     s.n_elems = n_elems;
     s.npe = npe;
     const int32_t N = (int32_t)n_nodes;
-    // node -> (element, local) incidence, sorted by element
+    // node -> (element, local) incidence, sorted by element (the run starts always: the solve
+    // looks up the nodes no element touches there)
     s.inc_ptr.assign(N + 1, 0);
     for (int64_t k = 0; k < n_elems * npe; ++k) s.inc_ptr[conn[k] + 1]++;
     for (int32_t v = 0; v < N; ++v) s.inc_ptr[v + 1] += s.inc_ptr[v];
-    s.inc.resize(n_elems * npe);
-    {
+    if (incidence) {
+        s.inc.resize(n_elems * npe);
         std::vector<int64_t> cur(s.inc_ptr.begin(), s.inc_ptr.end() - 1);
         for (int64_t k = 0; k < n_elems * npe; ++k) s.inc[cur[conn[k]]++] = (int32_t)k;
     }

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -327,31 +328,32 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
     h->h_fixed.assign(n3, 0);
     if (p->fixed)
         for (int64_t k = 0; k < n3; ++k) h->h_fixed[k] = p->fixed[k] ? 1 : 0;
-    h->h_imposed.assign(n3, 0.0);
-    if (p->imposed)
-        for (int64_t k = 0; k < n3; ++k)
-            if (h->h_fixed[k]) {
-                h->h_imposed[k] = p->imposed[k];
-                if (p->imposed[k] != 0.0) h->any_imposed = true;
-            }
-    h->h_f.assign(n3, 0.0);
-    if (p->f) std::memcpy(h->h_f.data(), p->f, n3 * sizeof(double));
-
-    // the element kernels index with the connectivity: check it before any device work
+    // the element kernels index with the connectivity: check it before any device work (a
+    // min / max pass; the offending entry is looked for only when there is one)
     if (p->nodes_per_elem != 4 && p->nodes_per_elem != 10)
         return fail({MAILLE_INVALID_INPUT, "nodes_per_elem must be 4 or 10"});
-    for (int64_t k = 0; k < p->n_elems * p->nodes_per_elem; ++k)
-        if (p->conn[k] < 0 || p->conn[k] >= p->n_nodes)
-            return fail({MAILLE_INVALID_INPUT, "element " + std::to_string(k / p->nodes_per_elem) +
-                                                   " refers to unknown node " + std::to_string(p->conn[k])});
+    {
+        const int64_t nc = p->n_elems * p->nodes_per_elem;
+        int64_t lo = INT64_MAX, hi = INT64_MIN;
+        for (int64_t k = 0; k < nc; ++k) {
+            lo = std::min(lo, p->conn[k]);
+            hi = std::max(hi, p->conn[k]);
+        }
+        if (nc > 0 && (lo < 0 || hi >= p->n_nodes))
+            for (int64_t k = 0; k < nc; ++k)
+                if (p->conn[k] < 0 || p->conn[k] >= p->n_nodes)
+                    return fail({MAILLE_INVALID_INPUT, "element " + std::to_string(k / p->nodes_per_elem) +
+                                                           " refers to unknown node " + std::to_string(p->conn[k])});
+    }
     if (std::all_of(h->h_fixed.begin(), h->h_fixed.end(), [](uint8_t f) { return f != 0; }))
         return fail({MAILLE_INVALID_INPUT, "every DOF is fixed"});
     if (p->n_nodes >= (int64_t(1) << 30) || p->n_elems * node_pairs(p->nodes_per_elem) >= (int64_t(1) << 31))
         return fail({MAILLE_INVALID_INPUT, "mesh too large for 32-bit node and element-pair indices"});
-    // The ordering runs on the device (ordering.cu) once the inputs are there; the host keeps the
-    // part that does not depend on it (node incidence, boundary lists) on a thread of its own
-    // meanwhile. MAILLE_HOST_ORDERING=1 orders on that host thread instead (the same permutation:
-    // the same algorithms on the same graph). The pattern and scatter map follow on the device
+    // The ordering and the node incidence run on the device (ordering.cu) once the inputs are
+    // there; the host keeps the part that does not depend on them (kept nodes, boundary lists, the
+    // host copies of the loads and the imposed-value flag) on a thread of its own meanwhile.
+    // MAILLE_HOST_ORDERING=1 orders on that host thread instead (the same permutation: the same
+    // algorithms on the same graph). The pattern and scatter map follow on the device
     // (analysis.cu).
     const bool host_ordering = env_int("MAILLE_HOST_ORDERING", 0) != 0;
     // AUTO: MULTICOLOR_ITERATED (Tet10 40^3 mixed: 15 levels against 18, 1.6 % more iterations,
@@ -367,7 +369,17 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
                                h->sym, err, /*pattern=*/false);
         else
             analysed = analyse_topology(p->n_nodes, p->nodes_per_elem, p->n_elems, p->conn, h->h_fixed.data(),
-                                        h->sym, kept, kept_of, err, /*boundary_lists=*/true);
+                                        h->sym, kept, kept_of, err, /*boundary_lists=*/true,
+                                        /*incidence=*/false);
+        if (p->imposed)
+            for (int64_t k = 0; k < n3; ++k)
+                if (h->h_fixed[k] && p->imposed[k] != 0.0) {
+                    h->any_imposed = true;
+                    break;
+                }
+        h->h_f.assign(n3, 0.0);
+        if (p->f) std::memcpy(h->h_f.data(), p->f, n3 * sizeof(double));
+        h->h_f0 = h->h_f;
         t_setup1 = now_ms();
     });
     struct Joiner {
@@ -399,19 +411,31 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         CK(cudaEventRecord(h->ev[0], st));
         tmark("context");
         const int np = node_pairs(h->npe);
-        // inputs
-        std::vector<int32_t> conn32(p->n_elems * p->nodes_per_elem);
-        for (size_t k = 0; k < conn32.size(); ++k) conn32[k] = (int32_t)p->conn[k];
+        // inputs, straight from the caller's buffers: the connectivity is narrowed to 32 bits and
+        // the imposed values kept at fixed DOFs only on the device
+        const int64_t nconn = p->n_elems * p->nodes_per_elem;
+        struct DevTemp {
+            void* p = nullptr;
+            ~DevTemp() { dfree(p); }
+        } conn64;
+        conn64.p = dupload(p->conn, nconn, st);
         h->coords = dupload(p->coords, n3, st);
-        h->conn = dupload(conn32.data(), conn32.size(), st);
+        h->conn = dalloc<int32_t>(nconn);
+        gpu_narrow(static_cast<const int64_t*>(conn64.p), nconn, h->conn, st);
         h->young = dupload(p->young, p->n_elems, st);
         h->poisson = dupload(p->poisson, p->n_elems, st);
-        h->imposed = dupload(h->h_imposed.data(), n3, st);
-        h->f0 = dupload(h->h_f.data(), n3, st);
+        h->fixed = dupload(h->h_fixed.data(), n3, st);
+        h->imposed = dupload(p->imposed, n3, st);
+        if (p->imposed)
+            gpu_zero_free(n3, h->fixed, h->imposed, st);
+        else
+            CK(cudaMemsetAsync(h->imposed, 0, n3 * sizeof(double), st));
+        h->f0 = dupload(p->f, n3, st);
+        if (!p->f) CK(cudaMemsetAsync(h->f0, 0, n3 * sizeof(double), st));
         h->f = dalloc<double>(n3);
         h->f_cur = h->f0;
-        h->h_f0 = h->h_f;
-        h->fixed = dupload(h->h_fixed.data(), n3, st);
+        h->inc_ptr = dalloc<int64_t>(p->n_nodes + 1);
+        h->inc = dalloc<int32_t>(nconn);
         h->ke = dalloc<double>((size_t)p->n_elems * np * 9);
         CK(cudaEventRecord(h->ev[8], st));  // inputs copied
         {
@@ -420,6 +444,7 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
         }
         CK(cudaEventRecord(h->ev[9], st));  // element matrices integrated
         const double t_wait0 = now_ms();
+        gpu_incidence(h->conn, nconn, p->n_nodes, st, h->inc_ptr, h->inc);
         if (host_ordering) {
             analysis.join();
             if (!analysed) return fail(err);
@@ -482,8 +507,6 @@ int32_t create_impl(const MailleElasticProblem* p, MailleGpuHandle** out, Maille
             h->pu.upload(pt, s.nb, st);
         }
         CK(cudaEventRecord(h->ev[11], st));  // pattern and layouts on the device
-        h->inc_ptr = dupload(s.inc_ptr.data(), s.inc_ptr.size(), st);
-        h->inc = dupload(s.inc.data(), s.inc.size(), st);
         h->belem = dupload(s.belem.data(), s.belem.size(), st);
         h->bnodes = dupload(s.bnodes.data(), s.bnodes.size(), st);
         std::vector<int32_t> slot(p->n_elems, -1);

@@ -1195,7 +1195,7 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
                                /*boundary_lists=*/false);
         else
             analysed = analyse_topology(n, npe, ne, p->conn, fixed3.data(), sym, kept, kept_of, err,
-                                        /*boundary_lists=*/false);
+                                        /*boundary_lists=*/false, /*incidence=*/false);
         t_setup1 = now_ms();
     });
     struct Joiner {
@@ -1233,9 +1233,7 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
         for (auto& e : ev) CK(cudaEventCreate(&e));
         ensure_rules();
         CK(cudaEventRecord(ev[0], st));
-        // inputs
-        std::vector<int32_t> conn32(ne * npe);
-        for (size_t k = 0; k < conn32.size(); ++k) conn32[k] = (int32_t)p->conn[k];
+        // inputs (the connectivity is narrowed to 32 bits on the device)
         // convection faces grouped by element, the model's order kept inside an element
         std::vector<int32_t> face_ptr(ne + 1, 0), face_id;
         std::vector<double> face_film;
@@ -1256,15 +1254,20 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
                 face_film[at] = p->conv_film[k];
             }
         }
-        std::vector<double> imposed(n, 0.0);
-        if (p->imposed)
-            for (int64_t v = 0; v < n; ++v) imposed[v] = p->fixed[v] ? p->imposed[v] : 0.0;
         double* coords = mem.take(dupload(p->coords, 3 * n, st));
-        int32_t* conn = mem.take(dupload(conn32.data(), conn32.size(), st));
+        int64_t* conn64 = mem.take(dupload(p->conn, ne * npe, st));
+        int32_t* conn = mem.take(dalloc<int32_t>(ne * npe));
+        gpu_narrow(conn64, ne * npe, conn, st);
         double* kcond = mem.take(dupload(p->conductivity, ne, st));
         double* rhoc = mem.take(dupload(p->rho_c, ne, st));
         uint8_t* fixed = mem.take(dupload(p->fixed, n, st));
-        double* imp = mem.take(dupload(imposed.data(), n, st));
+        double* imp = mem.take(dupload(p->imposed, n, st));
+        if (p->imposed)
+            gpu_zero_free(n, fixed, imp, st);
+        else
+            CK(cudaMemsetAsync(imp, 0, n * sizeof(double), st));
+        int64_t* inc_ptr = mem.take(dalloc<int64_t>(n + 1));
+        int32_t* inc = mem.take(dalloc<int32_t>(ne * npe));
         double* f = p->f ? mem.take(dupload(p->f, n, st)) : nullptr;
         double* initial = mem.take(dupload(p->initial, n, st));
         int32_t* fptr = mem.take(dupload(face_ptr.data(), face_ptr.size(), st));
@@ -1283,6 +1286,7 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
             CK(cudaGetLastError());
         }
         CK(cudaEventRecord(ev[2], st));
+        gpu_incidence(conn, ne * npe, n, st, inc_ptr, inc);
         if (host_ordering) {
             analysis.join();
             if (!analysed) return th_fail(err.status, err.message);
@@ -1304,8 +1308,6 @@ int32_t thermal_transient(const MailleThermalProblem* p, MailleThermalResult* re
         const int32_t nb = sym.nb;
         int32_t* perm = mem.take(dupload(sym.perm.data(), sym.perm.size(), st));
         int32_t* inv = mem.take(dupload(sym.inv.data(), sym.inv.size(), st));
-        int64_t* inc_ptr = mem.take(dupload(sym.inc_ptr.data(), sym.inc_ptr.size(), st));
-        int32_t* inc = mem.take(dupload(sym.inc.data(), sym.inc.size(), st));
         std::vector<int32_t> fixed_nodes;
         for (int64_t v = 0; v < n; ++v)
             if (p->fixed[v]) fixed_nodes.push_back((int32_t)v);
