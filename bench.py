@@ -423,7 +423,12 @@ def large_strain_section(mb, mg, steps, device):
     out.update({"forward_ms": statistics.median(fw), "backward_ms": statistics.median(bw),
                 "backward_over_forward": statistics.median(bw) / statistics.median(fw),
                 "newton_total": int(h.newton_total), "pcg_total": int(h.pcg_total),
-                "tip_reaction": float(h.reactions[-1, tip].sum())})
+                "tip_reaction": float(h.reactions[-1, tip].sum()),
+                "ms_per_pcg_iteration": statistics.median(fw) / max(1, int(h.pcg_total)),
+                "roofline": None,
+                "roofline_note": "no HBM roofline: the tangent matrix and factor (about 19 MB) stay in the "
+                                 "126 MB L2, so the inner PCG is bound by the sweeps' latency; the kernel's "
+                                 "ncu summary is profiles/k_pcg_large_strain_64x16x16.md"})
     path = os.path.join(ROOT, "tests", "golden", "large_strain_oracle_summary.json")
     if os.path.exists(path):
         g = json.load(open(path))
@@ -759,6 +764,19 @@ def run_ours(args):
     clk = clocks.stop()
     mixed_field = hm.solve()
     err_mixed = float(np.linalg.norm(mixed_field.displacements - u_ref) / np.linalg.norm(u_ref))
+    # and against the CPU oracle's own full-size solve at 1e-13 (sampled DOFs and compliance of
+    # the committed golden summary), so the accuracy gate does not rest on the GPU alone
+    err_oracle = None
+    gpath = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
+                         "tet10_40_oracle_tol1e-13.json")
+    if args.cells == 40 and os.path.exists(gpath):
+        with open(gpath) as fh:
+            gold = json.load(fh)
+        dofs, gu = np.array(gold["dofs"]), np.array(gold["u"])
+        err_oracle = {
+            "rel_err_sampled_dofs": float(np.linalg.norm(mixed_field.displacements[dofs] - gu) / np.linalg.norm(gu)),
+            "rel_err_compliance": float(abs(f @ mixed_field.displacements - gold["compliance"]) / abs(gold["compliance"])),
+            "samples": int(dofs.size), "oracle_tol": gold["tol"]}
 
     # max over ranks of the per-step time
     if world > 1:
@@ -871,7 +889,9 @@ def run_ours(args):
                    "tol": args.tol, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (matrices > 1 GB)", "ordering": args.ordering,
                    "levels": info_m["levels"], "blocks": info_m["blocks"]},
-        "accuracy": {"rel_err_vs_fp64": err_mixed, "target": 1e-8, "ok": err_mixed <= 1e-8},
+        "accuracy": {"rel_err_vs_fp64": err_mixed, "target": 1e-8,
+                     "ok": err_mixed <= 1e-8 and (err_oracle is None or err_oracle["rel_err_sampled_dofs"] <= 1e-8),
+                     "vs_oracle": err_oracle},
         "mixed": {"iterations": info_m["iterations"], "outer": info_m["outer_iterations"],
                   "ms_assembly": info_m["ms_assembly"], "ms_factor": info_m["ms_factor"],
                   "ms_solve": info_m["ms_solve"], "ms_post": info_m["ms_post"]},
