@@ -470,23 +470,32 @@ __global__ void __launch_bounds__(256) k_batch_pcg(BatchArgs<M, T> a, int passes
                     stx<T, Gm::N, AB>(a.z + o, zv);
                     st_release(a.flags + (int64_t)row * Gm::G + g, epoch);
                 }
+                // the slice's column partials go to its slot; the instance totals are summed after
+                // the barrier (no ticket: a warp never waits on an atomic's round trip per slice)
                 const double tot = cols_to_lanes<R, Q, SUB>(part);
                 const int us = __ldg(a.uslot + sl);
-                const int b0 = __ldg(a.inst_uslot + inst), cnt = __ldg(a.inst_uslot + inst + 1) - b0;
-                if (publish<R>(tot, a.part_u, us, a.tickets + a.n_inst + inst, cnt)) {
-                    const double rz = ordered_total<R>(a.part_u, b0, cnt);
-                    if (lane < R) {
-                        const int64_t s = (int64_t)inst * R + lane;
-                        const bool live = !((dm >> lane) & 1u);
-                        // iterative.rs:237-239: beta = rz_new / rz_old (0 on the first pass)
-                        st.beta[s] = (live && !first) ? rz / st.rz[s] : 0.0;
-                        if (live) st.rz[s] = rz;
-                    }
-                    if (MIXED && lane == 0) st.flagged[inst] = 0u;
-                }
+                if (lane < R) a.part_u[(int64_t)us * R + lane] = tot;
             }
             if (!ok) atomicExch(st.ctrl + 2, 1);
             if (MIXED && blockIdx.x == 0 && threadIdx.x == 0) st.ctrl[1] = 0;
+        }
+        grid.sync();
+        // ---- r.z per column: one warp per instance sums its slots in slot order ---------------
+        if (__ldcg(st.ctrl + 2) == 0) {
+            for (int32_t inst = warp; inst < a.n_inst; inst += nwarps) {
+                const uint32_t dm = __ldcg(st.done + inst);
+                if (dm == FULL) continue;
+                const int b0 = __ldg(a.inst_uslot + inst), cnt = __ldg(a.inst_uslot + inst + 1) - b0;
+                const double rz = ordered_total<R>(a.part_u, b0, cnt);
+                if (lane < R) {
+                    const int64_t s = (int64_t)inst * R + lane;
+                    const bool live = !((dm >> lane) & 1u);
+                    // iterative.rs:237-239: beta = rz_new / rz_old (0 on the first pass)
+                    st.beta[s] = (live && !first) ? rz / st.rz[s] : 0.0;
+                    if (live) st.rz[s] = rz;
+                }
+                if (MIXED && lane == 0) st.flagged[inst] = 0u;
+            }
         }
         grid.sync();
         mark(4);
@@ -547,8 +556,15 @@ __global__ void __launch_bounds__(256) k_batch_pcg(BatchArgs<M, T> a, int passes
                 stx<T, Gm::N, AB>(a.ap + o, av);
             }
             const double tot = cols_to_lanes<R, Q, SUB>(part);
+            if (lane < R) a.part_k[(int64_t)t * R + lane] = tot;
+        }
+        grid.sync();
+        // ---- p.ap per column: one warp per instance sums its task slots in order -------------
+        for (int32_t inst = warp; inst < a.n_inst; inst += nwarps) {
+            const uint32_t dm = __ldcg(st.done + inst);
+            if (dm == FULL) continue;
             const int b0 = a.inst_task[inst], cnt = a.inst_task[inst + 1] - b0;
-            if (publish<R>(tot, a.part_k, t, a.tickets + inst, cnt)) {
+            {
                 const double pap = ordered_total<R>(a.part_k, b0, cnt);
                 bool bad = false;
                 if (lane < R) {
@@ -605,8 +621,15 @@ __global__ void __launch_bounds__(256) k_batch_pcg(BatchArgs<M, T> a, int passes
                 stx<T, Gm::N, AB>(a.r + o, rv);
             }
             const double tot = cols_to_lanes<R, Q, SUB>(part);
+            if (lane < R) a.part_k[(int64_t)t * R + lane] = tot;
+        }
+        grid.sync();
+        // ---- ||r||^2 per column and the stopping test: one warp per instance -----------------
+        for (int32_t inst = warp; inst < a.n_inst; inst += nwarps) {
+            const uint32_t dm = __ldcg(st.done + inst);
+            if (dm == FULL) continue;
             const int b0 = a.inst_task[inst], cnt = a.inst_task[inst + 1] - b0;
-            if (publish<R>(tot, a.part_k, t, a.tickets + inst, cnt)) {
+            {
                 const double rrv = ordered_total<R>(a.part_k, b0, cnt);
                 const int it = __ldcg(st.iter + inst);
                 const bool capped = it >= a.max_iter;
