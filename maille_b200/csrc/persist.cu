@@ -12,7 +12,10 @@
 //
 // Sweeps are dataflow instead of one barrier per level: warps take slices in level order on a
 // fixed round-robin schedule; before gathering a neighbour's value a lane waits until that row
-// has been written in the current sweep (epoch). A slice only depends on slices of earlier
+// has been written in the current sweep (epoch): while any record of the warp is stale, one lane
+// polls the one likely written last and the warp then re-reads its stale records together (a
+// poll by every lane is up to 128 scattered L2 requests per warp, and the waiting warps' polls
+// delayed the working warps' own instructions). A slice only depends on slices of earlier
 // levels, which come earlier in every warp's schedule, and all warps are co-resident
 // (cooperative launch), so every wait ends; each wait is also bounded and reports a timeout
 // status instead of spinning forever. How a lane knows a row is ready depends on the precision:
