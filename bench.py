@@ -584,11 +584,12 @@ def oracle_section(name):
     import oracle
     from maille_b200 import meshgen as mg
     t0 = time.perf_counter()
-    if name == "plain_tet4_20":
+    if name in ("plain_tet4_20", "plain_tet4_20_tol1e-12"):
+        tol = 1e-12 if name.endswith("1e-12") else 1e-10
         p = mg.plain_tet4(20)
-        r = oracle.model_solve(p, solver=2, tol=1e-10)
+        r = oracle.model_solve(p, solver=2, tol=tol)
         wall = time.perf_counter() - t0
-        return {"workload": "tet4_20^3_plain_fp64", "status": r["status"], "free_dofs": p.free_dofs,
+        return {"workload": "tet4_20^3_plain_fp64", "tol": tol, "status": r["status"], "free_dofs": p.free_dofs,
                 "iterations": r["iterations"], "wall_s": wall, "value": p.free_dofs / wall, "unit": UNIT}
     if name == "thermal":
         p = mg.thermal_cube(40, True, increments=10, time_period=0.1)
@@ -627,7 +628,7 @@ def run_reference(args):
     small = mg.mixed_tet10(4)
     for _ in range(args.warmup):  # untimed warm-up on a small mesh of the same family
         oracle.model_solve(small, solver=2, tol=args.tol)
-    sides = ["plain_tet4_20", "thermal", "large_strain"]
+    sides = ["plain_tet4_20", "plain_tet4_20_tol1e-12", "thermal", "large_strain"]
     cores = os.cpu_count() or 1
     pool = None
     futures = {}
@@ -852,6 +853,8 @@ def run_ours(args):
                            "another (ms_ordering: the device ordering, wall time)")}
 
     plain_tet4 = plain_tet4_section(torch, mb, mg, L, args.steps, args.warmup, local)
+    # the same configuration at the reference's default tolerance (iterative.rs:9)
+    plain_tet4_12 = plain_tet4_section(torch, mb, mg, L, args.steps, args.warmup, local, tol=1e-12)
 
     batched = None
     if not args.no_batched:
@@ -911,6 +914,7 @@ def run_ours(args):
                  "fp64": {"achieved": gbs64, "frac": gbs64 / hbm, "bytes_per_launch": bytes64,
                           "ms_per_launch": ms64}},
         "plain_tet4_20": plain_tet4,
+        "plain_tet4_20_tol1e-12": plain_tet4_12,
         "batched": batched,
         "large_strain": large_strain,
         "adjoint": adjoint,
