@@ -78,7 +78,8 @@ typedef struct {
     const double* young;     /* [n_elems] E per element (Tet4/Tet10 carry their Material) */
     const double* poisson;   /* [n_elems] nu per element */
     const uint8_t* fixed;    /* [3 n_nodes] 1 where a Bc fixes the DOF (3 node + c) */
-    const double* imposed;   /* [3 n_nodes] imposed values at fixed DOFs (ignored elsewhere) */
+    const double* imposed;   /* [3 n_nodes] imposed values at fixed DOFs (ignored elsewhere, any
+                                value there), or NULL for zero */
     const double* f;         /* [3 n_nodes] assembled nodal loads F (loads + face pressures), or
                                 NULL for zero */
     double rel_tol;          /* stop at ||r|| <= rel_tol ||b|| (the reference uses 1e-12);
